@@ -1,0 +1,178 @@
+/*
+ * ehd.h -- C ABI of the B200 (sm_100a) EHD convection time step.
+ *
+ * Drop-in for the reference solver's step (gyf135/EHD-convection-3D).  The
+ * reference has no plugin or FFI layer: its step is a sequence of free host
+ * functions called from main() (main.cu:184-206) over global device pointers
+ * and compile-time constants (LBM.h:30-113).  Each entry point below names the
+ * reference interface it replaces.  Conventions:
+ *
+ *   - every function returns 0 (EHD_OK) or a negative ehd_status; nothing
+ *     calls exit() (the reference exits on any error, LBM.cu:39-57,
+ *     LBM.h:140-161).  ehd_last_error() gives the message of the last failure
+ *     on the calling thread;
+ *   - all field arguments are HOST pointers to NX*NY*NZ doubles in the
+ *     reference layout, index x + NX*(y + NY*z) (LBM.cu:21-24), unless the
+ *     name ends in _device;
+ *   - one context per simulation instance; a context is not thread-safe.
+ *     All device work of a context runs on its stream (ehd_config.stream, or
+ *     a stream the context creates).
+ */
+#ifndef EHD_H
+#define EHD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EHD_ABI_VERSION 1
+
+typedef enum ehd_status {
+    EHD_OK = 0,
+    EHD_ERR_INVALID = -1,   /* bad argument or parameter                  */
+    EHD_ERR_CUDA = -2,      /* a CUDA runtime call failed                 */
+    EHD_ERR_NOMEM = -3,     /* device or host allocation failed           */
+    EHD_ERR_STATE = -4,     /* call out of order (e.g. step before set)   */
+    EHD_ERR_NUMERIC = -5,   /* non-finite value detected                  */
+    EHD_ERR_IO = -6         /* file read/write failed                     */
+} ehd_status;
+
+/* Physical, geometric and scheme parameters: the reference's compile-time
+ * constants and __device__ scalars (LBM.h:30-80, main.cu:27-36) as a runtime
+ * struct.  nz counts nodes; the electrodes are the planes z=0 and z=nz-1. */
+typedef struct ehd_params {
+    int32_t nx, ny, nz;      /* NX, NY, NZ (LBM.h:34-36)                       */
+    int32_t pad_;            /* must be 0                                      */
+    double lx, ly, lz;       /* Lx, Ly, Lz (LBM.h:40-42)                       */
+    double dx, dy, dz;       /* dx, dy, dz (LBM.h:43-45)                       */
+    double dt, cfl;          /* dt, CFL (LBM.h:50-52); cs^2 = 1/(3 CFL^2)      */
+    double rho0, charge0;    /* rho0, charge0 (LBM.h:54-55)                    */
+    double voltage, eps;     /* voltage, eps (LBM.h:56-57)                     */
+    double diffu, nu, K;     /* diffu, nu, K (LBM.h:58-62)                     */
+    double uw, exf;          /* uw, exf (LBM.h:47-50)                          */
+    double lambda_f;         /* TRT magic parameter of f, V (LBM.h:79)        */
+    double lambda_g;         /* TRT magic parameter of g, VC (LBM.h:80)       */
+} ehd_params;
+
+/* Arithmetic of the step.  The reference computes and stores in FP64. */
+typedef enum ehd_precision {
+    EHD_PREC_FP64 = 0,       /* FP64 compute, FP64 populations                 */
+    EHD_PREC_FP32 = 1,       /* FP32 compute, FP32 populations                 */
+    EHD_PREC_FP16 = 2,       /* FP32 compute, FP16 population deviations       */
+    EHD_PREC_BF16 = 3        /* FP32 compute, BF16 population deviations       */
+} ehd_precision;
+
+typedef struct ehd_config {
+    int32_t precision;       /* ehd_precision                                  */
+    int32_t device;          /* CUDA device ordinal                            */
+    void *stream;            /* cudaStream_t to run on, or NULL: own stream    */
+    uint32_t flags;          /* EHD_FLAG_*                                     */
+    uint32_t reserved[7];    /* must be 0                                      */
+} ehd_config;
+
+#define EHD_FLAG_NO_GRAPH 0x1u /* launch kernels one by one, no CUDA graphs   */
+
+typedef struct ehd_ctx ehd_ctx;
+
+/* Scalar diagnostics, reduced on the device in FP64. */
+typedef struct ehd_diag {
+    double current;          /* I = K dy^2 sum_xy q(NZ-1) Ez(NZ-1), LBM.cu:1647 */
+    double nu_e;             /* I / I0 (I0 from ehd_set_reference_current)     */
+    double kinetic_energy;   /* 0.5 sum rho |u|^2 dx dy dz                      */
+    double total_charge;     /* sum q dx dy dz                                  */
+    double umax;             /* max uz over the domain, LBM.cu:1673-1713        */
+    double time;             /* physical time t (main.cu:208)                   */
+    int64_t step;            /* steps taken since ehd_set_fields               */
+    int32_t nonfinite;       /* 1 if any field holds a NaN or Inf              */
+    int32_t pad_;
+} ehd_diag;
+
+/* --- lifetime ------------------------------------------------------------ */
+
+/* Allocates every device buffer of one instance and prepares the Poisson
+ * solver.  Replaces main.cu:79-143 (cudaMalloc of the fields and populations,
+ * cufftPlan3d, the kx/ky/kz tables). */
+int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out);
+
+/* Frees everything.  Replaces main.cu:283-304. */
+int ehd_destroy(ehd_ctx *ctx);
+
+/* --- state ----------------------------------------------------------------- */
+
+/* Uploads the nine macroscopic fields and builds the equilibrium populations
+ * from them.  Replaces read_data (LBM.cu:1597-1643) + init_equilibrium
+ * (LBM.cu:98-276).  The first step after this call uses the given E; later
+ * steps use E = -grad(phi) from the Poisson solve, as the reference does. */
+int ehd_set_fields(ehd_ctx *ctx, const double *rho, const double *u, const double *v,
+                   const double *w, const double *q, const double *phi, const double *ex,
+                   const double *ey, const double *ez);
+
+/* The reference's own start (initialization, LBM.cu:69-96, then
+ * init_equilibrium): rho = rho0, q = 0, phi linear, u = E = 0. */
+int ehd_initialize(ehd_ctx *ctx);
+
+/* Downloads the nine fields, raw (no wall extrapolation), in the reference
+ * layout.  Any pointer may be NULL to skip that field.  Replaces the D2H
+ * copies of save_data_* (LBM.cu:1427-1566). */
+int ehd_get_fields(ehd_ctx *ctx, double *rho, double *u, double *v, double *w, double *q,
+                   double *phi, double *ex, double *ey, double *ez);
+
+/* --- the time step ------------------------------------------------------ */
+
+/* Advances nsteps time steps: per step the fused LBM stream-collide with its
+ * wall and injection rules, then the Poisson solve and E = -grad(phi).
+ * Replaces the loop body main.cu:184-208: stream_collide_save (LBM.cu:278),
+ * extension (poisson.cu:78), cufftExecZ2Z x2 (main.cu:194,200), derivative
+ * (poisson.cu:123), extract (poisson.cu:145), efield (poisson.cu:33).
+ * Asynchronous on the context's stream. */
+int ehd_step(ehd_ctx *ctx, int nsteps);
+
+/* The LBM half of one step only (stream_collide_save, LBM.cu:278-293). */
+int ehd_stream_collide_save(ehd_ctx *ctx);
+
+/* The Poisson half of one step only, from the current q: extension,
+ * forward FFT, derivative, inverse FFT, extract and efield
+ * (poisson.cu:33-167, main.cu:190-206). */
+int ehd_poisson(ehd_ctx *ctx);
+
+/* Blocks until the context's queued work is done. */
+int ehd_synchronize(ehd_ctx *ctx);
+
+/* --- diagnostics ---------------------------------------------------------- */
+
+/* Collector current of the present fields.  Replaces current()
+ * (LBM.cu:1647-1671) with its host loop over a full-field D2H copy. */
+int ehd_current(ehd_ctx *ctx, double *current);
+
+/* Sets I0, the hydrostatic current that normalises nu_e. */
+int ehd_set_reference_current(ehd_ctx *ctx, double i0);
+
+/* All scalar diagnostics, reduced on the device (blocks until done). */
+int ehd_diagnostics(ehd_ctx *ctx, ehd_diag *out);
+
+/* --- information -------------------------------------------------------- */
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *ehd_last_error(void);
+
+/* Bytes of device memory the context holds. */
+int ehd_device_bytes(const ehd_ctx *ctx, size_t *bytes);
+
+/* Inverse of compute_parameters (LBM.cu:1356-1379): fills K, nu, charge0 and
+ * diffu of *p from the dimensionless groups T, M, C, Fe, keeping eps,
+ * voltage, rho0 and lz as they are in *p. */
+int ehd_params_from_groups(ehd_params *p, double T, double M, double C, double Fe);
+
+/* compute_parameters itself (LBM.cu:1356-1379). */
+int ehd_groups_from_params(const ehd_params *p, double *T, double *M, double *C, double *Fe);
+
+int ehd_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EHD_H */
