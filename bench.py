@@ -1,0 +1,407 @@
+"""Benchmark: MLUPS of the full EHD time step on 256 x 256 x 129 nodes.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One "step" is one time step of the whole domain: the fused LBM stream-collide
+for f and g with the wall and injection rules, then the Poisson solve and
+E = -grad(phi).  The workload is the production-size configuration
+(256 x 256 cells x 128 cells in z, i.e. 256 x 256 x 129 nodes, Lx = Ly = 2,
+T = 200, M = 10, C = 10, Fe = 4000, TRT magic parameters 1/4), FP32 compute
+with FP32 population storage for the headline; FP16 / BF16 deviation storage
+and FP64 are measured in the same run as variants.  Inputs are synthetic:
+the reference's initial state (LBM.cu:81-96) plus a seeded 1e-3 velocity
+perturbation.  The working set (3.7 GB in FP32) is far larger than the
+126 MB L2, so no explicit flush is needed between steps.
+
+Multi-GPU: the single-domain step does not shard (the Poisson z-solve couples
+all planes); N GPUs run N independent replicas ("weak" scaling), timed as
+the max over ranks.
+
+--impl reference times the reference's own CUDA build of the same step
+(compiled from its sources into oracle/_ref/bench/ehd_ref, FP64 as it runs)
+on the same grid and physics.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG = ROOT / "ehd-convection-3d_b200"
+NX, NY, NZ = 256, 256, 129  # the workload; --grid overrides it for profiling only
+NODES = NX * NY * NZ
+KERNELS_PER_STEP = 6  # lbm_step + 5 Poisson kernels (rows_fwd, cols, zsolve, cols, rows_inv)
+# Algorithmic bytes per node of one lbm_step launch (macros written, as
+# ehd_stream_collide_save does): 27 f + 27 g read and written, q written,
+# phi' read, rho/u/v/w written.  s = population bytes, p = field bytes.
+def lbm_bytes_per_node(s: int, p: int) -> int:
+    return 2 * 27 * 2 * s + p * (1 + 1 + 4)
+
+
+# DRAM traffic per lbm_step launch from ncu (profiles/lbm_step_fp32.md), scaled
+# to one full 256x256x129 launch; None until captured.
+NCU_TRAFFIC_BYTES = None
+
+
+def load_ehd():
+    spec = importlib.util.spec_from_file_location("ehd", PKG / "ehd.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["ehd"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.file:
+            return None
+        try:
+            rows = [r.split(",") for r in Path(self.file.name).read_text().splitlines() if r.strip()]
+            os.unlink(self.file.name)
+        except Exception:
+            return None
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for i, nm in enumerate(names):
+                if r[5 + i].strip() == "Active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload_params(ehd):
+    return ehd.params_from_groups(NX, NY, NZ, 2.0, 2.0, T=200, M=10, C=10, Fe=4000,
+                                  lambda_f=0.25, lambda_g=0.25)
+
+
+def initial_fields(p, seed=0):
+    sh = (p.nz, p.ny, p.nx)
+    rng = np.random.default_rng(seed)
+    z = np.arange(p.nz, dtype=np.float64)[:, None, None] * p.dz
+    f = {"rho": np.full(sh, p.rho0), "q": np.zeros(sh),
+         "phi": np.broadcast_to(p.voltage * (p.lz - z) / p.lz, sh).copy(),
+         "ex": np.zeros(sh), "ey": np.zeros(sh), "ez": np.zeros(sh)}
+    for k in ("u", "v", "w"):
+        a = rng.uniform(-1e-3, 1e-3, sh)
+        a[0] = 0.0
+        a[-1] = 0.0
+        f[k] = a
+    return f
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    ehd = load_ehd()
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local_rank))
+    p = workload_params(ehd)
+    fields = initial_fields(p, seed=rank)
+    stream = torch.cuda.Stream()
+    K, W = args.steps, args.warmup
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def device_mlups(prec, sampler_gpu=None):
+        sim = ehd.Simulation(p, prec, device=local_rank, stream=stream.cuda_stream)
+        cs = ClockSampler(sampler_gpu) if sampler_gpu is not None else None
+        try:
+            sim.set_fields(fields)
+            if cs:
+                cs.__enter__()  # samples through the warm-up and the timed region
+            sim.step(W)
+            sim.synchronize()
+            torch.cuda.synchronize()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            clocks = None
+            e0.record(stream)
+            sim.step(K)
+            e1.record(stream)
+            e1.synchronize()
+            if cs:
+                cs.__exit__()
+                clocks = cs.summary()
+            torch.cuda.synchronize()
+            ms = max_over_ranks(e0.elapsed_time(e1))
+            barrier()
+            # dominant kernel alone: lbm_step via ehd_stream_collide_save
+            e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            nk = max(5, min(K, 50))
+            e2.record(stream)
+            for _ in range(nk):
+                sim.stream_collide_save()
+            e3.record(stream)
+            e3.synchronize()
+            lbm_ms = e2.elapsed_time(e3) / nk
+            diag = sim.diagnostics()
+            return ms, lbm_ms, clocks, diag
+        finally:
+            sim.close()
+
+    ms, lbm_ms, clocks, diag = device_mlups(args.precision, sampler_gpu=local_rank)
+    value = world * K * NODES / (ms * 1e-3) / 1e6
+    if args.no_e2e:
+        if rank == 0:
+            print(json.dumps({"profile_run": True, "value": round(value, 1),
+                              "ms_per_step": round(ms / K, 4), "lbm_kernel_ms": round(lbm_ms, 4),
+                              "grid": [NX, NY, NZ], "precision": args.precision}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    # ---- end to end through the public API, host buffers ----
+    pinned_in = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory()
+                 for k, v in fields.items()}
+    pinned_out = {k: torch.empty(p.nz * p.ny * p.nx, dtype=torch.float64).pin_memory()
+                  for k in ehd.FIELDS}
+    sim = ehd.Simulation(p, "fp32", device=local_rank, stream=stream.cuda_stream)
+    import ctypes
+    dp = ctypes.POINTER(ctypes.c_double)
+
+    def host_ptr(t):
+        return ctypes.cast(ctypes.c_void_p(t.data_ptr()), dp)
+
+    L = ehd.lib()
+    # warm-up of the same sequence
+    L.ehd_set_fields(sim.h, *[host_ptr(pinned_in[k]) for k in ehd.FIELDS])
+    sim.step(W)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    rc = L.ehd_set_fields(sim.h, *[host_ptr(pinned_in[k]) for k in ehd.FIELDS])
+    cur = 0.0
+    for _ in range(K):
+        sim.step(1)
+        cur = sim.current()
+    rc |= L.ehd_get_fields(sim.h, *[host_ptr(pinned_out[k]) for k in ehd.FIELDS])
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    sim.close()
+    if rc != 0:
+        raise RuntimeError("e2e API call failed: " + L.ehd_last_error().decode())
+    e2e = world * K * NODES / e2e_s / 1e6
+    field_bytes = 9 * NODES * 8
+
+    # ---- storage variants, same workload ----
+    variants = {}
+    if not args.no_variants:
+        for prec in ("fp16", "bf16", "fp64"):
+            vms, vlbm, _, vdiag = device_mlups(prec)
+            s = {"fp16": 2, "bf16": 2, "fp64": 8}[prec]
+            pf = 8 if prec == "fp64" else 4
+            variants[prec] = {
+                "value": round(world * K * NODES / (vms * 1e-3) / 1e6, 1),
+                "ms_per_step": round(vms / K, 4),
+                "lbm_kernel_ms": round(vlbm, 4),
+                "lbm_kernel_gbs": round(lbm_bytes_per_node(s, pf) * NODES / (vlbm * 1e-3) / 1e9, 1),
+                "nonfinite": vdiag["nonfinite"]}
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    peak, peak_kind = peaks()
+    achieved = lbm_bytes_per_node(4, 4) * NODES / (lbm_ms * 1e-3) / 1e9
+    line = {
+        "metric": "MLUPS full EHD step at 256x256x128 cells (256x256x129 nodes)",
+        "value": round(value, 1),
+        "unit": "MLUPS",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": round(ms / K, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32",
+        "data": "synthetic: reference initial state + seeded 1e-3 velocity noise",
+        "config": {"workload": "EHD step 256x256x129 nodes, Lx=Ly=2, T=200 M=10 C=10 Fe=4000, "
+                               "TRT 1/4, FP32 populations",
+                   "nodes": NODES, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (3.7 GB working set vs 126 MB L2), no flush"},
+        "e2e": {"value": round(e2e, 1), "unit": "MLUPS",
+                "h2d_bytes_per_step": round(field_bytes / K),
+                "d2h_bytes_per_step": round(8 + field_bytes / K),
+                "how": "ehd_set_fields from pinned host memory, K x (ehd_step(1) + "
+                       "ehd_current readback), ehd_get_fields to pinned host memory; wall clock"},
+        "roofline": {"bound": "hbm", "kernel": "lbm_step_kernel<float,float>",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "bytes_per_node": lbm_bytes_per_node(4, 4),
+                     "kernel_ms": round(lbm_ms, 4), "traffic": NCU_TRAFFIC_BYTES},
+        "gpu_launches": K * KERNELS_PER_STEP,
+        "clocks": clocks,
+        "variants": variants,
+        "diag": {k: diag[k] for k in ("current", "kinetic_energy", "nonfinite")},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(steps=2):
+    """The oracle (FP64 C/OpenMP port of the reference step) on all host cores,
+    a bounded sample: `steps` time steps of the full 256x256x129 grid."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    p = O.params_from_groups(NX, NY, NZ, 2.0, 2.0, T=200, M=10, C=10, Fe=4000)
+    o = O.Oracle(p)
+    o.set_fields(initial_fields(p))
+    o.step(1)  # warm-up (page faults)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    o.close()
+    return {"value": round(steps * NODES / dt / 1e6, 3), "unit": "MLUPS", "cores": cores,
+            "kind": "port", "sample": f"{steps} steps of 256x256x129, FP64, oracle/ehd_oracle.c "
+                                      f"with OpenMP ({dt:.1f} s)"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    exe = ROOT / "oracle" / "_ref" / "bench" / "ehd_ref"
+    K, W = args.steps, args.warmup
+    base = {"impl": "reference", "metric": "MLUPS full EHD step at 256x256x128 cells "
+            "(256x256x129 nodes)", "unit": "MLUPS", "n_gpus": 1, "steps": K, "warmup": W,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "data": "synthetic: the reference's own initialization (flag = 0)",
+            "config": {"workload": "EHD step 256x256x129 nodes, Lx=Ly=2, T=200 M=10 C=10 "
+                                   "Fe=4000, TRT 1/4", "nodes": NODES}}
+    if not exe.exists():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference binary oracle/_ref/bench/ehd_ref was not built"}))
+        return
+
+    def gpu_seconds(n):
+        with tempfile.TemporaryDirectory() as tmp:
+            r = subprocess.run([str(exe)], cwd=tmp, capture_output=True, text=True,
+                               env=dict(os.environ, EHD_REF_NSTEPS=str(n)), timeout=900)
+            if r.returncode != 0:
+                raise RuntimeError(r.stdout[-2000:] + r.stderr[-2000:])
+            for line in r.stdout.splitlines():
+                if "gpu runtime" in line:
+                    return float(line.split(":")[1].split("(")[0])
+        raise RuntimeError("no gpu runtime in the reference output")
+
+    t_w = gpu_seconds(W)
+    t_all = gpu_seconds(W + K)
+    sec = max(t_all - t_w, 1e-9)
+    value = K * NODES / sec / 1e6
+    line = dict(base, value=round(value, 1), ms_per_step=round(1e3 * sec / K, 4), dtype="fp64",
+                e2e={"value": round(value, 1), "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                     "d2h_bytes_per_step": 0},
+                cpu_baseline={"value": round(value, 1), "unit": "MLUPS", "cores": 1,
+                              "kind": "reference",
+                              "sample": f"the reference's own CUDA step (it has no CPU "
+                                        f"implementation), sm_100a build of its sources, "
+                                        f"{K} steps timed by its own cudaEvent pair as the "
+                                        f"difference of runs of {W + K} and {W} steps"})
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32", "fp16", "bf16"],
+                    help="storage of the headline run (profiling)")
+    ap.add_argument("--grid", type=int, nargs=3, metavar=("NX", "NY", "NZ"),
+                    help="smaller grid for profiling captures; not a bench line")
+    args = ap.parse_args()
+    if args.grid:
+        global NX, NY, NZ, NODES
+        NX, NY, NZ = args.grid
+        NODES = NX * NY * NZ
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

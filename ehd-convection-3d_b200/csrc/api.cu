@@ -1,0 +1,652 @@
+// api.cu -- the C ABI (include/ehd.h): context, buffers, the time step, graphs.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ehd.h"
+#include "common.cuh"
+#include "kernels.h"
+
+using namespace ehd;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define EHD_CK(call)                                                                      \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(EHD_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                              \
+    } while (0)
+
+// Makes the context's device current for the scope of one API call.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+bool only_235(int n) {
+    if (n < 1) return false;
+    for (int f : {2, 3, 5})
+        while (n % f == 0) n /= f;
+    return n == 1;
+}
+
+FftPlan make_plan(int n) {
+    FftPlan p{};
+    p.n = n;
+    p.nrad = 0;
+    while (n % 4 == 0) { p.rad[p.nrad++] = 4; n /= 4; }
+    while (n % 2 == 0) { p.rad[p.nrad++] = 2; n /= 2; }
+    while (n % 3 == 0) { p.rad[p.nrad++] = 3; n /= 3; }
+    while (n % 5 == 0) { p.rad[p.nrad++] = 5; n /= 5; }
+    return p;
+}
+
+}  // namespace
+
+struct ehd_ctx {
+    ehd_params p{};
+    ehd_config cfg{};
+    int prec = EHD_PREC_FP64;
+    int device = 0;
+    StepConst sc{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    size_t tsize = 8, rsize = 8;  // storage / compute bytes
+    std::vector<void *> allocs;
+    size_t bytes = 0;
+
+    void *f[2] = {nullptr, nullptr}, *h[2] = {nullptr, nullptr};
+    int cur = 0;  // buffer holding the populations read by the next step
+    void *q = nullptr, *rho = nullptr, *u = nullptr, *v = nullptr, *w = nullptr;
+    void *phip = nullptr;
+    double *phi00 = nullptr, *ez00 = nullptr;
+    double *ref = nullptr;  // per-plane rho_ref, q_ref (FP64)
+    void *zref = nullptr;   // the step's reference table (compute type)
+    double *out[9] = {};
+    double **out_dev = nullptr;
+    PoissonArgs pa{};
+    double *diag_partial = nullptr, *diag_result = nullptr, *host_diag = nullptr;
+    int diag_blocks = 0;
+
+    bool have_state = false;
+    bool pops_local = false;  // populations are pre-collision, in place
+    bool e_arrays = false;    // E still comes from the uploaded arrays
+    bool out_valid = false;   // FP64 field arrays match the state
+    long long step = 0;
+    double t = 0.0;
+    double i0 = 0.0;
+
+    bool use_graphs = true;
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [cur][macros]
+};
+
+namespace {
+
+int dalloc(ehd_ctx *c, void **p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(EHD_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    c->allocs.push_back(*p);
+    c->bytes += bytes;
+    return EHD_OK;
+}
+
+int validate(const ehd_params *p) {
+    if (!p) return fail(EHD_ERR_INVALID, "params is NULL");
+    if (p->nx < 1 || p->ny < 1) return fail(EHD_ERR_INVALID, "nx, ny must be >= 1");
+    if (p->nz < 4) return fail(EHD_ERR_INVALID, "nz must be >= 4 (got %d)", p->nz);
+    if (!only_235(p->nx) || !only_235(p->ny))
+        return fail(EHD_ERR_INVALID, "nx and ny must factor into 2, 3 and 5 (got %d, %d)", p->nx,
+                    p->ny);
+    if ((long long)p->nx * p->ny * p->nz > (1LL << 31))
+        return fail(EHD_ERR_INVALID, "grid too large: nx*ny*nz must be <= 2^31");
+    const double pos[] = {p->lx, p->ly, p->lz, p->dx, p->dy, p->dz, p->dt, p->cfl,
+                          p->rho0, p->eps, p->diffu, p->nu, p->lambda_f, p->lambda_g};
+    const char *names[] = {"lx", "ly", "lz", "dx", "dy", "dz", "dt", "cfl",
+                           "rho0", "eps", "diffu", "nu", "lambda_f", "lambda_g"};
+    for (int i = 0; i < 14; ++i)
+        if (!(pos[i] > 0.0) || !std::isfinite(pos[i]))
+            return fail(EHD_ERR_INVALID, "%s must be positive and finite", names[i]);
+    const double other[] = {p->charge0, p->voltage, p->K, p->uw, p->exf};
+    for (double x : other)
+        if (!std::isfinite(x)) return fail(EHD_ERR_INVALID, "non-finite parameter");
+    if (p->pad_ != 0) return fail(EHD_ERR_INVALID, "pad_ must be 0");
+    return EHD_OK;
+}
+
+StepConst make_const(const ehd_params *p) {
+    StepConst c{};
+    c.nx = p->nx;
+    c.ny = p->ny;
+    c.nz = p->nz;
+    c.nxy = (long long)p->nx * p->ny;
+    c.n = c.nxy * p->nz;
+    c.dt = p->dt;
+    c.cfl = p->cfl;
+    c.cs2 = 1.0 / 3.0 / (p->cfl * p->cfl);
+    c.cflinv = 1.0 / p->cfl;
+    c.cflinv2 = c.cflinv * c.cflinv / c.cs2;
+    const double dt = p->dt, cs2 = c.cs2;
+    // LBM.cu:297-302
+    const double omega_plus = 1.0 / (p->nu / cs2 / dt + 1.0 / 2.0) / dt;
+    const double omega_minus = 1.0 / (p->lambda_f / (p->nu / cs2 / dt) + 1.0 / 2.0) / dt;
+    const double omega_c_minus = 1.0 / (p->diffu / cs2 / dt + 1.0 / 2.0) / dt;
+    const double omega_c_plus = 1.0 / (p->lambda_g / (p->diffu / cs2 / dt) + 1.0 / 2.0) / dt;
+    c.tw0rp = omega_plus * dt;
+    c.tw0rm = omega_minus * dt;
+    c.tw0cp = omega_c_plus * dt;
+    c.tw0cm = omega_c_minus * dt;
+    const double rates[4] = {c.tw0rp, c.tw0rm, c.tw0cp, c.tw0cm};
+    for (int i = 0; i < 4; ++i) {
+        c.rate_hi[i] = rates[i] >= 1.0 ? 2.0 : rates[i];
+        c.rate_lo[i] = rates[i] >= 1.0 ? 2.0 - rates[i] : 0.0;
+    }
+    c.sp = 1.0 - 0.5 * dt * omega_plus;  // LBM.cu:987-988
+    c.sm = 1.0 - 0.5 * dt * omega_minus;
+    c.rho0 = p->rho0;
+    c.q0 = p->charge0;
+    c.K = p->K;
+    c.exf = p->exf;
+    c.inv2dx = 0.5 / p->dx;
+    c.inv2dy = 0.5 / p->dy;
+    c.inv2dz = 0.5 / p->dz;
+    // LBM.cu:1137-1139
+    const double multis = 2.0 * p->rho0 * p->uw / cs2 * w_of(1) / p->cfl;
+    const double multia = 2.0 * p->rho0 * p->uw / cs2 * w_of(7) / p->cfl;
+    const double multid = 2.0 * p->rho0 * p->uw / cs2 * w_of(19) / p->cfl;
+    for (int d = 0; d < Q; ++d) {
+        const double m = d <= 6 ? multis : (d <= 18 ? multia : multid);
+        c.mw[d] = mw_sign_of(d) * m;
+    }
+    return c;
+}
+
+int lbm(ehd_ctx *c, bool macros) {
+    LbmArgs a{};
+    a.fa = c->f[c->cur];
+    a.ha = c->h[c->cur];
+    a.fb = c->f[c->cur ^ 1];
+    a.hb = c->h[c->cur ^ 1];
+    a.phip = c->phip;
+    a.ez00 = c->ez00;
+    a.exa = c->out[6];
+    a.eya = c->out[7];
+    a.eza = c->out[8];
+    a.q = c->q;
+    a.rho = c->rho;
+    a.u = c->u;
+    a.v = c->v;
+    a.w = c->w;
+    a.zref = c->zref;
+    const int loc = c->pops_local ? 1 : 0, ea = c->e_arrays ? 1 : 0;
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (c->prec) {
+        case EHD_PREC_FP64: e = launch_lbm_step<double, double>(a, c->sc, loc, ea, macros, c->stream); break;
+        case EHD_PREC_FP32: e = launch_lbm_step<float, float>(a, c->sc, loc, ea, macros, c->stream); break;
+        case EHD_PREC_FP16: e = launch_lbm_step<__half, float>(a, c->sc, loc, ea, macros, c->stream); break;
+        case EHD_PREC_BF16: e = launch_lbm_step<__nv_bfloat16, float>(a, c->sc, loc, ea, macros, c->stream); break;
+    }
+    if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "LBM step launch: %s", cudaGetErrorString(e));
+    c->cur ^= 1;
+    c->pops_local = false;
+    return EHD_OK;
+}
+
+int poisson(ehd_ctx *c) {
+    cudaError_t e = c->prec == EHD_PREC_FP64 ? launch_poisson<double>(c->pa, c->stream)
+                                             : launch_poisson<float>(c->pa, c->stream);
+    if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "Poisson launch: %s", cudaGetErrorString(e));
+    c->e_arrays = false;
+    return EHD_OK;
+}
+
+void drop_graphs(ehd_ctx *c) {
+    for (auto &row : c->graph)
+        for (auto &g : row)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+}
+
+// One steady-state step (pull, E from phi) as a CUDA graph, captured once per
+// (buffer parity, macro output) pair.
+int step_graph(ehd_ctx *c, bool macros) {
+    cudaGraphExec_t &ge = c->graph[c->cur][macros ? 1 : 0];
+    if (!ge) {
+        cudaGraph_t g = nullptr;
+        EHD_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const int cur0 = c->cur;
+        int r1 = lbm(c, macros);
+        int r2 = r1 == EHD_OK ? poisson(c) : r1;
+        c->cur = cur0;
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (r1 != EHD_OK || r2 != EHD_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            c->use_graphs = false;  // fall back to direct launches for good
+            return 1;
+        }
+        e = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            ge = nullptr;
+            cudaGetLastError();
+            c->use_graphs = false;
+            return 1;
+        }
+    }
+    EHD_CK(cudaGraphLaunch(ge, c->stream));
+    c->cur ^= 1;
+    return EHD_OK;
+}
+
+int after_upload(ehd_ctx *c) {
+    cudaError_t e = c->rsize == 8
+                        ? launch_plane_refs<double>(c->out[0], c->out[4], c->ref, c->zref, c->sc, c->stream)
+                        : launch_plane_refs<float>(c->out[0], c->out[4], c->ref, c->zref, c->sc, c->stream);
+    if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "plane references: %s", cudaGetErrorString(e));
+    switch (c->prec) {
+        case EHD_PREC_FP64: e = launch_init_equilibrium<double>(c->f[c->cur], c->h[c->cur], c->out, c->ref, c->sc, c->stream); break;
+        case EHD_PREC_FP32: e = launch_init_equilibrium<float>(c->f[c->cur], c->h[c->cur], c->out, c->ref, c->sc, c->stream); break;
+        case EHD_PREC_FP16: e = launch_init_equilibrium<__half>(c->f[c->cur], c->h[c->cur], c->out, c->ref, c->sc, c->stream); break;
+        default: e = launch_init_equilibrium<__nv_bfloat16>(c->f[c->cur], c->h[c->cur], c->out, c->ref, c->sc, c->stream); break;
+    }
+    if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "init_equilibrium: %s", cudaGetErrorString(e));
+    e = c->prec == EHD_PREC_FP64
+            ? launch_fields_to_compute<double>(c->out_dev, c->rho, c->u, c->v, c->w, c->q, c->sc.n, c->stream)
+            : launch_fields_to_compute<float>(c->out_dev, c->rho, c->u, c->v, c->w, c->q, c->sc.n, c->stream);
+    if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "fields_to_compute: %s", cudaGetErrorString(e));
+    EHD_CK(cudaStreamSynchronize(c->stream));
+    c->have_state = true;
+    c->pops_local = true;
+    c->e_arrays = true;
+    c->out_valid = true;
+    c->step = 0;
+    c->t = 0.0;
+    return EHD_OK;
+}
+
+int materialize(ehd_ctx *c) {
+    if (c->out_valid) return EHD_OK;
+    // phi and E stay as uploaded until the first Poisson solve
+    const int mask = c->e_arrays ? 1 : 3;
+    cudaError_t e =
+        c->prec == EHD_PREC_FP64
+            ? launch_materialize<double>(c->rho, c->u, c->v, c->w, c->q, c->phip, c->phi00, c->out, mask, c->sc, c->stream)
+            : launch_materialize<float>(c->rho, c->u, c->v, c->w, c->q, c->phip, c->phi00, c->out, mask, c->sc, c->stream);
+    if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "materialize: %s", cudaGetErrorString(e));
+    c->out_valid = true;
+    return EHD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ehd_abi_version(void) { return EHD_ABI_VERSION; }
+
+const char *ehd_last_error(void) { return g_err.c_str(); }
+
+int ehd_params_from_groups(ehd_params *p, double T, double M, double C, double Fe) {
+    if (!p) return fail(EHD_ERR_INVALID, "params is NULL");
+    if (!(T > 0) || !(M > 0) || !(C > 0) || !(Fe > 0))
+        return fail(EHD_ERR_INVALID, "T, M, C, Fe must be positive");
+    if (!(p->eps > 0) || !(p->rho0 > 0) || !(p->lz > 0) || p->voltage == 0.0)
+        return fail(EHD_ERR_INVALID, "eps, rho0, lz, voltage must be set");
+    // inverse of LBM.cu:1375-1378
+    p->K = std::sqrt(p->eps / p->rho0) / M;
+    p->nu = p->eps * p->voltage / (p->K * T * p->rho0);
+    p->charge0 = C * p->voltage * p->eps / (p->lz * p->lz);
+    p->diffu = p->K * p->voltage / Fe;
+    return EHD_OK;
+}
+
+int ehd_groups_from_params(const ehd_params *p, double *T, double *M, double *C, double *Fe) {
+    if (!p) return fail(EHD_ERR_INVALID, "params is NULL");
+    if (M) *M = std::sqrt(p->eps / p->rho0) / p->K;
+    if (T) *T = p->eps * p->voltage / p->K / p->nu / p->rho0;
+    if (C) *C = p->charge0 * p->lz * p->lz / (p->voltage * p->eps);
+    if (Fe) *Fe = p->K * p->voltage / p->diffu;
+    return EHD_OK;
+}
+
+int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out) {
+    if (!out) return fail(EHD_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    int r = validate(params);
+    if (r != EHD_OK) return r;
+    ehd_config cfg{};
+    if (config) cfg = *config;
+    if (cfg.precision < EHD_PREC_FP64 || cfg.precision > EHD_PREC_BF16)
+        return fail(EHD_ERR_INVALID, "unknown precision %d", cfg.precision);
+    int ndev = 0;
+    EHD_CK(cudaGetDeviceCount(&ndev));
+    if (cfg.device < 0 || cfg.device >= ndev)
+        return fail(EHD_ERR_INVALID, "device %d out of range (%d devices)", cfg.device, ndev);
+    DeviceGuard dg(cfg.device);
+    if (!dg.ok) return fail(EHD_ERR_CUDA, "cudaSetDevice(%d) failed", cfg.device);
+
+    ehd_ctx *c = new ehd_ctx();
+    c->p = *params;
+    c->cfg = cfg;
+    c->prec = cfg.precision;
+    c->device = cfg.device;
+    c->sc = make_const(params);
+    c->use_graphs = !(cfg.flags & EHD_FLAG_NO_GRAPH);
+    c->tsize = c->prec == EHD_PREC_FP64 ? 8 : (c->prec == EHD_PREC_FP32 ? 4 : 2);
+    c->rsize = c->prec == EHD_PREC_FP64 ? 8 : 4;
+    auto bail = [&](int code) {
+        ehd_destroy(c);
+        return code;
+    };
+    if (cfg.stream) {
+        c->stream = (cudaStream_t)cfg.stream;
+    } else {
+        cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete c;
+            return fail(EHD_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+        }
+        c->own_stream = true;
+    }
+    const size_t n = (size_t)c->sc.n;
+    const int nx = params->nx, ny = params->ny, nz = params->nz;
+    for (int i = 0; i < 2; ++i) {
+        if ((r = dalloc(c, &c->f[i], (size_t)Q * n * c->tsize))) return bail(r);
+        if ((r = dalloc(c, &c->h[i], (size_t)Q * n * c->tsize))) return bail(r);
+    }
+    void **macro[] = {&c->q, &c->rho, &c->u, &c->v, &c->w, &c->phip};
+    for (void **m : macro)
+        if ((r = dalloc(c, m, n * c->rsize))) return bail(r);
+    if ((r = dalloc(c, (void **)&c->phi00, sizeof(double) * nz))) return bail(r);
+    if ((r = dalloc(c, (void **)&c->ez00, sizeof(double) * nz))) return bail(r);
+    if ((r = dalloc(c, (void **)&c->ref, sizeof(double) * 2 * nz))) return bail(r);
+    if ((r = dalloc(c, &c->zref, c->rsize * 6 * nz))) return bail(r);
+    for (int i = 0; i < 9; ++i)
+        if ((r = dalloc(c, (void **)&c->out[i], sizeof(double) * n))) return bail(r);
+    if ((r = dalloc(c, (void **)&c->out_dev, sizeof(double *) * 9))) return bail(r);
+
+    // Poisson solver set-up: replaces cufftPlan3d and the wavenumber tables
+    // (main.cu:104-143)
+    PoissonArgs &pa = c->pa;
+    pa.nx = nx;
+    pa.ny = ny;
+    pa.nz = nz;
+    pa.nxh = nx / 2 + 1;
+    pa.pitch = (pa.nxh + 15) / 16 * 16;
+    const size_t c2 = 2 * c->rsize;  // complex compute type
+    {
+        int rows = 16;
+        while (rows > 1 && (size_t)2 * rows * nx * c2 > 64 * 1024) rows >>= 1;
+        pa.rows_per_block = rows;
+        int cols = (int)(128 / c2);
+        while (cols > 1 && (size_t)2 * cols * ny * c2 > 160 * 1024) cols >>= 1;
+        pa.cols_per_block = cols;
+        if ((size_t)2 * rows * nx * c2 > 200 * 1024 || (size_t)2 * cols * ny * c2 > 200 * 1024)
+            return bail(fail(EHD_ERR_INVALID, "nx or ny too large for the in-shared-memory FFT"));
+    }
+    pa.px = make_plan(nx);
+    pa.py = make_plan(ny);
+    const size_t nspec = (size_t)(nz - 2) * ny * pa.pitch;
+    if ((r = dalloc(c, &pa.spec, nspec * c2))) return bail(r);
+    if ((r = dalloc(c, (void **)&pa.specd, nspec * sizeof(double2)))) return bail(r);
+    if ((r = dalloc(c, (void **)&pa.rowsum, sizeof(double) * (size_t)(nz - 2) * ny))) return bail(r);
+    if ((r = dalloc(c, (void **)&pa.planesum, sizeof(double) * nz))) return bail(r);
+    void *twx = nullptr, *twy = nullptr;
+    if ((r = dalloc(c, &twx, (size_t)nx * c2))) return bail(r);
+    if ((r = dalloc(c, &twy, (size_t)ny * c2))) return bail(r);
+    double *kx2 = nullptr, *ky2 = nullptr;
+    if ((r = dalloc(c, (void **)&kx2, sizeof(double) * pa.nxh))) return bail(r);
+    if ((r = dalloc(c, (void **)&ky2, sizeof(double) * ny))) return bail(r);
+    pa.twx = twx;
+    pa.twy = twy;
+    pa.kx2 = kx2;
+    pa.ky2 = ky2;
+    pa.phi00 = c->phi00;
+    pa.ez00 = c->ez00;
+    pa.q = c->q;
+    pa.phip = c->phip;
+    pa.eps = params->eps;
+    pa.voltage = params->voltage;
+    pa.dz = params->dz;
+    {
+        auto table = [&](int N, void *dst) -> cudaError_t {
+            std::vector<double> t(2 * (size_t)N);
+            for (int k = 0; k < N; ++k) {
+                const double a = -2.0 * M_PI * (double)k / (double)N;
+                t[2 * k] = std::cos(a);
+                t[2 * k + 1] = std::sin(a);
+            }
+            if (c->rsize == 8)
+                return cudaMemcpy(dst, t.data(), sizeof(double) * 2 * N, cudaMemcpyHostToDevice);
+            std::vector<float> tf(t.begin(), t.end());
+            return cudaMemcpy(dst, tf.data(), sizeof(float) * 2 * N, cudaMemcpyHostToDevice);
+        };
+        EHD_CK(table(nx, twx));
+        EHD_CK(table(ny, twy));
+        std::vector<double> hx(pa.nxh), hy(ny);
+        for (int i = 0; i < pa.nxh; ++i) {  // main.cu:110-113
+            const double k = (double)i * 2.0 * M_PI / params->lx;
+            hx[i] = k * k;
+        }
+        for (int j = 0; j < ny; ++j) {  // main.cu:119-127
+            const double k = (j <= ny / 2 ? (double)j : (double)j - ny) * 2.0 * M_PI / params->ly;
+            hy[j] = k * k;
+        }
+        EHD_CK(cudaMemcpy(kx2, hx.data(), sizeof(double) * pa.nxh, cudaMemcpyHostToDevice));
+        EHD_CK(cudaMemcpy(ky2, hy.data(), sizeof(double) * ny, cudaMemcpyHostToDevice));
+    }
+    EHD_CK(cudaMemcpy(c->out_dev, c->out, sizeof(double *) * 9, cudaMemcpyHostToDevice));
+    EHD_CK(cudaMemset(c->phip, 0, n * c->rsize));
+    EHD_CK(cudaMemset(c->phi00, 0, sizeof(double) * nz));
+    EHD_CK(cudaMemset(c->ez00, 0, sizeof(double) * nz));
+    // diagnostics scratch
+    c->diag_blocks = (int)std::min<long long>(1024, (c->sc.n + 2047) / 2048);
+    if (c->diag_blocks < 1) c->diag_blocks = 1;
+    if ((r = dalloc(c, (void **)&c->diag_partial, sizeof(double) * 5 * c->diag_blocks))) return bail(r);
+    if ((r = dalloc(c, (void **)&c->diag_result, sizeof(double) * 8))) return bail(r);
+    {
+        cudaError_t e = cudaMallocHost((void **)&c->host_diag, sizeof(double) * 8);
+        if (e != cudaSuccess) return bail(fail(EHD_ERR_NOMEM, "cudaMallocHost failed"));
+    }
+    *out = c;
+    return EHD_OK;
+}
+
+int ehd_destroy(ehd_ctx *c) {
+    if (!c) return EHD_OK;
+    DeviceGuard dg(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
+    for (void *p : c->allocs) cudaFree(p);
+    if (c->host_diag) cudaFreeHost(c->host_diag);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return EHD_OK;
+}
+
+int ehd_device_bytes(const ehd_ctx *c, size_t *bytes) {
+    if (!c || !bytes) return fail(EHD_ERR_INVALID, "NULL argument");
+    *bytes = c->bytes;
+    return EHD_OK;
+}
+
+int ehd_set_fields(ehd_ctx *c, const double *rho, const double *u, const double *v,
+                   const double *w, const double *q, const double *phi, const double *ex,
+                   const double *ey, const double *ez) {
+    if (!c) return fail(EHD_ERR_INVALID, "ctx is NULL");
+    const double *in[9] = {rho, u, v, w, q, phi, ex, ey, ez};
+    for (int i = 0; i < 9; ++i)
+        if (!in[i]) return fail(EHD_ERR_INVALID, "field %d is NULL", i);
+    DeviceGuard dg(c->device);
+    const size_t b = sizeof(double) * (size_t)c->sc.n;
+    for (int i = 0; i < 9; ++i)
+        EHD_CK(cudaMemcpyAsync(c->out[i], in[i], b, cudaMemcpyHostToDevice, c->stream));
+    return after_upload(c);
+}
+
+int ehd_initialize(ehd_ctx *c) {
+    if (!c) return fail(EHD_ERR_INVALID, "ctx is NULL");
+    DeviceGuard dg(c->device);
+    cudaError_t e = launch_reference_init(c->out_dev, c->sc, c->p.voltage, c->p.lz, c->p.dz,
+                                          c->stream);
+    if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "initialization: %s", cudaGetErrorString(e));
+    return after_upload(c);
+}
+
+int ehd_get_fields(ehd_ctx *c, double *rho, double *u, double *v, double *w, double *q,
+                   double *phi, double *ex, double *ey, double *ez) {
+    if (!c) return fail(EHD_ERR_INVALID, "ctx is NULL");
+    if (!c->have_state) return fail(EHD_ERR_STATE, "no state: call ehd_set_fields first");
+    DeviceGuard dg(c->device);
+    double *dst[9] = {rho, u, v, w, q, phi, ex, ey, ez};
+    int r = materialize(c);
+    if (r != EHD_OK) return r;
+    const size_t b = sizeof(double) * (size_t)c->sc.n;
+    for (int i = 0; i < 9; ++i)
+        if (dst[i]) EHD_CK(cudaMemcpyAsync(dst[i], c->out[i], b, cudaMemcpyDeviceToHost, c->stream));
+    EHD_CK(cudaStreamSynchronize(c->stream));
+    return EHD_OK;
+}
+
+int ehd_step(ehd_ctx *c, int nsteps) {
+    if (!c) return fail(EHD_ERR_INVALID, "ctx is NULL");
+    if (nsteps < 0) return fail(EHD_ERR_INVALID, "nsteps < 0");
+    if (!c->have_state) return fail(EHD_ERR_STATE, "no state: call ehd_set_fields first");
+    DeviceGuard dg(c->device);
+    for (int i = 0; i < nsteps; ++i) {
+        const bool macros = (i == nsteps - 1);
+        int r;
+        if (c->pops_local || c->e_arrays || !c->use_graphs) {
+            if ((r = lbm(c, macros)) != EHD_OK) return r;
+            if ((r = poisson(c)) != EHD_OK) return r;
+        } else {
+            r = step_graph(c, macros);
+            if (r == 1) {  // capture unavailable: direct launches
+                if ((r = lbm(c, macros)) != EHD_OK) return r;
+                if ((r = poisson(c)) != EHD_OK) return r;
+            } else if (r != EHD_OK) {
+                return r;
+            }
+        }
+        c->step += 1;
+        c->t += c->p.dt;
+    }
+    if (nsteps > 0) c->out_valid = false;
+    return EHD_OK;
+}
+
+int ehd_stream_collide_save(ehd_ctx *c) {
+    if (!c) return fail(EHD_ERR_INVALID, "ctx is NULL");
+    if (!c->have_state) return fail(EHD_ERR_STATE, "no state: call ehd_set_fields first");
+    DeviceGuard dg(c->device);
+    int r = lbm(c, true);
+    if (r != EHD_OK) return r;
+    c->out_valid = false;
+    return EHD_OK;
+}
+
+int ehd_poisson(ehd_ctx *c) {
+    if (!c) return fail(EHD_ERR_INVALID, "ctx is NULL");
+    if (!c->have_state) return fail(EHD_ERR_STATE, "no state: call ehd_set_fields first");
+    DeviceGuard dg(c->device);
+    int r = poisson(c);
+    if (r != EHD_OK) return r;
+    c->out_valid = false;
+    return EHD_OK;
+}
+
+int ehd_synchronize(ehd_ctx *c) {
+    if (!c) return fail(EHD_ERR_INVALID, "ctx is NULL");
+    DeviceGuard dg(c->device);
+    EHD_CK(cudaStreamSynchronize(c->stream));
+    return EHD_OK;
+}
+
+int ehd_set_reference_current(ehd_ctx *c, double i0) {
+    if (!c) return fail(EHD_ERR_INVALID, "ctx is NULL");
+    if (!std::isfinite(i0)) return fail(EHD_ERR_INVALID, "i0 not finite");
+    c->i0 = i0;
+    return EHD_OK;
+}
+
+int ehd_diagnostics(ehd_ctx *c, ehd_diag *o) {
+    if (!c || !o) return fail(EHD_ERR_INVALID, "NULL argument");
+    if (!c->have_state) return fail(EHD_ERR_STATE, "no state: call ehd_set_fields first");
+    DeviceGuard dg(c->device);
+    DiagArgs a{};
+    a.nx = c->p.nx;
+    a.ny = c->p.ny;
+    a.nz = c->p.nz;
+    a.rho = c->rho;
+    a.u = c->u;
+    a.v = c->v;
+    a.w = c->w;
+    a.q = c->q;
+    a.phip = c->phip;
+    a.ez00 = c->ez00;
+    a.ez = c->e_arrays ? c->out[8] : nullptr;
+    a.inv2dz = c->sc.inv2dz;
+    a.partial = c->diag_partial;
+    a.result = c->diag_result;
+    a.nblocks = c->diag_blocks;
+    cudaError_t e = c->rsize == 8 ? launch_diag<double>(a, c->stream) : launch_diag<float>(a, c->stream);
+    if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "diagnostics: %s", cudaGetErrorString(e));
+    EHD_CK(cudaMemcpyAsync(c->host_diag, c->diag_result, sizeof(double) * 5,
+                           cudaMemcpyDeviceToHost, c->stream));
+    EHD_CK(cudaStreamSynchronize(c->stream));
+    const double *r = c->host_diag;
+    const double dv = c->p.dx * c->p.dy * c->p.dz;
+    std::memset(o, 0, sizeof(*o));
+    o->current = r[0] * c->p.K * c->p.dy * c->p.dy;  // LBM.cu:1669
+    o->nu_e = c->i0 != 0.0 ? o->current / c->i0 : 0.0;
+    o->kinetic_energy = 0.5 * r[1] * dv;
+    o->total_charge = r[2] * dv;
+    o->umax = r[3];
+    o->time = c->t;
+    o->step = c->step;
+    o->nonfinite = r[4] > 0.0 ? 1 : 0;
+    return EHD_OK;
+}
+
+int ehd_current(ehd_ctx *c, double *current) {
+    if (!current) return fail(EHD_ERR_INVALID, "NULL argument");
+    ehd_diag d;
+    int r = ehd_diagnostics(c, &d);
+    if (r != EHD_OK) return r;
+    *current = d.current;
+    return EHD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,94 @@
+// common.cuh -- lattice tables, per-step constants and storage conversions
+// shared by the step kernels.
+//
+// D3Q27 in the reference's numbering: population d at node x is pulled from
+// x - e_d (gpu_stream, LBM.cu:1225-1250); opposite pairs are (2k-1, 2k);
+// weights 8/27, 2/27, 1/54, 1/216 (LBM.h:73-76).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ehd {
+
+constexpr int Q = 27;
+
+__host__ __device__ constexpr int ex_of(int d) {
+    constexpr int t[Q] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1,
+                          1, -1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1};
+    return t[d];
+}
+__host__ __device__ constexpr int ey_of(int d) {
+    constexpr int t[Q] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1,
+                          0, 0, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1};
+    return t[d];
+}
+__host__ __device__ constexpr int ez_of(int d) {
+    constexpr int t[Q] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0,
+                          -1, 1, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1};
+    return t[d];
+}
+__host__ __device__ constexpr int opp_of(int d) { return d == 0 ? 0 : ((d & 1) ? d + 1 : d - 1); }
+__host__ __device__ constexpr double w_of(int d) {
+    return d == 0 ? 8.0 / 27.0 : (d <= 6 ? 2.0 / 27.0 : (d <= 18 ? 1.0 / 54.0 : 1.0 / 216.0));
+}
+// sign of the moving upper wall term (LBM.cu:1145-1170); direction 3 gets +,
+// direction 4 nothing, as the reference writes it.
+__host__ __device__ constexpr int mw_sign_of(int d) {
+    constexpr int t[Q] = {0, 1, -1, 1, 0, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1,
+                          1, -1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1};
+    return t[d];
+}
+
+// Everything a step kernel needs, derived once on the host in FP64 from
+// ehd_params (formulas of LBM.cu:297-302, 688, 1017-1018, 1137-1139).
+struct StepConst {
+    int nx, ny, nz;
+    int pad_;
+    long long nxy, n;         // nodes per plane, nodes
+    double dt, cfl, cs2;
+    double cflinv, cflinv2;   // 1/CFL, 1/(CFL^2 cs^2)
+    double tw0rp, tw0rm;      // omega_+ dt, omega_- dt for f
+    double tw0cp, tw0cm;      // omega_c+ dt, omega_c- dt for g
+    // The same four rates split as rate = hi - lo, applied as hi*X - lo*X:
+    // hi = 2, lo = 2 - rate for an over-relaxed rate (rate >= 1), so that the
+    // small complement 2 - rate, which sets the transport coefficient
+    // (1/rate - 1/2), keeps full relative precision in FP32; hi = rate, lo = 0
+    // otherwise.  Order: rp, rm, cp, cm.
+    double rate_hi[4], rate_lo[4];
+    double sp, sm;            // 1 - dt omega_+/2, 1 - dt omega_-/2
+    double rho0, q0, K, exf;
+    double inv2dx, inv2dy, inv2dz;  // 0.5/dx, 0.5/dy, 0.5/dz
+    double mw[Q];             // moving-wall increment per direction at z=nz-1
+};
+
+// ---- storage types ---------------------------------------------------------
+template <typename T> struct Store;
+template <> struct Store<double> {
+    __device__ __forceinline__ static double ld(const double *p) { return __ldg(p); }
+    __device__ __forceinline__ static void st(double *p, double v) { *p = v; }
+};
+template <> struct Store<float> {
+    __device__ __forceinline__ static float ld(const float *p) { return __ldg(p); }
+    __device__ __forceinline__ static void st(float *p, float v) { *p = v; }
+};
+template <> struct Store<__half> {
+    __device__ __forceinline__ static float ld(const __half *p) { return __half2float(__ldg(p)); }
+    __device__ __forceinline__ static void st(__half *p, float v) { *p = __float2half_rn(v); }
+};
+template <> struct Store<__nv_bfloat16> {
+    __device__ __forceinline__ static float ld(const __nv_bfloat16 *p) {
+        return __bfloat162float(__ldg(p));
+    }
+    __device__ __forceinline__ static void st(__nv_bfloat16 *p, float v) {
+        *p = __float2bfloat16_rn(v);
+    }
+};
+
+template <typename R> struct Cplx;
+template <> struct Cplx<float> { using T = float2; };
+template <> struct Cplx<double> { using T = double2; };
+
+}  // namespace ehd

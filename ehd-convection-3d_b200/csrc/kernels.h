@@ -1,0 +1,98 @@
+// kernels.h -- launchers of the step kernels, called by the C ABI layer.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace ehd {
+
+struct LbmArgs {
+    const void *fa, *ha;  // populations read this step (pulled)
+    void *fb, *hb;        // populations written this step
+    const void *phip;     // phi' (compute type), zero on both electrodes
+    const double *ez00;   // per-plane Ez of the mean potential phi00
+    const double *exa, *eya, *eza;  // explicit E (first step after set_fields)
+    void *q, *rho, *u, *v, *w;      // macroscopic outputs (compute type)
+    const void *zref;               // per-plane reference table, 6 per plane (compute type)
+};
+
+template <typename T, typename R>
+cudaError_t launch_lbm_step(const LbmArgs &a, const StepConst &c, int local_pops, int e_arrays,
+                            bool macros, cudaStream_t s);
+
+// ref: per-plane {rho_ref, q_ref} in FP64
+template <typename T>
+cudaError_t launch_init_equilibrium(void *f, void *h, const double *const fields[9],
+                                    const double *ref, const StepConst &c, cudaStream_t s);
+
+template <typename R>
+cudaError_t launch_materialize(const void *rho, const void *u, const void *v, const void *w,
+                               const void *q, const void *phip, const double *phi00,
+                               double *const out[9], int macros, const StepConst &c,
+                               cudaStream_t s);
+
+// out_dev: device array of the 9 FP64 field pointers
+cudaError_t launch_reference_init(double *const *out_dev, const StepConst &c, double voltage,
+                                  double lz, double dz, cudaStream_t s);
+template <typename R>
+cudaError_t launch_fields_to_compute(double *const *out_dev, void *rho, void *u, void *v,
+                                     void *w, void *q, long long n, cudaStream_t s);
+
+// Per-plane means of rho and q (ref, FP64, 2 per plane) and the step's
+// reference table (zref, compute type, 6 per plane).
+template <typename R>
+cudaError_t launch_plane_refs(const double *rho, const double *q, double *ref, void *zref,
+                              const StepConst &c, cudaStream_t s);
+
+// ---- Poisson solve ---------------------------------------------------------
+
+constexpr int kMaxRadix = 24;
+struct FftPlan {
+    int n;
+    int nrad;
+    int rad[kMaxRadix];
+};
+
+// Buffers and sizes of the FFT / tridiagonal Poisson solve.  spec holds the
+// x,y spectrum of the planes z = 1..NZ-2 in the compute type, specd the same
+// in FP64 for the z solve.  Layout [z-1][ky][kx], kx pitch `pitch`.
+struct PoissonArgs {
+    int nx, ny, nz, nxh, pitch;
+    int rows_per_block;  // x-row FFT batch per block
+    int cols_per_block;  // y-column FFT batch per block
+    FftPlan px, py;
+    const void *twx, *twy;   // exp(-2 pi i k/N) tables in the compute type
+    const double *kx2, *ky2; // squared wavenumbers (main.cu:110-129)
+    void *spec;              // complex compute type
+    double2 *specd;          // complex FP64
+    double *rowsum;          // [z-1][y] FP64 sums of the source
+    double *planesum;        // [z] FP64 sums of the source
+    double *phi00, *ez00;    // [z] mean potential and its Ez
+    const void *q;           // charge (compute type)
+    void *phip;              // output phi' (compute type)
+    double eps, voltage, dz;
+};
+
+template <typename R>
+cudaError_t launch_poisson(const PoissonArgs &a, cudaStream_t s);
+
+size_t poisson_zsolve_smem(int nz, int threads);
+
+// ---- diagnostics ---------------------------------------------------------
+
+struct DiagArgs {
+    int nx, ny, nz;
+    const void *rho, *u, *v, *w, *q;  // type R (R = double for the FP64 field arrays)
+    const void *phip;                 // phi' (type R) when ez == nullptr
+    const double *ez00;               // mean-field Ez per plane when ez == nullptr
+    const double *ez;                 // explicit FP64 Ez field, or nullptr
+    double inv2dz;
+    double *partial;                  // scratch: nblocks x 5 doubles
+    double *result;                   // 5 doubles
+    int nblocks;
+};
+template <typename R>
+cudaError_t launch_diag(const DiagArgs &a, cudaStream_t s);
+
+}  // namespace ehd

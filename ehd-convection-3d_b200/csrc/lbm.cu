@@ -1,0 +1,603 @@
+// lbm.cu -- the fused D3Q27 TRT stream-collide for the flow populations f and
+// the charge populations g, with the electrode and injection rules, in one
+// pass per time step.
+//
+// The reference runs four kernels per step (stream_collide_save,
+// LBM.cu:278-293): collide (LBM.cu:295-1091), wall bounce-back
+// (LBM.cu:1093-1203), pull streaming periodic in x, y and z (LBM.cu:1205-1279)
+// and injection anti-bounce-back (LBM.cu:1281-1353).  Here the populations are
+// kept in the post-collision, post-wall-rule state P; one kernel pulls P from
+// the neighbours (the reference's stream), applies the injection rule while
+// loading (the reference's bc_charge), collides, applies the wall rules while
+// storing (the reference's boundary), and writes the new P into the other
+// buffer.  Each population set is read once and written once per step.
+//
+// Storage: SoA, pop[d][z][y][x] with d = 0..26 in one array (d = 0 is the rest
+// population).  Flow populations are stored as deviations f_d - w_d rho0; the
+// charge populations as they are.  Where the reference's boundary kernel
+// replaces a value with another node's or another direction's, the same value
+// is written here by the thread that owns it:
+//   z = 0      f: P_d = f_opp(d) pulled this step, rest f unchanged
+//                 (LBM.cu:1103-1131 with f0bc, LBM.cu:309)
+//              g: pulled as -P_opp(d)(own node) + 2 q0 w_d (LBM.cu:1320-1348);
+//                 rest g stored already as -g0' + 2 q0 w0
+//   z = NZ-1   f: P_d = f_opp(d) + moving-wall term (LBM.cu:1143-1170)
+//              g: P = post-collision g of z = NZ-2 (LBM.cu:1173-1200), written
+//                 by the z = NZ-2 thread
+//   z = 0 velocity: minus the z = 1 velocity built from z = 1 pre-collision
+//                 populations, z = 1 charge and E, and the LOCAL 1/rho
+//                 (LBM.cu:417-492).  The reference reads z = 1's rest
+//                 populations while z = 1 threads overwrite them; here the
+//                 rest populations are double-buffered, so the z = 0 node
+//                 always sees the pre-collision value.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace ehd {
+
+namespace {
+
+template <typename R>
+struct PullIdx {
+    long long row[3][3];  // [dy+1][dz+1] -> NX*(ys + NY*zs) for source (y - dy, z - dz)
+    int xs[3];            // [dx+1] -> source x - dx
+};
+
+template <typename R>
+__device__ __forceinline__ void make_pull(PullIdx<R> &P, int x, int y, int z, int NX, int NY,
+                                          int NZ) {
+    const int xm = x == 0 ? NX - 1 : x - 1, xp = x == NX - 1 ? 0 : x + 1;
+    const int ym = y == 0 ? NY - 1 : y - 1, yp = y == NY - 1 ? 0 : y + 1;
+    const int zm = z == 0 ? NZ - 1 : z - 1, zp = z == NZ - 1 ? 0 : z + 1;
+    P.xs[0] = xp;  // e_x = -1: source x + 1
+    P.xs[1] = x;
+    P.xs[2] = xm;  // e_x = +1: source x - 1
+    const int ys[3] = {yp, y, ym};
+    const int zs[3] = {zp, z, zm};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+            P.row[a][b] = (long long)NX * ((long long)ys[a] + (long long)NY * zs[b]);
+}
+
+template <typename R>
+__device__ __forceinline__ long long pull_src(const PullIdx<R> &P, int d) {
+    return P.row[ey_of(d) + 1][ez_of(d) + 1] + P.xs[ex_of(d) + 1];
+}
+
+// Per-plane reference state.  Populations are stored as deviations from
+// w_d rho_ref(z) and w_d q_ref(z) of the plane z they are stored in; a
+// population pulled from plane z - e_z is moved to this plane's reference by
+// adding w_d (rho_ref(z - e_z) - rho_ref(z)).  Table layout per plane:
+// {rho_ref, q_ref, rho_ref(z-1)-rho_ref(z), rho_ref(z+1)-rho_ref(z),
+//  q_ref(z-1)-q_ref(z), q_ref(z+1)-q_ref(z)}, z +- 1 periodic.
+template <typename R>
+struct ZRef {
+    R rref, qref, dr_m, dr_p, dq_m, dq_p;
+    // offset for a population with z-velocity e (source plane z - e)
+    __device__ __forceinline__ R dr(int e) const { return e > 0 ? dr_m : (e < 0 ? dr_p : (R)0); }
+    __device__ __forceinline__ R dq(int e) const { return e > 0 ? dq_m : (e < 0 ? dq_p : (R)0); }
+};
+
+// rate * x with rate = hi - lo (see StepConst::rate_hi)
+template <typename R>
+__device__ __forceinline__ R relax(R hi, R lo, R x) {
+    return hi * x - lo * x;
+}
+
+template <typename R>
+__device__ __forceinline__ ZRef<R> load_zref(const R *__restrict__ t, int z) {
+    const R *p = t + 6 * z;
+    return ZRef<R>{__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3), __ldg(p + 4), __ldg(p + 5)};
+}
+
+}  // namespace
+
+// GENERAL = false: the steady-state step (pull, E from phi).  GENERAL = true
+// adds two run-time switches used right after ehd_set_fields:
+//   local_pops: the buffers hold the pre-collision populations of each node
+//               (the reference's f1/h1 after init_equilibrium), so they are
+//               read in place, without pull or injection rule;
+//   e_arrays:   E comes from the uploaded FP64 arrays instead of phi.
+template <typename T, typename R, bool GENERAL, bool MACROS>
+__global__ void __launch_bounds__(128)
+lbm_step_kernel(const T *__restrict__ fa, T *__restrict__ fb, const T *__restrict__ ha,
+                T *__restrict__ hb, const R *__restrict__ phip, const double *__restrict__ ez00,
+                const double *__restrict__ exa, const double *__restrict__ eya,
+                const double *__restrict__ eza, R *__restrict__ qout, R *__restrict__ rout,
+                R *__restrict__ uout, R *__restrict__ vout, R *__restrict__ wout,
+                const R *__restrict__ zref, StepConst c, int local_pops, int e_arrays) {
+    const bool LOCAL = GENERAL && local_pops;
+    const bool EARR = GENERAL && e_arrays;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= c.nx || y >= c.ny) return;
+    const int NX = c.nx, NY = c.ny, NZ = c.nz;
+    const long long N = c.n;
+    const long long node = (long long)x + (long long)NX * ((long long)y + (long long)NY * z);
+
+    const R q0 = (R)c.q0;
+    // per-plane reference state (rho_ref, q_ref) and the offsets that carry a
+    // population stored relative to its own plane over to this plane
+    const ZRef<R> zr = load_zref(zref, z);
+
+    PullIdx<R> P;
+    make_pull(P, x, y, z, NX, NY, NZ);
+
+    // ---- pull (the reference's stream + injection rule), as deviations
+    // ft_d = f_d - w_d rho_ref(z), ht_d = g_d - w_d q_ref(z) ----
+    R f[Q], h[Q];
+#pragma unroll
+    for (int d = 0; d < Q; ++d) {
+        f[d] = Store<T>::ld(fa + d * N + (LOCAL ? node : pull_src(P, d)));
+        if (!LOCAL) f[d] += (R)w_of(d) * zr.dr(ez_of(d));
+    }
+    if (LOCAL) {
+#pragma unroll
+        for (int d = 0; d < Q; ++d) h[d] = Store<T>::ld(ha + d * N + node);
+    } else if (z == 0) {
+        // g_d = -g_opp(d) + 2 q0 w_d (LBM.cu:1320-1348), on deviations
+        h[0] = Store<T>::ld(ha + node);
+        const R inj = (R)2 * (q0 - zr.qref);
+#pragma unroll
+        for (int d = 1; d < Q; ++d)
+            h[d] = -Store<T>::ld(ha + opp_of(d) * N + node) + inj * (R)w_of(d);
+    } else {
+#pragma unroll
+        for (int d = 0; d < Q; ++d)
+            h[d] = Store<T>::ld(ha + d * N + pull_src(P, d)) + (R)w_of(d) * zr.dq(ez_of(d));
+    }
+
+    // ---- moments ----
+    R drho = 0, dq = 0, mx = 0, my = 0, mz = 0;
+#pragma unroll
+    for (int d = 0; d < Q; ++d) {
+        drho += f[d];
+        dq += h[d];
+        if (ex_of(d)) mx += ex_of(d) > 0 ? f[d] : -f[d];
+        if (ey_of(d)) my += ey_of(d) > 0 ? f[d] : -f[d];
+        if (ez_of(d)) mz += ez_of(d) > 0 ? f[d] : -f[d];
+    }
+    const R rho = zr.rref + drho;
+    const R charge = zr.qref + dq;
+
+    // ---- E at this node (and at z = 1 for the injector override) ----
+    R Ex, Ey, Ez;
+    const long long row = (long long)NX * ((long long)y + (long long)NY * z);
+    const int xm = x == 0 ? NX - 1 : x - 1, xp = x == NX - 1 ? 0 : x + 1;
+    const int ym = y == 0 ? NY - 1 : y - 1, yp = y == NY - 1 ? 0 : y + 1;
+    if (!EARR) {
+        // E = -grad(phi), central differences (gpu_efield, poisson.cu:44-60);
+        // phi = phi00(z) + phi'(x,y,z) with phi' = 0 on both electrodes, and
+        // Ez on the electrodes copied from the planes inside (gpu_bc,
+        // poisson.cu:61-73).
+        Ex = (__ldg(phip + row + xm) - __ldg(phip + row + xp)) * (R)c.inv2dx;
+        Ey = (__ldg(phip + (long long)NX * ((long long)ym + (long long)NY * z) + x) -
+              __ldg(phip + (long long)NX * ((long long)yp + (long long)NY * z) + x)) *
+             (R)c.inv2dy;
+        const int zc = z < 1 ? 1 : (z > NZ - 2 ? NZ - 2 : z);
+        Ez = (R)__ldg(ez00 + zc) +
+             (__ldg(phip + (long long)NX * ((long long)y + (long long)NY * (zc - 1)) + x) -
+              __ldg(phip + (long long)NX * ((long long)y + (long long)NY * (zc + 1)) + x)) *
+                 (R)c.inv2dz;
+    } else {
+        Ex = (R)__ldg(exa + node);
+        Ey = (R)__ldg(eya + node);
+        Ez = (R)__ldg(eza + node);
+    }
+
+    const R dt = (R)c.dt, cfl = (R)c.cfl;
+    const R fx = charge * Ex + (R)c.exf, fy = charge * Ey, fz = charge * Ez;
+    const R rhoinv = (R)1 / rho;
+    R ux = rhoinv * (mx / cfl + fx * dt * (R)0.5);
+    R uy = rhoinv * (my / cfl + fy * dt * (R)0.5);
+    R uz = rhoinv * (mz / cfl + fz * dt * (R)0.5);
+
+    if (z == 0) {
+        // LBM.cu:417-492
+        const ZRef<R> z1 = load_zref(zref, 1);
+        PullIdx<R> P1;
+        make_pull(P1, x, y, 1, NX, NY, NZ);
+        const long long node1 = node + c.nxy;
+        R dqm = Store<T>::ld(ha + node1);
+        R mxm = 0, mym = 0, mzm = 0;
+#pragma unroll
+        for (int d = 1; d < Q; ++d) {
+            const long long s1 = LOCAL ? node1 : pull_src(P1, d);
+            R fm = Store<T>::ld(fa + d * N + s1);
+            R hm = Store<T>::ld(ha + d * N + s1);
+            if (!LOCAL) {
+                fm += (R)w_of(d) * z1.dr(ez_of(d));
+                hm += (R)w_of(d) * z1.dq(ez_of(d));
+            }
+            dqm += hm;
+            if (ex_of(d)) mxm += ex_of(d) > 0 ? fm : -fm;
+            if (ey_of(d)) mym += ey_of(d) > 0 ? fm : -fm;
+            if (ez_of(d)) mzm += ez_of(d) > 0 ? fm : -fm;
+        }
+        const R chargem = z1.qref + dqm;
+        R Exm, Eym, Ezm;
+        if (!EARR) {
+            const long long row1 = row + c.nxy;
+            Exm = (__ldg(phip + row1 + xm) - __ldg(phip + row1 + xp)) * (R)c.inv2dx;
+            Eym = (__ldg(phip + (long long)NX * ((long long)ym + (long long)NY) + x) -
+                   __ldg(phip + (long long)NX * ((long long)yp + (long long)NY) + x)) *
+                  (R)c.inv2dy;
+            Ezm = (R)__ldg(ez00 + 1) +
+                  (__ldg(phip + (long long)NX * (long long)y + x) -
+                   __ldg(phip + (long long)NX * ((long long)y + 2LL * NY) + x)) *
+                      (R)c.inv2dz;
+        } else {
+            Exm = (R)__ldg(exa + node1);
+            Eym = (R)__ldg(eya + node1);
+            Ezm = (R)__ldg(eza + node1);
+        }
+        const R fxm = chargem * Exm + (R)c.exf, fym = chargem * Eym, fzm = chargem * Ezm;
+        ux = -rhoinv * (mxm / cfl + fxm * dt * (R)0.5);
+        uy = -rhoinv * (mym / cfl + fym * dt * (R)0.5);
+        uz = -rhoinv * (mzm / cfl + fzm * dt * (R)0.5);
+    }
+
+    qout[node] = charge;
+    if (MACROS) {
+        rout[node] = rho;
+        uout[node] = ux;
+        vout[node] = uy;
+        wout[node] = uz;
+    }
+
+    const R inv_cs2 = (R)(1.0 / c.cs2);
+    const R inv_cs2cfl = (R)(1.0 / (c.cs2 * c.cfl));
+
+    // ---- f: collide (interior) or wall rule; TRT on deviations:
+    // feq+ - w rho_ref = w drho + w rho (cu^2/2 - |u|^2/(2 cs^2)),
+    // feq- = w rho cu (LBM.cu:519-660, 704-1089) ----
+    if (z == 0 || z == NZ - 1) {
+        Store<T>::st(fb + node, f[0]);
+#pragma unroll
+        for (int d = 1; d < Q; ++d) {
+            R v = f[opp_of(d)];
+            if (z == NZ - 1 && mw_sign_of(d) != 0) v += (R)c.mw[d];
+            Store<T>::st(fb + d * N + node, v);
+        }
+    } else {
+        const R rp_hi = (R)c.rate_hi[0], rp_lo = (R)c.rate_lo[0];
+        const R rm_hi = (R)c.rate_hi[1], rm_lo = (R)c.rate_lo[1];
+        const R sp = (R)c.sp, sm = (R)c.sm;
+        const R cflinv = (R)c.cflinv, cflinv2 = (R)c.cflinv2;
+        const R usq = (R)0.5 * (ux * ux + uy * uy + uz * uz) * inv_cs2;
+        const R tux = ux * inv_cs2cfl, tuy = uy * inv_cs2cfl, tuz = uz * inv_cs2cfl;
+        const R uF = ux * fx + uy * fy + uz * fz;
+        {
+            const R fe0 = (R)w_of(0) * (drho - rho * usq);
+            const R fpop0 = -((R)w_of(0) * inv_cs2) * uF;
+            Store<T>::st(fb + node, f[0] - relax(rp_hi, rp_lo, f[0] - fe0) + dt * sp * fpop0);
+        }
+#pragma unroll
+        for (int d = 1; d < Q; d += 2) {
+            const int o = d + 1;
+            const R wd = (R)w_of(d);
+            const R cu = (R)ex_of(d) * tux + (R)ey_of(d) * tuy + (R)ez_of(d) * tuz;
+            const R eu = (R)ex_of(d) * ux + (R)ey_of(d) * uy + (R)ez_of(d) * uz;
+            const R eF = (R)ex_of(d) * fx + (R)ey_of(d) * fy + (R)ez_of(d) * fz;
+            const R fep = wd * (drho + rho * ((R)0.5 * cu * cu - usq));
+            const R fem = wd * rho * cu;
+            const R fp = (R)0.5 * (f[d] + f[o]);
+            const R fm = (R)0.5 * (f[d] - f[o]);
+            const R frp = (wd * inv_cs2) * (-uF + cflinv2 * eu * eF);
+            const R frm = (wd * inv_cs2) * (cflinv * eF);
+            const R relp = relax(rp_hi, rp_lo, fp - fep);
+            const R relm = relax(rm_hi, rm_lo, fm - fem);
+            Store<T>::st(fb + d * N + node, f[d] - (relp + relm) + dt * (sp * frp + sm * frm));
+            Store<T>::st(fb + o * N + node, f[o] - (relp - relm) + dt * (sp * frp - sm * frm));
+        }
+    }
+
+    // ---- g: collide (z <= NZ-2); the NZ-1 plane is written by z = NZ-2,
+    // relative to q_ref(NZ-1) ----
+    if (z != NZ - 1) {
+        const R cp_hi = (R)c.rate_hi[2], cp_lo = (R)c.rate_lo[2];
+        const R cm_hi = (R)c.rate_hi[3], cm_lo = (R)c.rate_lo[3];
+        const R K = (R)c.K;
+        const R ucx = ux + K * Ex, ucy = uy + K * Ey, ucz = uz + K * Ez;
+        const R usq = (R)0.5 * (ucx * ucx + ucy * ucy + ucz * ucz) * inv_cs2;
+        const R tux = ucx * inv_cs2cfl, tuy = ucy * inv_cs2cfl, tuz = ucz * inv_cs2cfl;
+        const bool dup = (z == NZ - 2);
+        const long long nodeup = node + c.nxy;
+        const R up = -zr.dq(-1);  // q_ref(z) - q_ref(z+1)
+        {
+            const R he0 = (R)w_of(0) * (dq - charge * usq);
+            const R out = h[0] - relax(cp_hi, cp_lo, h[0] - he0);
+            Store<T>::st(hb + node,
+                         z == 0 ? -out + (R)2 * (q0 - zr.qref) * (R)w_of(0) : out);
+            if (dup) Store<T>::st(hb + nodeup, out + (R)w_of(0) * up);
+        }
+#pragma unroll
+        for (int d = 1; d < Q; d += 2) {
+            const int o = d + 1;
+            const R wd = (R)w_of(d);
+            const R cu = (R)ex_of(d) * tux + (R)ey_of(d) * tuy + (R)ez_of(d) * tuz;
+            const R hep = wd * (dq + charge * ((R)0.5 * cu * cu - usq));
+            const R hem = wd * charge * cu;
+            const R hp = (R)0.5 * (h[d] + h[o]);
+            const R hm = (R)0.5 * (h[d] - h[o]);
+            const R relp = relax(cp_hi, cp_lo, hp - hep);
+            const R relm = relax(cm_hi, cm_lo, hm - hem);
+            const R outd = h[d] - (relp + relm);
+            const R outo = h[o] - (relp - relm);
+            Store<T>::st(hb + d * N + node, outd);
+            Store<T>::st(hb + o * N + node, outo);
+            if (dup) {
+                Store<T>::st(hb + d * N + nodeup, outd + wd * up);
+                Store<T>::st(hb + o * N + nodeup, outo + wd * up);
+            }
+        }
+    }
+}
+
+// Equilibrium populations from the FP64 fields (gpu_init_equilibrium,
+// LBM.cu:110-276), computed in FP64 and stored as deviations from the plane's
+// reference state.
+template <typename T>
+__global__ void init_equilibrium_kernel(T *__restrict__ f, T *__restrict__ h,
+                                        const double *__restrict__ r,
+                                        const double *__restrict__ u,
+                                        const double *__restrict__ v,
+                                        const double *__restrict__ w,
+                                        const double *__restrict__ q,
+                                        const double *__restrict__ ex,
+                                        const double *__restrict__ ey,
+                                        const double *__restrict__ ez,
+                                        const double *__restrict__ ref, StepConst c) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const int z = (int)(i / c.nxy);
+    const double rref = ref[2 * z], qref = ref[2 * z + 1];
+    const double cs2 = c.cs2;
+    const double rho = r[i], ux = u[i], uy = v[i], uz = w[i], ch = q[i];
+    const double ucx = ux + c.K * ex[i], ucy = uy + c.K * ey[i], ucz = uz + c.K * ez[i];
+    const double omusq = 1.0 - 0.5 * (ux * ux + uy * uy + uz * uz) / cs2;
+    const double omusq_c = 1.0 - 0.5 * (ucx * ucx + ucy * ucy + ucz * ucz) / cs2;
+    const double tux = ux / cs2 / c.cfl, tuy = uy / cs2 / c.cfl, tuz = uz / cs2 / c.cfl;
+    const double tcx = ucx / cs2 / c.cfl, tcy = ucy / cs2 / c.cfl, tcz = ucz / cs2 / c.cfl;
+#pragma unroll
+    for (int d = 0; d < Q; ++d) {
+        const double cu = ex_of(d) * tux + ey_of(d) * tuy + ez_of(d) * tuz;
+        const double cc = ex_of(d) * tcx + ey_of(d) * tcy + ez_of(d) * tcz;
+        const double fe = w_of(d) * rho * (omusq + cu * (1.0 + 0.5 * cu));
+        const double he = w_of(d) * ch * (omusq_c + cc * (1.0 + 0.5 * cc));
+        Store<T>::st(f + d * c.n + i, (decltype(Store<T>::ld(f)))(fe - w_of(d) * rref));
+        Store<T>::st(h + d * c.n + i, (decltype(Store<T>::ld(h)))(he - w_of(d) * qref));
+    }
+}
+
+// Driver-visible FP64 fields from the step's working buffers.  mask bit 1:
+// rho, u, v, w, q widened; bit 2: phi = phi00(z) + phi' and E = -grad(phi)
+// with the electrode copy of Ez (poisson.cu:44-73, 154-167).
+template <typename R>
+__global__ void materialize_kernel(const R *__restrict__ rho, const R *__restrict__ u,
+                                   const R *__restrict__ v, const R *__restrict__ w,
+                                   const R *__restrict__ q, const R *__restrict__ phip,
+                                   const double *__restrict__ phi00, double *__restrict__ o_rho,
+                                   double *__restrict__ o_u, double *__restrict__ o_v,
+                                   double *__restrict__ o_w, double *__restrict__ o_q,
+                                   double *__restrict__ o_phi, double *__restrict__ o_ex,
+                                   double *__restrict__ o_ey, double *__restrict__ o_ez,
+                                   int mask, StepConst c) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= c.nx) return;
+    const int NX = c.nx, NY = c.ny, NZ = c.nz;
+    auto idx = [&](int xx, int yy, int zz) {
+        return (long long)xx + (long long)NX * ((long long)yy + (long long)NY * zz);
+    };
+    auto phi = [&](int xx, int yy, int zz) { return phi00[zz] + (double)phip[idx(xx, yy, zz)]; };
+    const long long i = idx(x, y, z);
+    if (mask & 1) {
+        o_rho[i] = rho[i];
+        o_u[i] = u[i];
+        o_v[i] = v[i];
+        o_w[i] = w[i];
+        o_q[i] = q[i];
+    }
+    if (!(mask & 2)) return;
+    o_phi[i] = phi(x, y, z);
+    const int xm = (NX + x - 1) % NX, xp = (x + 1) % NX;
+    const int ym = (NY + y - 1) % NY, yp = (y + 1) % NY;
+    o_ex[i] = 0.5 * (phi(xm, y, z) - phi(xp, y, z)) * (2.0 * c.inv2dx);
+    o_ey[i] = 0.5 * (phi(x, ym, z) - phi(x, yp, z)) * (2.0 * c.inv2dy);
+    const int zc = z < 1 ? 1 : (z > NZ - 2 ? NZ - 2 : z);
+    o_ez[i] = 0.5 * (phi(x, y, zc - 1) - phi(x, y, zc + 1)) * (2.0 * c.inv2dz);
+}
+
+// The reference's start, gpu_initialization (LBM.cu:81-96): rho = rho0, q = 0,
+// phi = V (Lz - dz z)/Lz, u = E = 0, into the FP64 field arrays.
+__global__ void reference_init_kernel(double *const *out, StepConst c, double voltage,
+                                      double lz, double dz) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const int z = (int)(i / c.nxy);
+    out[0][i] = c.rho0;
+    out[1][i] = 0.0;
+    out[2][i] = 0.0;
+    out[3][i] = 0.0;
+    out[4][i] = 0.0;
+    out[5][i] = voltage * (lz - dz * z) / lz;
+    out[6][i] = 0.0;
+    out[7][i] = 0.0;
+    out[8][i] = 0.0;
+}
+
+// FP64 fields -> the step's compute-type macroscopic buffers.
+template <typename R>
+__global__ void fields_to_compute_kernel(const double *const *out, R *rho, R *u, R *v, R *w,
+                                         R *q, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    rho[i] = (R)out[0][i];
+    u[i] = (R)out[1][i];
+    v[i] = (R)out[2][i];
+    w[i] = (R)out[3][i];
+    q[i] = (R)out[4][i];
+}
+
+// ---- launchers ---------------------------------------------------------------
+
+template <typename T, typename R>
+cudaError_t launch_lbm_step(const LbmArgs &a, const StepConst &c, int local_pops, int e_arrays,
+                            bool macros, cudaStream_t s) {
+    dim3 block(c.nx >= 64 ? 64 : 32, c.nx >= 64 ? 2 : 4, 1);
+    dim3 grid((c.nx + block.x - 1) / block.x, (c.ny + block.y - 1) / block.y, c.nz);
+    const T *fa = (const T *)a.fa;
+    T *fb = (T *)a.fb;
+    const T *ha = (const T *)a.ha;
+    T *hb = (T *)a.hb;
+    const R *phip = (const R *)a.phip;
+    R *q = (R *)a.q, *r = (R *)a.rho, *u = (R *)a.u, *v = (R *)a.v, *w = (R *)a.w;
+    const bool general = local_pops || e_arrays;
+#define EHD_LAUNCH(G, M)                                                                    \
+    lbm_step_kernel<T, R, G, M><<<grid, block, 0, s>>>(fa, fb, ha, hb, phip, a.ez00, a.exa, \
+                                                       a.eya, a.eza, q, r, u, v, w,         \
+                                                       (const R *)a.zref, c, local_pops,    \
+                                                       e_arrays)
+    if (general) {
+        if (macros) EHD_LAUNCH(true, true);
+        else EHD_LAUNCH(true, false);
+    } else {
+        if (macros) EHD_LAUNCH(false, true);
+        else EHD_LAUNCH(false, false);
+    }
+#undef EHD_LAUNCH
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_init_equilibrium(void *f, void *h, const double *const fields[9],
+                                    const double *ref, const StepConst &c, cudaStream_t s) {
+    const int bs = 128;
+    const long long nb = (c.n + bs - 1) / bs;
+    init_equilibrium_kernel<T><<<(unsigned)nb, bs, 0, s>>>(
+        (T *)f, (T *)h, fields[0], fields[1], fields[2], fields[3], fields[4], fields[6],
+        fields[7], fields[8], ref, c);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_materialize(const void *rho, const void *u, const void *v, const void *w,
+                               const void *q, const void *phip, const double *phi00,
+                               double *const out[9], int mask, const StepConst &c,
+                               cudaStream_t s) {
+    dim3 block(c.nx >= 128 ? 128 : 32);
+    dim3 grid((c.nx + block.x - 1) / block.x, c.ny, c.nz);
+    materialize_kernel<R><<<grid, block, 0, s>>>(
+        (const R *)rho, (const R *)u, (const R *)v, (const R *)w, (const R *)q,
+        (const R *)phip, phi00, out[0], out[1], out[2], out[3], out[4], out[5], out[6],
+        out[7], out[8], mask, c);
+    return cudaGetLastError();
+}
+
+#define EHD_INST_LBM(T, R) template cudaError_t launch_lbm_step<T, R>(const LbmArgs &, \
+    const StepConst &, int, int, bool, cudaStream_t);
+EHD_INST_LBM(double, double)
+EHD_INST_LBM(float, float)
+EHD_INST_LBM(__half, float)
+EHD_INST_LBM(__nv_bfloat16, float)
+template cudaError_t launch_init_equilibrium<double>(void *, void *, const double *const[9],
+                                                    const double *, const StepConst &, cudaStream_t);
+template cudaError_t launch_init_equilibrium<float>(void *, void *, const double *const[9],
+                                                   const double *, const StepConst &, cudaStream_t);
+template cudaError_t launch_init_equilibrium<__half>(void *, void *, const double *const[9],
+                                                    const double *, const StepConst &, cudaStream_t);
+template cudaError_t launch_init_equilibrium<__nv_bfloat16>(void *, void *,
+                                                           const double *const[9],
+                                                           const double *, const StepConst &,
+                                                           cudaStream_t);
+template cudaError_t launch_materialize<double>(const void *, const void *, const void *,
+                                               const void *, const void *, const void *,
+                                               const double *, double *const[9], int,
+                                               const StepConst &, cudaStream_t);
+template cudaError_t launch_materialize<float>(const void *, const void *, const void *,
+                                              const void *, const void *, const void *,
+                                              const double *, double *const[9], int,
+                                              const StepConst &, cudaStream_t);
+
+cudaError_t launch_reference_init(double *const *out_dev, const StepConst &c, double voltage,
+                                  double lz, double dz, cudaStream_t s) {
+    const int bs = 256;
+    reference_init_kernel<<<(unsigned)((c.n + bs - 1) / bs), bs, 0, s>>>(out_dev, c, voltage,
+                                                                         lz, dz);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_fields_to_compute(double *const *out_dev, void *rho, void *u, void *v,
+                                     void *w, void *q, long long n, cudaStream_t s) {
+    const int bs = 256;
+    fields_to_compute_kernel<R><<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(
+        out_dev, (R *)rho, (R *)u, (R *)v, (R *)w, (R *)q, n);
+    return cudaGetLastError();
+}
+template cudaError_t launch_fields_to_compute<float>(double *const *, void *, void *, void *,
+                                                     void *, void *, long long, cudaStream_t);
+template cudaError_t launch_fields_to_compute<double>(double *const *, void *, void *, void *,
+                                                      void *, void *, long long, cudaStream_t);
+
+// Per-plane reference state from the FP64 fields: ref[2z] = mean rho,
+// ref[2z+1] = mean q over the plane (one block per plane, fixed-order FP64
+// reduction), then the compute-type table of load_zref.
+__global__ void plane_mean_kernel(const double *__restrict__ rho, const double *__restrict__ q,
+                                  double *__restrict__ ref, long long nxy) {
+    __shared__ double sr[256], sq[256];
+    const int z = blockIdx.x;
+    double a = 0.0, b = 0.0;
+    for (long long i = threadIdx.x; i < nxy; i += blockDim.x) {
+        a += rho[z * nxy + i];
+        b += q[z * nxy + i];
+    }
+    sr[threadIdx.x] = a;
+    sq[threadIdx.x] = b;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            sr[threadIdx.x] += sr[threadIdx.x + o];
+            sq[threadIdx.x] += sq[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        ref[2 * z] = sr[0] / (double)nxy;
+        ref[2 * z + 1] = sq[0] / (double)nxy;
+    }
+}
+
+template <typename R>
+__global__ void build_zref_kernel(const double *__restrict__ ref, R *__restrict__ zref, int nz) {
+    for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+        const int zm = z == 0 ? nz - 1 : z - 1, zp = z == nz - 1 ? 0 : z + 1;
+        zref[6 * z + 0] = (R)ref[2 * z];
+        zref[6 * z + 1] = (R)ref[2 * z + 1];
+        zref[6 * z + 2] = (R)(ref[2 * zm] - ref[2 * z]);
+        zref[6 * z + 3] = (R)(ref[2 * zp] - ref[2 * z]);
+        zref[6 * z + 4] = (R)(ref[2 * zm + 1] - ref[2 * z + 1]);
+        zref[6 * z + 5] = (R)(ref[2 * zp + 1] - ref[2 * z + 1]);
+    }
+}
+
+template <typename R>
+cudaError_t launch_plane_refs(const double *rho, const double *q, double *ref, void *zref,
+                              const StepConst &c, cudaStream_t s) {
+    plane_mean_kernel<<<c.nz, 256, 0, s>>>(rho, q, ref, c.nxy);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    build_zref_kernel<R><<<1, 256, 0, s>>>(ref, (R *)zref, c.nz);
+    return cudaGetLastError();
+}
+template cudaError_t launch_plane_refs<float>(const double *, const double *, double *, void *,
+                                              const StepConst &, cudaStream_t);
+template cudaError_t launch_plane_refs<double>(const double *, const double *, double *, void *,
+                                               const StepConst &, cudaStream_t);
+
+}  // namespace ehd

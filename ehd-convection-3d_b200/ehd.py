@@ -1,0 +1,220 @@
+"""Python binding of libehd.so (include/ehd.h) through ctypes.
+
+This is the host-side mirror used by the tests and the benchmark: one
+``Simulation`` is one ``ehd_ctx``.  Field arrays are numpy float64 of shape
+(nz, ny, nx), the reference layout x + NX*(y + NY*z) (LBM.cu:21-24).  The
+binding adds no computation of its own: every call goes to the CUDA library,
+and a missing library is an error (there is no CPU path).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libehd.so"
+
+FIELDS = ("rho", "u", "v", "w", "q", "phi", "ex", "ey", "ez")
+PRECISIONS = {"fp64": 0, "fp32": 1, "fp16": 2, "bf16": 3}
+FLAG_NO_GRAPH = 0x1
+
+
+class EhdError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"ehd error {code}: {msg}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    """ehd_params (include/ehd.h)."""
+
+    _fields_ = [
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+        ("pad_", ctypes.c_int32),
+        ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("lz", ctypes.c_double),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
+        ("dt", ctypes.c_double), ("cfl", ctypes.c_double),
+        ("rho0", ctypes.c_double), ("charge0", ctypes.c_double),
+        ("voltage", ctypes.c_double), ("eps", ctypes.c_double),
+        ("diffu", ctypes.c_double), ("nu", ctypes.c_double), ("K", ctypes.c_double),
+        ("uw", ctypes.c_double), ("exf", ctypes.c_double),
+        ("lambda_f", ctypes.c_double), ("lambda_g", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad_"}
+
+    @classmethod
+    def from_dict(cls, d):
+        p = cls()
+        for k, v in d.items():
+            setattr(p, k, v)
+        p.pad_ = 0
+        return p
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int32), ("device", ctypes.c_int32),
+                ("stream", ctypes.c_void_p), ("flags", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 7)]
+
+
+class Diag(ctypes.Structure):
+    _fields_ = [("current", ctypes.c_double), ("nu_e", ctypes.c_double),
+                ("kinetic_energy", ctypes.c_double), ("total_charge", ctypes.c_double),
+                ("umax", ctypes.c_double), ("time", ctypes.c_double),
+                ("step", ctypes.c_int64), ("nonfinite", ctypes.c_int32),
+                ("pad_", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad_"}
+
+
+# every symbol include/ehd.h declares, with (restype, argtypes)
+_dp = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+SIGNATURES = {
+    "ehd_abi_version": (_i, []),
+    "ehd_last_error": (ctypes.c_char_p, []),
+    "ehd_create": (_i, [ctypes.POINTER(Params), ctypes.POINTER(Config), ctypes.POINTER(_vp)]),
+    "ehd_destroy": (_i, [_vp]),
+    "ehd_set_fields": (_i, [_vp] + [_dp] * 9),
+    "ehd_initialize": (_i, [_vp]),
+    "ehd_get_fields": (_i, [_vp] + [_dp] * 9),
+    "ehd_step": (_i, [_vp, _i]),
+    "ehd_stream_collide_save": (_i, [_vp]),
+    "ehd_poisson": (_i, [_vp]),
+    "ehd_synchronize": (_i, [_vp]),
+    "ehd_current": (_i, [_vp, _dp]),
+    "ehd_set_reference_current": (_i, [_vp, ctypes.c_double]),
+    "ehd_diagnostics": (_i, [_vp, ctypes.POINTER(Diag)]),
+    "ehd_device_bytes": (_i, [_vp, ctypes.POINTER(ctypes.c_size_t)]),
+    "ehd_params_from_groups": (_i, [ctypes.POINTER(Params)] + [ctypes.c_double] * 4),
+    "ehd_groups_from_params": (_i, [ctypes.POINTER(Params)] + [_dp] * 4),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libehd.so; raise if it was not built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing: build it with `make -C {HERE}` (no CPU fallback)")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise EhdError(rc, lib().ehd_last_error().decode(errors="replace"))
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+def params_from_groups(nx, ny, nz, lx, ly, T, M, C, Fe, lambda_f=0.25, lambda_g=0.25,
+                       cfl=0.01, lz=1.0, **over) -> Params:
+    """Grid + dimensionless groups -> ehd_params, through ehd_params_from_groups
+    (the inverse of the reference's compute_parameters, LBM.cu:1356-1379)."""
+    dz = lz / (nz - 1)
+    p = Params(nx=nx, ny=ny, nz=nz, pad_=0, lx=lx, ly=ly, lz=lz, dx=lx / nx, dy=ly / ny, dz=dz,
+               dt=cfl * dz, cfl=cfl, rho0=1600.0, charge0=0.0, voltage=1.0e4, eps=1.0e-4,
+               diffu=0.0, nu=0.0, K=0.0, uw=0.0, exf=0.0, lambda_f=lambda_f, lambda_g=lambda_g)
+    _check(lib().ehd_params_from_groups(ctypes.byref(p), T, M, C, Fe))
+    for k, v in over.items():
+        setattr(p, k, v)
+    return p
+
+
+def groups_of(p: Params):
+    out = [ctypes.c_double() for _ in range(4)]
+    _check(lib().ehd_groups_from_params(ctypes.byref(p), *[ctypes.byref(o) for o in out]))
+    return dict(zip(("T", "M", "C", "Fe"), [o.value for o in out]))
+
+
+class Simulation:
+    """One simulation instance (ehd_ctx) on one GPU."""
+
+    def __init__(self, params: Params, precision: str = "fp32", device: int = 0,
+                 stream: int | None = None, graphs: bool = True):
+        self.p = params
+        self.shape = (params.nz, params.ny, params.nx)
+        cfg = Config(precision=PRECISIONS[precision], device=device, stream=stream,
+                     flags=0 if graphs else FLAG_NO_GRAPH)
+        h = _vp()
+        _check(lib().ehd_create(ctypes.byref(params), ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ehd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_fields(self, fields: dict):
+        arrs = [np.ascontiguousarray(np.broadcast_to(fields[k], self.shape), dtype=np.float64)
+                for k in FIELDS]
+        _check(lib().ehd_set_fields(self.h, *[_ptr(a) for a in arrs]))
+
+    def initialize(self):
+        _check(lib().ehd_initialize(self.h))
+
+    def get_fields(self, names=FIELDS) -> dict:
+        out = {k: np.empty(self.shape, np.float64) for k in names}
+        ptrs = [(_ptr(out[k]) if k in out else None) for k in FIELDS]
+        _check(lib().ehd_get_fields(self.h, *ptrs))
+        return out
+
+    def step(self, n: int = 1):
+        _check(lib().ehd_step(self.h, int(n)))
+
+    def stream_collide_save(self):
+        _check(lib().ehd_stream_collide_save(self.h))
+
+    def poisson(self):
+        _check(lib().ehd_poisson(self.h))
+
+    def synchronize(self):
+        _check(lib().ehd_synchronize(self.h))
+
+    def current(self) -> float:
+        c = ctypes.c_double()
+        _check(lib().ehd_current(self.h, ctypes.byref(c)))
+        return c.value
+
+    def set_reference_current(self, i0: float):
+        _check(lib().ehd_set_reference_current(self.h, float(i0)))
+
+    def diagnostics(self) -> dict:
+        d = Diag()
+        _check(lib().ehd_diagnostics(self.h, ctypes.byref(d)))
+        return d.as_dict()
+
+    def device_bytes(self) -> int:
+        b = ctypes.c_size_t()
+        _check(lib().ehd_device_bytes(self.h, ctypes.byref(b)))
+        return b.value

@@ -226,6 +226,8 @@ void orc_fft1d(double *a, int n, int sign) { fft_lines(a, n, 1, n, 1, sign); }
 /* context                                                                  */
 /* ------------------------------------------------------------------------ */
 
+void orc_destroy(orc_ctx *c);
+
 orc_ctx *orc_create(const orc_params *p) {
     orc_ctx *c = (orc_ctx *)calloc(1, sizeof(orc_ctx));
     c->p = *p;
@@ -249,6 +251,16 @@ orc_ctx *orc_create(const orc_params *p) {
     size_t ns = (size_t)p->nx * p->ny * c->ne;
     c->ext = calloc(2 * ns, sizeof(double));
     c->ext2 = calloc(2 * ns, sizeof(double));
+    {
+        double *all[] = {c->f0, c->h0, c->f0pre, c->h0pre, c->f1, c->f2, c->h1, c->h2,
+                         c->rho, c->q, c->u, c->v, c->w, c->phi, c->ex, c->ey, c->ez,
+                         c->f0bc, c->kx, c->ky, c->kz, c->ext, c->ext2};
+        for (size_t i = 0; i < sizeof(all) / sizeof(all[0]); ++i)
+            if (!all[i]) {
+                orc_destroy(c);
+                return NULL;
+            }
+    }
     /* wavenumbers, main.cu:110-136 */
     for (int i = 0; i < p->nx; ++i)
         c->kx[i] = (i <= p->nx / 2 ? (double)i : (double)i - p->nx) * 2.0 * M_PI / p->lx;
@@ -623,6 +635,16 @@ void orc_step_lbm(orc_ctx *c) {
     boundary(c);
     stream(c);
     bc_charge(c);
+}
+
+/* Test hooks: the collide pass alone, and the post-collision / post-wall
+ * populations f2, h2 (with the in-place rest populations f0, h0). */
+void orc_collide_only(orc_ctx *c) { collide(c); }
+void orc_get_post(const orc_ctx *c, double *f0, double *f2, double *h0, double *h2) {
+    memcpy(f0, c->f0, c->n * sizeof(double));
+    memcpy(h0, c->h0, c->n * sizeof(double));
+    memcpy(f2, c->f2, 26 * c->n * sizeof(double));
+    memcpy(h2, c->h2, 26 * c->n * sizeof(double));
 }
 
 /* current(), LBM.cu:1647-1671: q at the collector extrapolated linearly from

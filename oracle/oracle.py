@@ -119,6 +119,8 @@ def lib():
         L.orc_current.restype = ctypes.c_double
         L.orc_current.argtypes = [ctypes.c_void_p]
         L.orc_fft1d.argtypes = [dp, ctypes.c_int, ctypes.c_int]
+        L.orc_collide_only.argtypes = [ctypes.c_void_p]
+        L.orc_get_post.argtypes = [ctypes.c_void_p] + [dp] * 4
         L.orc_set_threads.argtypes = [ctypes.c_int]
         L.orc_get_threads.restype = ctypes.c_int
         _lib = L
@@ -187,6 +189,16 @@ class Oracle:
     def set_pops(self, f0, f1, h0, h1):
         a = [np.ascontiguousarray(x, np.float64) for x in (f0, f1, h0, h1)]
         lib().orc_set_pops(self.h, *[_ptr(x) for x in a])
+
+    def collide_only(self):
+        lib().orc_collide_only(self.h)
+
+    def get_post(self):
+        n = self.shape
+        f0 = np.empty(n); h0 = np.empty(n)
+        f2 = np.empty((26,) + n); h2 = np.empty((26,) + n)
+        lib().orc_get_post(self.h, _ptr(f0), _ptr(f2), _ptr(h0), _ptr(h2))
+        return f0, f2, h0, h2
 
     def initialization(self):
         lib().orc_initialization(self.h)
