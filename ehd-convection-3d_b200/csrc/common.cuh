@@ -64,6 +64,36 @@ struct StepConst {
     double mw[Q];             // moving-wall increment per direction at z=nz-1
 };
 
+// weight class: 0 rest, 1 axis (2/27), 2 face diagonal (1/54), 3 body diagonal (1/216)
+__host__ __device__ constexpr int cls_of(int d) { return d == 0 ? 0 : (d <= 6 ? 1 : (d <= 18 ? 2 : 3)); }
+
+// Per-direction base pointers of the two population buffers, passed by value
+// so each access is a 32-bit node offset from a kernel-parameter base.
+template <typename T>
+struct PopPtrs {
+    const T *fa[Q];
+    T *fb[Q];
+    const T *ha[Q];
+    T *hb[Q];
+};
+
+// The step constants in the compute type, with the per-weight-class factors
+// of the collision precomputed (see lbm_step_kernel).
+template <typename R>
+struct KConst {
+    int nx, ny, nz;
+    unsigned nxy;
+    R dt_half, cflinv, inv_cs2, inv_cs2cfl;
+    R rate_hi[4], rate_lo[4];
+    R q0, K, exf;
+    R inv2dx, inv2dy, inv2dz;
+    R w[4];
+    R c1[4];  // dt sp w cflinv2 CFL   (times cu eF)
+    R c2[4];  // dt sm (w/cs2) cflinv  (times eF)
+    R c3[4];  // dt sp (w/cs2)         (times u.F)
+    R mw[Q];
+};
+
 // ---- storage types ---------------------------------------------------------
 template <typename T> struct Store;
 template <> struct Store<double> {
@@ -90,5 +120,38 @@ template <> struct Store<__nv_bfloat16> {
 template <typename R> struct Cplx;
 template <> struct Cplx<float> { using T = float2; };
 template <> struct Cplx<double> { using T = double2; };
+
+template <typename R>
+inline KConst<R> make_kconst(const StepConst &c) {
+    KConst<R> k{};
+    k.nx = c.nx;
+    k.ny = c.ny;
+    k.nz = c.nz;
+    k.nxy = (unsigned)c.nxy;
+    k.dt_half = (R)(0.5 * c.dt);
+    k.cflinv = (R)c.cflinv;
+    k.inv_cs2 = (R)(1.0 / c.cs2);
+    k.inv_cs2cfl = (R)(1.0 / (c.cs2 * c.cfl));
+    for (int i = 0; i < 4; ++i) {
+        k.rate_hi[i] = (R)c.rate_hi[i];
+        k.rate_lo[i] = (R)c.rate_lo[i];
+    }
+    k.q0 = (R)c.q0;
+    k.K = (R)c.K;
+    k.exf = (R)c.exf;
+    k.inv2dx = (R)c.inv2dx;
+    k.inv2dy = (R)c.inv2dy;
+    k.inv2dz = (R)c.inv2dz;
+    const int rep[4] = {0, 1, 7, 19};
+    for (int i = 0; i < 4; ++i) {
+        const double w = w_of(rep[i]);
+        k.w[i] = (R)w;
+        k.c1[i] = (R)(c.dt * c.sp * w * c.cflinv2 * c.cfl);
+        k.c2[i] = (R)(c.dt * c.sm * (w / c.cs2) * c.cflinv);
+        k.c3[i] = (R)(c.dt * c.sp * (w / c.cs2));
+    }
+    for (int d = 0; d < Q; ++d) k.mw[d] = (R)c.mw[d];
+    return k;
+}
 
 }  // namespace ehd

@@ -37,14 +37,12 @@ namespace ehd {
 
 namespace {
 
-template <typename R>
 struct PullIdx {
-    long long row[3][3];  // [dy+1][dz+1] -> NX*(ys + NY*zs) for source (y - dy, z - dz)
-    int xs[3];            // [dx+1] -> source x - dx
+    unsigned row[3][3];  // [e_y+1][e_z+1] -> NX*(ys + NY*zs) for source (y - e_y, z - e_z)
+    int xs[3];           // [e_x+1] -> source x - e_x
 };
 
-template <typename R>
-__device__ __forceinline__ void make_pull(PullIdx<R> &P, int x, int y, int z, int NX, int NY,
+__device__ __forceinline__ void make_pull(PullIdx &P, int x, int y, int z, int NX, int NY,
                                           int NZ) {
     const int xm = x == 0 ? NX - 1 : x - 1, xp = x == NX - 1 ? 0 : x + 1;
     const int ym = y == 0 ? NY - 1 : y - 1, yp = y == NY - 1 ? 0 : y + 1;
@@ -58,12 +56,21 @@ __device__ __forceinline__ void make_pull(PullIdx<R> &P, int x, int y, int z, in
     for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int b = 0; b < 3; ++b)
-            P.row[a][b] = (long long)NX * ((long long)ys[a] + (long long)NY * zs[b]);
+            P.row[a][b] = (unsigned)NX * ((unsigned)ys[a] + (unsigned)NY * (unsigned)zs[b]);
 }
 
+__device__ __forceinline__ unsigned pull_src(const PullIdx &P, int d) {
+    return P.row[ey_of(d) + 1][ez_of(d) + 1] + (unsigned)P.xs[ex_of(d) + 1];
+}
+
+// e_d . (a, b, c) with the components of e_d in {-1, 0, 1}
 template <typename R>
-__device__ __forceinline__ long long pull_src(const PullIdx<R> &P, int d) {
-    return P.row[ey_of(d) + 1][ez_of(d) + 1] + P.xs[ex_of(d) + 1];
+__device__ __forceinline__ R dot_e(int d, R a, R b, R c) {
+    R s = 0;
+    if (ex_of(d)) s = ex_of(d) > 0 ? a : -a;
+    if (ey_of(d)) s = ey_of(d) > 0 ? s + b : s - b;
+    if (ez_of(d)) s = ez_of(d) > 0 ? s + c : s - c;
+    return s;
 }
 
 // Per-plane reference state.  Populations are stored as deviations from
@@ -100,14 +107,23 @@ __device__ __forceinline__ ZRef<R> load_zref(const R *__restrict__ t, int z) {
 //               (the reference's f1/h1 after init_equilibrium), so they are
 //               read in place, without pull or injection rule;
 //   e_arrays:   E comes from the uploaded FP64 arrays instead of phi.
+//
+// Collision algebra (LBM.cu:519-1089 rewritten on deviations, per opposite
+// pair d, o = d+1 of weight class k, s = f_d + f_o):
+//   fp - feq+  = s/2 + P_k - (w_k rho / 2) cu^2,  P_k = w_k rho usq - w_k drho
+//   fm - feq-  = (f_d - f_o)/2 - w_k rho cu
+//   A = rate+ (fp - feq+) + dt sp (w_k/cs2) uF - dt sp w_k cflinv2 CFL cu eF
+//   B = rate- (fm - feq-) - dt sm (w_k/cs2) cflinv eF
+//   f_d' = f_d - A - B,  f_o' = f_o - A + B
+// (e.u = cu cs2 CFL); the same with q, u + K E and no source for g.
 template <typename T, typename R, bool GENERAL, bool MACROS>
-__global__ void __launch_bounds__(128)
-lbm_step_kernel(const T *__restrict__ fa, T *__restrict__ fb, const T *__restrict__ ha,
-                T *__restrict__ hb, const R *__restrict__ phip, const double *__restrict__ ez00,
-                const double *__restrict__ exa, const double *__restrict__ eya,
-                const double *__restrict__ eza, R *__restrict__ qout, R *__restrict__ rout,
-                R *__restrict__ uout, R *__restrict__ vout, R *__restrict__ wout,
-                const R *__restrict__ zref, StepConst c, int local_pops, int e_arrays) {
+__global__ void __launch_bounds__(128, sizeof(R) == 8 ? 2 : 4)
+lbm_step_kernel(const PopPtrs<T> pp, const R *__restrict__ phip,
+                const double *__restrict__ ez00, const double *__restrict__ exa,
+                const double *__restrict__ eya, const double *__restrict__ eza,
+                R *__restrict__ qout, R *__restrict__ rout, R *__restrict__ uout,
+                R *__restrict__ vout, R *__restrict__ wout, const R *__restrict__ zref,
+                const KConst<R> c, int local_pops, int e_arrays) {
     const bool LOCAL = GENERAL && local_pops;
     const bool EARR = GENERAL && e_arrays;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -115,15 +131,10 @@ lbm_step_kernel(const T *__restrict__ fa, T *__restrict__ fb, const T *__restric
     const int z = blockIdx.z;
     if (x >= c.nx || y >= c.ny) return;
     const int NX = c.nx, NY = c.ny, NZ = c.nz;
-    const long long N = c.n;
-    const long long node = (long long)x + (long long)NX * ((long long)y + (long long)NY * z);
-
-    const R q0 = (R)c.q0;
-    // per-plane reference state (rho_ref, q_ref) and the offsets that carry a
-    // population stored relative to its own plane over to this plane
+    const unsigned node = (unsigned)x + (unsigned)NX * ((unsigned)y + (unsigned)NY * z);
     const ZRef<R> zr = load_zref(zref, z);
 
-    PullIdx<R> P;
+    PullIdx P;
     make_pull(P, x, y, z, NX, NY, NZ);
 
     // ---- pull (the reference's stream + injection rule), as deviations
@@ -131,23 +142,25 @@ lbm_step_kernel(const T *__restrict__ fa, T *__restrict__ fb, const T *__restric
     R f[Q], h[Q];
 #pragma unroll
     for (int d = 0; d < Q; ++d) {
-        f[d] = Store<T>::ld(fa + d * N + (LOCAL ? node : pull_src(P, d)));
-        if (!LOCAL) f[d] += (R)w_of(d) * zr.dr(ez_of(d));
+        f[d] = Store<T>::ld(pp.fa[d] + (LOCAL ? node : pull_src(P, d)));
+        if (!LOCAL && ez_of(d) != 0) f[d] += c.w[cls_of(d)] * zr.dr(ez_of(d));
     }
     if (LOCAL) {
 #pragma unroll
-        for (int d = 0; d < Q; ++d) h[d] = Store<T>::ld(ha + d * N + node);
+        for (int d = 0; d < Q; ++d) h[d] = Store<T>::ld(pp.ha[d] + node);
     } else if (z == 0) {
         // g_d = -g_opp(d) + 2 q0 w_d (LBM.cu:1320-1348), on deviations
-        h[0] = Store<T>::ld(ha + node);
-        const R inj = (R)2 * (q0 - zr.qref);
+        h[0] = Store<T>::ld(pp.ha[0] + node);
+        const R inj = (R)2 * (c.q0 - zr.qref);
 #pragma unroll
         for (int d = 1; d < Q; ++d)
-            h[d] = -Store<T>::ld(ha + opp_of(d) * N + node) + inj * (R)w_of(d);
+            h[d] = -Store<T>::ld(pp.ha[opp_of(d)] + node) + inj * c.w[cls_of(d)];
     } else {
 #pragma unroll
-        for (int d = 0; d < Q; ++d)
-            h[d] = Store<T>::ld(ha + d * N + pull_src(P, d)) + (R)w_of(d) * zr.dq(ez_of(d));
+        for (int d = 0; d < Q; ++d) {
+            h[d] = Store<T>::ld(pp.ha[d] + pull_src(P, d));
+            if (ez_of(d) != 0) h[d] += c.w[cls_of(d)] * zr.dq(ez_of(d));
+        }
     }
 
     // ---- moments ----
@@ -165,52 +178,50 @@ lbm_step_kernel(const T *__restrict__ fa, T *__restrict__ fb, const T *__restric
 
     // ---- E at this node (and at z = 1 for the injector override) ----
     R Ex, Ey, Ez;
-    const long long row = (long long)NX * ((long long)y + (long long)NY * z);
+    const unsigned row = (unsigned)NX * ((unsigned)y + (unsigned)NY * z);
     const int xm = x == 0 ? NX - 1 : x - 1, xp = x == NX - 1 ? 0 : x + 1;
     const int ym = y == 0 ? NY - 1 : y - 1, yp = y == NY - 1 ? 0 : y + 1;
+    const unsigned rym = (unsigned)NX * ((unsigned)ym + (unsigned)NY * z);
+    const unsigned ryp = (unsigned)NX * ((unsigned)yp + (unsigned)NY * z);
     if (!EARR) {
         // E = -grad(phi), central differences (gpu_efield, poisson.cu:44-60);
         // phi = phi00(z) + phi'(x,y,z) with phi' = 0 on both electrodes, and
         // Ez on the electrodes copied from the planes inside (gpu_bc,
         // poisson.cu:61-73).
-        Ex = (__ldg(phip + row + xm) - __ldg(phip + row + xp)) * (R)c.inv2dx;
-        Ey = (__ldg(phip + (long long)NX * ((long long)ym + (long long)NY * z) + x) -
-              __ldg(phip + (long long)NX * ((long long)yp + (long long)NY * z) + x)) *
-             (R)c.inv2dy;
+        Ex = (__ldg(phip + row + xm) - __ldg(phip + row + xp)) * c.inv2dx;
+        Ey = (__ldg(phip + rym + x) - __ldg(phip + ryp + x)) * c.inv2dy;
         const int zc = z < 1 ? 1 : (z > NZ - 2 ? NZ - 2 : z);
+        const unsigned rzc = (unsigned)NX * ((unsigned)y + (unsigned)NY * zc);
         Ez = (R)__ldg(ez00 + zc) +
-             (__ldg(phip + (long long)NX * ((long long)y + (long long)NY * (zc - 1)) + x) -
-              __ldg(phip + (long long)NX * ((long long)y + (long long)NY * (zc + 1)) + x)) *
-                 (R)c.inv2dz;
+             (__ldg(phip + rzc - c.nxy + x) - __ldg(phip + rzc + c.nxy + x)) * c.inv2dz;
     } else {
         Ex = (R)__ldg(exa + node);
         Ey = (R)__ldg(eya + node);
         Ez = (R)__ldg(eza + node);
     }
 
-    const R dt = (R)c.dt, cfl = (R)c.cfl;
-    const R fx = charge * Ex + (R)c.exf, fy = charge * Ey, fz = charge * Ez;
+    const R fx = charge * Ex + c.exf, fy = charge * Ey, fz = charge * Ez;
     const R rhoinv = (R)1 / rho;
-    R ux = rhoinv * (mx / cfl + fx * dt * (R)0.5);
-    R uy = rhoinv * (my / cfl + fy * dt * (R)0.5);
-    R uz = rhoinv * (mz / cfl + fz * dt * (R)0.5);
+    R ux = rhoinv * (mx * c.cflinv + fx * c.dt_half);
+    R uy = rhoinv * (my * c.cflinv + fy * c.dt_half);
+    R uz = rhoinv * (mz * c.cflinv + fz * c.dt_half);
 
     if (z == 0) {
         // LBM.cu:417-492
         const ZRef<R> z1 = load_zref(zref, 1);
-        PullIdx<R> P1;
+        PullIdx P1;
         make_pull(P1, x, y, 1, NX, NY, NZ);
-        const long long node1 = node + c.nxy;
-        R dqm = Store<T>::ld(ha + node1);
+        const unsigned node1 = node + c.nxy;
+        R dqm = Store<T>::ld(pp.ha[0] + node1);
         R mxm = 0, mym = 0, mzm = 0;
 #pragma unroll
         for (int d = 1; d < Q; ++d) {
-            const long long s1 = LOCAL ? node1 : pull_src(P1, d);
-            R fm = Store<T>::ld(fa + d * N + s1);
-            R hm = Store<T>::ld(ha + d * N + s1);
-            if (!LOCAL) {
-                fm += (R)w_of(d) * z1.dr(ez_of(d));
-                hm += (R)w_of(d) * z1.dq(ez_of(d));
+            const unsigned s1 = LOCAL ? node1 : pull_src(P1, d);
+            R fm = Store<T>::ld(pp.fa[d] + s1);
+            R hm = Store<T>::ld(pp.ha[d] + s1);
+            if (!LOCAL && ez_of(d) != 0) {
+                fm += c.w[cls_of(d)] * z1.dr(ez_of(d));
+                hm += c.w[cls_of(d)] * z1.dq(ez_of(d));
             }
             dqm += hm;
             if (ex_of(d)) mxm += ex_of(d) > 0 ? fm : -fm;
@@ -220,24 +231,20 @@ lbm_step_kernel(const T *__restrict__ fa, T *__restrict__ fb, const T *__restric
         const R chargem = z1.qref + dqm;
         R Exm, Eym, Ezm;
         if (!EARR) {
-            const long long row1 = row + c.nxy;
-            Exm = (__ldg(phip + row1 + xm) - __ldg(phip + row1 + xp)) * (R)c.inv2dx;
-            Eym = (__ldg(phip + (long long)NX * ((long long)ym + (long long)NY) + x) -
-                   __ldg(phip + (long long)NX * ((long long)yp + (long long)NY) + x)) *
-                  (R)c.inv2dy;
+            const unsigned row1 = row + c.nxy;
+            Exm = (__ldg(phip + row1 + xm) - __ldg(phip + row1 + xp)) * c.inv2dx;
+            Eym = (__ldg(phip + rym + c.nxy + x) - __ldg(phip + ryp + c.nxy + x)) * c.inv2dy;
             Ezm = (R)__ldg(ez00 + 1) +
-                  (__ldg(phip + (long long)NX * (long long)y + x) -
-                   __ldg(phip + (long long)NX * ((long long)y + 2LL * NY) + x)) *
-                      (R)c.inv2dz;
+                  (__ldg(phip + row + x) - __ldg(phip + row + 2 * c.nxy + x)) * c.inv2dz;
         } else {
             Exm = (R)__ldg(exa + node1);
             Eym = (R)__ldg(eya + node1);
             Ezm = (R)__ldg(eza + node1);
         }
-        const R fxm = chargem * Exm + (R)c.exf, fym = chargem * Eym, fzm = chargem * Ezm;
-        ux = -rhoinv * (mxm / cfl + fxm * dt * (R)0.5);
-        uy = -rhoinv * (mym / cfl + fym * dt * (R)0.5);
-        uz = -rhoinv * (mzm / cfl + fzm * dt * (R)0.5);
+        const R fxm = chargem * Exm + c.exf, fym = chargem * Eym, fzm = chargem * Ezm;
+        ux = -rhoinv * (mxm * c.cflinv + fxm * c.dt_half);
+        uy = -rhoinv * (mym * c.cflinv + fym * c.dt_half);
+        uz = -rhoinv * (mzm * c.cflinv + fzm * c.dt_half);
     }
 
     qout[node] = charge;
@@ -248,90 +255,80 @@ lbm_step_kernel(const T *__restrict__ fa, T *__restrict__ fb, const T *__restric
         wout[node] = uz;
     }
 
-    const R inv_cs2 = (R)(1.0 / c.cs2);
-    const R inv_cs2cfl = (R)(1.0 / (c.cs2 * c.cfl));
-
-    // ---- f: collide (interior) or wall rule; TRT on deviations:
-    // feq+ - w rho_ref = w drho + w rho (cu^2/2 - |u|^2/(2 cs^2)),
-    // feq- = w rho cu (LBM.cu:519-660, 704-1089) ----
+    // ---- f: collide (interior) or wall rule ----
     if (z == 0 || z == NZ - 1) {
-        Store<T>::st(fb + node, f[0]);
+        Store<T>::st(pp.fb[0] + node, f[0]);
 #pragma unroll
         for (int d = 1; d < Q; ++d) {
             R v = f[opp_of(d)];
-            if (z == NZ - 1 && mw_sign_of(d) != 0) v += (R)c.mw[d];
-            Store<T>::st(fb + d * N + node, v);
+            if (z == NZ - 1 && mw_sign_of(d) != 0) v += c.mw[d];
+            Store<T>::st(pp.fb[d] + node, v);
         }
     } else {
-        const R rp_hi = (R)c.rate_hi[0], rp_lo = (R)c.rate_lo[0];
-        const R rm_hi = (R)c.rate_hi[1], rm_lo = (R)c.rate_lo[1];
-        const R sp = (R)c.sp, sm = (R)c.sm;
-        const R cflinv = (R)c.cflinv, cflinv2 = (R)c.cflinv2;
-        const R usq = (R)0.5 * (ux * ux + uy * uy + uz * uz) * inv_cs2;
-        const R tux = ux * inv_cs2cfl, tuy = uy * inv_cs2cfl, tuz = uz * inv_cs2cfl;
+        const R rp_hi = c.rate_hi[0], rp_lo = c.rate_lo[0];
+        const R rm_hi = c.rate_hi[1], rm_lo = c.rate_lo[1];
+        const R usq = (R)0.5 * (ux * ux + uy * uy + uz * uz) * c.inv_cs2;
+        const R tux = ux * c.inv_cs2cfl, tuy = uy * c.inv_cs2cfl, tuz = uz * c.inv_cs2cfl;
         const R uF = ux * fx + uy * fy + uz * fz;
-        {
-            const R fe0 = (R)w_of(0) * (drho - rho * usq);
-            const R fpop0 = -((R)w_of(0) * inv_cs2) * uF;
-            Store<T>::st(fb + node, f[0] - relax(rp_hi, rp_lo, f[0] - fe0) + dt * sp * fpop0);
+        R WR[4], PK[4], QK[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            WR[k] = c.w[k] * rho;
+            PK[k] = WR[k] * usq - c.w[k] * drho;
+            QK[k] = c.c3[k] * uF;
         }
+        Store<T>::st(pp.fb[0] + node, f[0] - relax(rp_hi, rp_lo, f[0] + PK[0]) - QK[0]);
 #pragma unroll
         for (int d = 1; d < Q; d += 2) {
-            const int o = d + 1;
-            const R wd = (R)w_of(d);
-            const R cu = (R)ex_of(d) * tux + (R)ey_of(d) * tuy + (R)ez_of(d) * tuz;
-            const R eu = (R)ex_of(d) * ux + (R)ey_of(d) * uy + (R)ez_of(d) * uz;
-            const R eF = (R)ex_of(d) * fx + (R)ey_of(d) * fy + (R)ez_of(d) * fz;
-            const R fep = wd * (drho + rho * ((R)0.5 * cu * cu - usq));
-            const R fem = wd * rho * cu;
-            const R fp = (R)0.5 * (f[d] + f[o]);
-            const R fm = (R)0.5 * (f[d] - f[o]);
-            const R frp = (wd * inv_cs2) * (-uF + cflinv2 * eu * eF);
-            const R frm = (wd * inv_cs2) * (cflinv * eF);
-            const R relp = relax(rp_hi, rp_lo, fp - fep);
-            const R relm = relax(rm_hi, rm_lo, fm - fem);
-            Store<T>::st(fb + d * N + node, f[d] - (relp + relm) + dt * (sp * frp + sm * frm));
-            Store<T>::st(fb + o * N + node, f[o] - (relp - relm) + dt * (sp * frp - sm * frm));
+            const int o = d + 1, k = cls_of(d);
+            const R cu = dot_e(d, tux, tuy, tuz);
+            const R eF = dot_e(d, fx, fy, fz);
+            const R X = (R)0.5 * (f[d] + f[o]) + PK[k] - (R)0.5 * WR[k] * cu * cu;
+            const R A = relax(rp_hi, rp_lo, X) + QK[k] - c.c1[k] * cu * eF;
+            const R Y = (R)0.5 * (f[d] - f[o]) - WR[k] * cu;
+            const R B = relax(rm_hi, rm_lo, Y) - c.c2[k] * eF;
+            Store<T>::st(pp.fb[d] + node, f[d] - A - B);
+            Store<T>::st(pp.fb[o] + node, f[o] - A + B);
         }
     }
 
     // ---- g: collide (z <= NZ-2); the NZ-1 plane is written by z = NZ-2,
     // relative to q_ref(NZ-1) ----
     if (z != NZ - 1) {
-        const R cp_hi = (R)c.rate_hi[2], cp_lo = (R)c.rate_lo[2];
-        const R cm_hi = (R)c.rate_hi[3], cm_lo = (R)c.rate_lo[3];
-        const R K = (R)c.K;
-        const R ucx = ux + K * Ex, ucy = uy + K * Ey, ucz = uz + K * Ez;
-        const R usq = (R)0.5 * (ucx * ucx + ucy * ucy + ucz * ucz) * inv_cs2;
-        const R tux = ucx * inv_cs2cfl, tuy = ucy * inv_cs2cfl, tuz = ucz * inv_cs2cfl;
+        const R cp_hi = c.rate_hi[2], cp_lo = c.rate_lo[2];
+        const R cm_hi = c.rate_hi[3], cm_lo = c.rate_lo[3];
+        const R ucx = ux + c.K * Ex, ucy = uy + c.K * Ey, ucz = uz + c.K * Ez;
+        const R usq = (R)0.5 * (ucx * ucx + ucy * ucy + ucz * ucz) * c.inv_cs2;
+        const R tux = ucx * c.inv_cs2cfl, tuy = ucy * c.inv_cs2cfl, tuz = ucz * c.inv_cs2cfl;
         const bool dup = (z == NZ - 2);
-        const long long nodeup = node + c.nxy;
+        const unsigned nodeup = node + c.nxy;
         const R up = -zr.dq(-1);  // q_ref(z) - q_ref(z+1)
+        R WQ[4], PQ[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            WQ[k] = c.w[k] * charge;
+            PQ[k] = WQ[k] * usq - c.w[k] * dq;
+        }
         {
-            const R he0 = (R)w_of(0) * (dq - charge * usq);
-            const R out = h[0] - relax(cp_hi, cp_lo, h[0] - he0);
-            Store<T>::st(hb + node,
-                         z == 0 ? -out + (R)2 * (q0 - zr.qref) * (R)w_of(0) : out);
-            if (dup) Store<T>::st(hb + nodeup, out + (R)w_of(0) * up);
+            const R out = h[0] - relax(cp_hi, cp_lo, h[0] + PQ[0]);
+            Store<T>::st(pp.hb[0] + node, z == 0 ? -out + (R)2 * (c.q0 - zr.qref) * c.w[0] : out);
+            if (dup) Store<T>::st(pp.hb[0] + nodeup, out + c.w[0] * up);
         }
 #pragma unroll
         for (int d = 1; d < Q; d += 2) {
-            const int o = d + 1;
-            const R wd = (R)w_of(d);
-            const R cu = (R)ex_of(d) * tux + (R)ey_of(d) * tuy + (R)ez_of(d) * tuz;
-            const R hep = wd * (dq + charge * ((R)0.5 * cu * cu - usq));
-            const R hem = wd * charge * cu;
-            const R hp = (R)0.5 * (h[d] + h[o]);
-            const R hm = (R)0.5 * (h[d] - h[o]);
-            const R relp = relax(cp_hi, cp_lo, hp - hep);
-            const R relm = relax(cm_hi, cm_lo, hm - hem);
-            const R outd = h[d] - (relp + relm);
-            const R outo = h[o] - (relp - relm);
-            Store<T>::st(hb + d * N + node, outd);
-            Store<T>::st(hb + o * N + node, outo);
+            const int o = d + 1, k = cls_of(d);
+            const R cu = dot_e(d, tux, tuy, tuz);
+            const R X = (R)0.5 * (h[d] + h[o]) + PQ[k] - (R)0.5 * WQ[k] * cu * cu;
+            const R Y = (R)0.5 * (h[d] - h[o]) - WQ[k] * cu;
+            const R A = relax(cp_hi, cp_lo, X);
+            const R B = relax(cm_hi, cm_lo, Y);
+            const R outd = h[d] - A - B;
+            const R outo = h[o] - A + B;
+            Store<T>::st(pp.hb[d] + node, outd);
+            Store<T>::st(pp.hb[o] + node, outo);
             if (dup) {
-                Store<T>::st(hb + d * N + nodeup, outd + wd * up);
-                Store<T>::st(hb + o * N + nodeup, outo + wd * up);
+                Store<T>::st(pp.hb[d] + nodeup, outd + c.w[k] * up);
+                Store<T>::st(pp.hb[o] + nodeup, outo + c.w[k] * up);
             }
         }
     }
@@ -451,18 +448,21 @@ cudaError_t launch_lbm_step(const LbmArgs &a, const StepConst &c, int local_pops
                             bool macros, cudaStream_t s) {
     dim3 block(c.nx >= 64 ? 64 : 32, c.nx >= 64 ? 2 : 4, 1);
     dim3 grid((c.nx + block.x - 1) / block.x, (c.ny + block.y - 1) / block.y, c.nz);
-    const T *fa = (const T *)a.fa;
-    T *fb = (T *)a.fb;
-    const T *ha = (const T *)a.ha;
-    T *hb = (T *)a.hb;
+    PopPtrs<T> pp;
+    for (int d = 0; d < Q; ++d) {
+        pp.fa[d] = (const T *)a.fa + (size_t)d * c.n;
+        pp.ha[d] = (const T *)a.ha + (size_t)d * c.n;
+        pp.fb[d] = (T *)a.fb + (size_t)d * c.n;
+        pp.hb[d] = (T *)a.hb + (size_t)d * c.n;
+    }
+    const KConst<R> k = make_kconst<R>(c);
     const R *phip = (const R *)a.phip;
     R *q = (R *)a.q, *r = (R *)a.rho, *u = (R *)a.u, *v = (R *)a.v, *w = (R *)a.w;
     const bool general = local_pops || e_arrays;
-#define EHD_LAUNCH(G, M)                                                                    \
-    lbm_step_kernel<T, R, G, M><<<grid, block, 0, s>>>(fa, fb, ha, hb, phip, a.ez00, a.exa, \
-                                                       a.eya, a.eza, q, r, u, v, w,         \
-                                                       (const R *)a.zref, c, local_pops,    \
-                                                       e_arrays)
+#define EHD_LAUNCH(G, M)                                                                     \
+    lbm_step_kernel<T, R, G, M><<<grid, block, 0, s>>>(pp, phip, a.ez00, a.exa, a.eya, a.eza, \
+                                                       q, r, u, v, w, (const R *)a.zref, k,   \
+                                                       local_pops, e_arrays)
     if (general) {
         if (macros) EHD_LAUNCH(true, true);
         else EHD_LAUNCH(true, false);
@@ -573,8 +573,20 @@ __global__ void plane_mean_kernel(const double *__restrict__ rho, const double *
     }
 }
 
+// The reference values only choose what the stored deviations are relative
+// to (any choice is exact in exact arithmetic); they are picked to keep the
+// deviations small: the collector plane holds copies of the g of the plane
+// below it (LBM.cu:1173-1200), so it takes that plane's references, and the
+// injector's charge alternates about q0 (LBM.cu:1320-1348), so q_ref(0) = q0.
 template <typename R>
-__global__ void build_zref_kernel(const double *__restrict__ ref, R *__restrict__ zref, int nz) {
+__global__ void build_zref_kernel(double *__restrict__ ref, R *__restrict__ zref, int nz,
+                                  double q0) {
+    if (threadIdx.x == 0) {
+        ref[2 * (nz - 1)] = ref[2 * (nz - 2)];
+        ref[2 * (nz - 1) + 1] = ref[2 * (nz - 2) + 1];
+        ref[1] = q0;
+    }
+    __syncthreads();
     for (int z = threadIdx.x; z < nz; z += blockDim.x) {
         const int zm = z == 0 ? nz - 1 : z - 1, zp = z == nz - 1 ? 0 : z + 1;
         zref[6 * z + 0] = (R)ref[2 * z];
@@ -592,7 +604,7 @@ cudaError_t launch_plane_refs(const double *rho, const double *q, double *ref, v
     plane_mean_kernel<<<c.nz, 256, 0, s>>>(rho, q, ref, c.nxy);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    build_zref_kernel<R><<<1, 256, 0, s>>>(ref, (R *)zref, c.nz);
+    build_zref_kernel<R><<<1, 256, 0, s>>>(ref, (R *)zref, c.nz, c.q0);
     return cudaGetLastError();
 }
 template cudaError_t launch_plane_refs<float>(const double *, const double *, double *, void *,

@@ -146,7 +146,7 @@ def collect(indir: Path) -> None:
             keep = O.FIELDS if name != "config0" else ("u", "v", "w", "q", "phi")
             dt = np.float64 if name != "config0" else np.float32
             if name == "config0" and n != steps[-1]:
-                keep = ()
+                keep = ("u", "w", "q", "phi")
             for k in keep:
                 pack[f"out{n}_{k}"] = a[k].astype(dt)
                 scale = max(np.abs(a[k]).max(), 1e-300)
