@@ -8,7 +8,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/ehd.h"
+#include "ehd.h"
 #include "common.cuh"
 #include "kernels.h"
 
@@ -87,8 +87,15 @@ struct ehd_ctx {
     void *q = nullptr, *rho = nullptr, *u = nullptr, *v = nullptr, *w = nullptr;
     void *phip = nullptr;
     double *phi00 = nullptr, *ez00 = nullptr;
-    double *ref = nullptr;  // per-plane rho_ref, q_ref (FP64)
-    void *zref = nullptr;   // the step's reference table (compute type)
+    // Reference tables, indexed by buffer parity (see lbm.cu): populations in
+    // buffer p are stored against wref[p]; mean[p] holds the plane means of
+    // the state in buffer p; ktab[p] is the step kernel's table for reading
+    // buffer p and writing buffer p^1.
+    double *wref[2] = {nullptr, nullptr};
+    double *mean[2] = {nullptr, nullptr};
+    void *ktab[2] = {nullptr, nullptr};
+    float2 *psum = nullptr;
+    int psum_blocks = 0;
     double *out[9] = {};
     double **out_dev = nullptr;
     PoissonArgs pa{};
@@ -207,7 +214,8 @@ int lbm(ehd_ctx *c, bool macros) {
     a.u = c->u;
     a.v = c->v;
     a.w = c->w;
-    a.zref = c->zref;
+    a.zref = c->ktab[c->cur];
+    a.psum = c->psum;
     const int loc = c->pops_local ? 1 : 0, ea = c->e_arrays ? 1 : 0;
     cudaError_t e = cudaErrorInvalidValue;
     switch (c->prec) {
@@ -217,12 +225,22 @@ int lbm(ehd_ctx *c, bool macros) {
         case EHD_PREC_BF16: e = launch_lbm_step<__nv_bfloat16, float>(a, c->sc, loc, ea, macros, c->stream); break;
     }
     if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "LBM step launch: %s", cudaGetErrorString(e));
+    // plane means of the new state, then the references of the next step:
+    // buffer p will next be written against the means of the state it holds
+    // now (the same phase of the injector's two-step alternation)
+    const int p = c->cur;
+    e = launch_psum_reduce(c->psum, c->mean[p ^ 1], c->psum_blocks, c->sc, c->stream);
+    if (e == cudaSuccess)
+        e = c->rsize == 8 ? launch_build_tables<double>(c->mean[p], c->wref[p], c->wref[p ^ 1], c->ktab[p ^ 1], c->sc, c->stream)
+                          : launch_build_tables<float>(c->mean[p], c->wref[p], c->wref[p ^ 1], c->ktab[p ^ 1], c->sc, c->stream);
+    if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "reference tables: %s", cudaGetErrorString(e));
     c->cur ^= 1;
     c->pops_local = false;
     return EHD_OK;
 }
 
 int poisson(ehd_ctx *c) {
+    c->pa.qmean = c->mean[c->cur];
     cudaError_t e = c->prec == EHD_PREC_FP64 ? launch_poisson<double>(c->pa, c->stream)
                                              : launch_poisson<float>(c->pa, c->stream);
     if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "Poisson launch: %s", cudaGetErrorString(e));
@@ -272,15 +290,21 @@ int step_graph(ehd_ctx *c, bool macros) {
 }
 
 int after_upload(ehd_ctx *c) {
-    cudaError_t e = c->rsize == 8
-                        ? launch_plane_refs<double>(c->out[0], c->out[4], c->ref, c->zref, c->sc, c->stream)
-                        : launch_plane_refs<float>(c->out[0], c->out[4], c->ref, c->zref, c->sc, c->stream);
-    if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "plane references: %s", cudaGetErrorString(e));
+    // references of the uploaded state: its plane means, for both buffers
+    const int p = c->cur;
+    cudaError_t e = launch_fields_plane_mean(c->out[0], c->out[4], c->mean[p], c->sc, c->stream);
+    if (e == cudaSuccess)
+        e = c->rsize == 8 ? launch_build_tables<double>(c->mean[p], c->wref[p], c->wref[p], c->ktab[p ^ 1], c->sc, c->stream)
+                          : launch_build_tables<float>(c->mean[p], c->wref[p], c->wref[p], c->ktab[p ^ 1], c->sc, c->stream);
+    if (e == cudaSuccess)
+        e = c->rsize == 8 ? launch_build_tables<double>(c->mean[p], c->wref[p ^ 1], c->wref[p], c->ktab[p], c->sc, c->stream)
+                          : launch_build_tables<float>(c->mean[p], c->wref[p ^ 1], c->wref[p], c->ktab[p], c->sc, c->stream);
+    if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "reference tables: %s", cudaGetErrorString(e));
     switch (c->prec) {
-        case EHD_PREC_FP64: e = launch_init_equilibrium<double>(c->f[c->cur], c->h[c->cur], c->out, c->ref, c->sc, c->stream); break;
-        case EHD_PREC_FP32: e = launch_init_equilibrium<float>(c->f[c->cur], c->h[c->cur], c->out, c->ref, c->sc, c->stream); break;
-        case EHD_PREC_FP16: e = launch_init_equilibrium<__half>(c->f[c->cur], c->h[c->cur], c->out, c->ref, c->sc, c->stream); break;
-        default: e = launch_init_equilibrium<__nv_bfloat16>(c->f[c->cur], c->h[c->cur], c->out, c->ref, c->sc, c->stream); break;
+        case EHD_PREC_FP64: e = launch_init_equilibrium<double>(c->f[c->cur], c->h[c->cur], c->out, c->wref[p], c->sc, c->stream); break;
+        case EHD_PREC_FP32: e = launch_init_equilibrium<float>(c->f[c->cur], c->h[c->cur], c->out, c->wref[p], c->sc, c->stream); break;
+        case EHD_PREC_FP16: e = launch_init_equilibrium<__half>(c->f[c->cur], c->h[c->cur], c->out, c->wref[p], c->sc, c->stream); break;
+        default: e = launch_init_equilibrium<__nv_bfloat16>(c->f[c->cur], c->h[c->cur], c->out, c->wref[p], c->sc, c->stream); break;
     }
     if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "init_equilibrium: %s", cudaGetErrorString(e));
     e = c->prec == EHD_PREC_FP64
@@ -391,8 +415,13 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
         if ((r = dalloc(c, m, n * c->rsize))) return bail(r);
     if ((r = dalloc(c, (void **)&c->phi00, sizeof(double) * nz))) return bail(r);
     if ((r = dalloc(c, (void **)&c->ez00, sizeof(double) * nz))) return bail(r);
-    if ((r = dalloc(c, (void **)&c->ref, sizeof(double) * 2 * nz))) return bail(r);
-    if ((r = dalloc(c, &c->zref, c->rsize * 6 * nz))) return bail(r);
+    for (int i = 0; i < 2; ++i) {
+        if ((r = dalloc(c, (void **)&c->wref[i], sizeof(double) * 2 * nz))) return bail(r);
+        if ((r = dalloc(c, (void **)&c->mean[i], sizeof(double) * 2 * nz))) return bail(r);
+        if ((r = dalloc(c, &c->ktab[i], c->rsize * 10 * nz))) return bail(r);
+    }
+    c->psum_blocks = lbm_blocks_per_plane(nx, ny);
+    if ((r = dalloc(c, (void **)&c->psum, sizeof(float2) * (size_t)c->psum_blocks * nz))) return bail(r);
     for (int i = 0; i < 9; ++i)
         if ((r = dalloc(c, (void **)&c->out[i], sizeof(double) * n))) return bail(r);
     if ((r = dalloc(c, (void **)&c->out_dev, sizeof(double *) * 9))) return bail(r);
@@ -420,19 +449,17 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
     pa.py = make_plan(ny);
     const size_t nspec = (size_t)(nz - 2) * ny * pa.pitch;
     if ((r = dalloc(c, &pa.spec, nspec * c2))) return bail(r);
-    if ((r = dalloc(c, (void **)&pa.specd, nspec * sizeof(double2)))) return bail(r);
     if ((r = dalloc(c, (void **)&pa.rowsum, sizeof(double) * (size_t)(nz - 2) * ny))) return bail(r);
     if ((r = dalloc(c, (void **)&pa.planesum, sizeof(double) * nz))) return bail(r);
     void *twx = nullptr, *twy = nullptr;
     if ((r = dalloc(c, &twx, (size_t)nx * c2))) return bail(r);
     if ((r = dalloc(c, &twy, (size_t)ny * c2))) return bail(r);
-    double *kx2 = nullptr, *ky2 = nullptr;
-    if ((r = dalloc(c, (void **)&kx2, sizeof(double) * pa.nxh))) return bail(r);
-    if ((r = dalloc(c, (void **)&ky2, sizeof(double) * ny))) return bail(r);
+    const size_t nmodes = (size_t)pa.nxh * ny;
+    double *cpt = nullptr;
+    if ((r = dalloc(c, (void **)&cpt, sizeof(double) * nmodes * (size_t)(nz - 2)))) return bail(r);
     pa.twx = twx;
     pa.twy = twy;
-    pa.kx2 = kx2;
-    pa.ky2 = ky2;
+    pa.cpt = cpt;
     pa.phi00 = c->phi00;
     pa.ez00 = c->ez00;
     pa.q = c->q;
@@ -455,17 +482,32 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
         };
         EHD_CK(table(nx, twx));
         EHD_CK(table(ny, twy));
+        // Thomas pivots per mode (kx, ky): beta = 2 + (kx^2 + ky^2) dz^2 with
+        // the wavenumbers of main.cu:110-129, cp_0 = -1/beta,
+        // cp_i = 1/(-beta - cp_{i-1}); layout [i][ky*nxh + kx].
         std::vector<double> hx(pa.nxh), hy(ny);
-        for (int i = 0; i < pa.nxh; ++i) {  // main.cu:110-113
+        for (int i = 0; i < pa.nxh; ++i) {
             const double k = (double)i * 2.0 * M_PI / params->lx;
             hx[i] = k * k;
         }
-        for (int j = 0; j < ny; ++j) {  // main.cu:119-127
+        for (int j = 0; j < ny; ++j) {
             const double k = (j <= ny / 2 ? (double)j : (double)j - ny) * 2.0 * M_PI / params->ly;
             hy[j] = k * k;
         }
-        EHD_CK(cudaMemcpy(kx2, hx.data(), sizeof(double) * pa.nxh, cudaMemcpyHostToDevice));
-        EHD_CK(cudaMemcpy(ky2, hy.data(), sizeof(double) * ny, cudaMemcpyHostToDevice));
+        const int n = nz - 2;
+        const double dz2 = params->dz * params->dz;
+        std::vector<double> cp(nmodes * (size_t)n);
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < pa.nxh; ++i) {
+                const size_t m = (size_t)j * pa.nxh + i;
+                const double beta = 2.0 + (hx[i] + hy[j]) * dz2;
+                double prev = 0.0;
+                for (int z = 0; z < n; ++z) {
+                    prev = 1.0 / (-beta - prev);
+                    cp[(size_t)z * nmodes + m] = prev;
+                }
+            }
+        EHD_CK(cudaMemcpy(cpt, cp.data(), sizeof(double) * cp.size(), cudaMemcpyHostToDevice));
     }
     EHD_CK(cudaMemcpy(c->out_dev, c->out, sizeof(double *) * 9, cudaMemcpyHostToDevice));
     EHD_CK(cudaMemset(c->phip, 0, n * c->rsize));

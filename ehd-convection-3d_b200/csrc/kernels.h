@@ -14,14 +14,15 @@ struct LbmArgs {
     const double *ez00;   // per-plane Ez of the mean potential phi00
     const double *exa, *eya, *eza;  // explicit E (first step after set_fields)
     void *q, *rho, *u, *v, *w;      // macroscopic outputs (compute type)
-    const void *zref;               // per-plane reference table, 6 per plane (compute type)
+    const void *zref;               // step kernel's reference table (compute type, 10 per plane)
+    float2 *psum;                   // per-warp sums of rho and q [z][block][warp]
 };
 
 template <typename T, typename R>
 cudaError_t launch_lbm_step(const LbmArgs &a, const StepConst &c, int local_pops, int e_arrays,
                             bool macros, cudaStream_t s);
 
-// ref: per-plane {rho_ref, q_ref} in FP64
+// ref: per-plane {rho_w, q_w} in FP64 (what the stored deviations are relative to)
 template <typename T>
 cudaError_t launch_init_equilibrium(void *f, void *h, const double *const fields[9],
                                     const double *ref, const StepConst &c, cudaStream_t s);
@@ -39,11 +40,17 @@ template <typename R>
 cudaError_t launch_fields_to_compute(double *const *out_dev, void *rho, void *u, void *v,
                                      void *w, void *q, long long n, cudaStream_t s);
 
-// Per-plane means of rho and q (ref, FP64, 2 per plane) and the step's
-// reference table (zref, compute type, 6 per plane).
+// Reference tables (see lbm.cu): plane means m (FP64, {rho, q} per plane)
+// from the FP64 fields or from the step kernel's per-block sums, and the
+// step kernel's table (compute type, 10 per plane).
+cudaError_t launch_fields_plane_mean(const double *rho, const double *q, double *m,
+                                     const StepConst &c, cudaStream_t s);
+cudaError_t launch_psum_reduce(const float2 *psum, double *m, int nblk, const StepConst &c,
+                               cudaStream_t s);
 template <typename R>
-cudaError_t launch_plane_refs(const double *rho, const double *q, double *ref, void *zref,
-                              const StepConst &c, cudaStream_t s);
+cudaError_t launch_build_tables(const double *msrc, double *wdst, const double *wread,
+                                void *ktab, const StepConst &c, cudaStream_t s);
+int lbm_blocks_per_plane(int nx, int ny);
 
 // ---- Poisson solve ---------------------------------------------------------
 
@@ -55,21 +62,21 @@ struct FftPlan {
 };
 
 // Buffers and sizes of the FFT / tridiagonal Poisson solve.  spec holds the
-// x,y spectrum of the planes z = 1..NZ-2 in the compute type, specd the same
-// in FP64 for the z solve.  Layout [z-1][ky][kx], kx pitch `pitch`.
+// x,y spectrum of the planes z = 1..NZ-2 in the compute type, layout
+// [z-1][ky][kx] with kx pitch `pitch`; the z solve works on it in place.
 struct PoissonArgs {
     int nx, ny, nz, nxh, pitch;
-    int rows_per_block;  // x-row FFT batch per block
-    int cols_per_block;  // y-column FFT batch per block
+    int rows_per_block;  // x-row FFT batch per block (run-time radix path)
+    int cols_per_block;  // y-column FFT batch per block (run-time radix path)
     FftPlan px, py;
     const void *twx, *twy;   // exp(-2 pi i k/N) tables in the compute type
-    const double *kx2, *ky2; // squared wavenumbers (main.cu:110-129)
+    const double *cpt;       // Thomas pivots [z-1][ky*nxh + kx], FP64
     void *spec;              // complex compute type
-    double2 *specd;          // complex FP64
     double *rowsum;          // [z-1][y] FP64 sums of the source
     double *planesum;        // [z] FP64 sums of the source
     double *phi00, *ez00;    // [z] mean potential and its Ez
     const void *q;           // charge (compute type)
+    const double *qmean;     // plane means {rho, q} of the current state, FP64: q_m = [2z+1]
     void *phip;              // output phi' (compute type)
     double eps, voltage, dz;
 };
@@ -78,6 +85,7 @@ template <typename R>
 cudaError_t launch_poisson(const PoissonArgs &a, cudaStream_t s);
 
 size_t poisson_zsolve_smem(int nz, int threads);
+bool poisson_fast_size(int n);
 
 // ---- diagnostics ---------------------------------------------------------
 

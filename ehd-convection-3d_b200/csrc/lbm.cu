@@ -73,18 +73,23 @@ __device__ __forceinline__ R dot_e(int d, R a, R b, R c) {
     return s;
 }
 
-// Per-plane reference state.  Populations are stored as deviations from
-// w_d rho_ref(z) and w_d q_ref(z) of the plane z they are stored in; a
-// population pulled from plane z - e_z is moved to this plane's reference by
-// adding w_d (rho_ref(z - e_z) - rho_ref(z)).  Table layout per plane:
-// {rho_ref, q_ref, rho_ref(z-1)-rho_ref(z), rho_ref(z+1)-rho_ref(z),
-//  q_ref(z-1)-q_ref(z), q_ref(z+1)-q_ref(z)}, z +- 1 periodic.
+// Per-plane reference state.  Populations are stored as deviations
+// f_d - w_d rho_w(z), g_d - w_d q_w(z) from the reference (rho_w, q_w) of the
+// step that wrote them and of the plane z they are stored in.  A step reads
+// populations written against the previous step's references (rho_r, q_r) and
+// writes against its own, so a population pulled from plane z - e_z is moved
+// to this step's reference of plane z by adding w_d (rho_r(z - e_z) -
+// rho_w(z)).  The kernel table holds per plane, in the compute type:
+// {rho_w, q_w, drho[e_z = -1, 0, +1], dq[e_z = -1, 0, +1], q_w(z) - q_w(z+1),
+// unused} with drho[e] = rho_r(z - e) - rho_w(z), z - e periodic.
+constexpr int kZRefStride = 10;
+
 template <typename R>
 struct ZRef {
-    R rref, qref, dr_m, dr_p, dq_m, dq_p;
+    R rref, qref, drm, dr0, drp, dqm, dq0, dqp, up;
     // offset for a population with z-velocity e (source plane z - e)
-    __device__ __forceinline__ R dr(int e) const { return e > 0 ? dr_m : (e < 0 ? dr_p : (R)0); }
-    __device__ __forceinline__ R dq(int e) const { return e > 0 ? dq_m : (e < 0 ? dq_p : (R)0); }
+    __device__ __forceinline__ R dr(int e) const { return e > 0 ? drm : (e < 0 ? drp : dr0); }
+    __device__ __forceinline__ R dq(int e) const { return e > 0 ? dqm : (e < 0 ? dqp : dq0); }
 };
 
 // rate * x with rate = hi - lo (see StepConst::rate_hi)
@@ -95,8 +100,9 @@ __device__ __forceinline__ R relax(R hi, R lo, R x) {
 
 template <typename R>
 __device__ __forceinline__ ZRef<R> load_zref(const R *__restrict__ t, int z) {
-    const R *p = t + 6 * z;
-    return ZRef<R>{__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3), __ldg(p + 4), __ldg(p + 5)};
+    const R *p = t + kZRefStride * z;
+    return ZRef<R>{__ldg(p),     __ldg(p + 1), __ldg(p + 2), __ldg(p + 3), __ldg(p + 4),
+                   __ldg(p + 5), __ldg(p + 6), __ldg(p + 7), __ldg(p + 8)};
 }
 
 }  // namespace
@@ -123,13 +129,19 @@ lbm_step_kernel(const PopPtrs<T> pp, const R *__restrict__ phip,
                 const double *__restrict__ eya, const double *__restrict__ eza,
                 R *__restrict__ qout, R *__restrict__ rout, R *__restrict__ uout,
                 R *__restrict__ vout, R *__restrict__ wout, const R *__restrict__ zref,
-                const KConst<R> c, int local_pops, int e_arrays) {
+                float2 *__restrict__ psum, const KConst<R> c, int local_pops, int e_arrays) {
     const bool LOCAL = GENERAL && local_pops;
     const bool EARR = GENERAL && e_arrays;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z;
-    if (x >= c.nx || y >= c.ny) return;
+    const bool inside = x < c.nx && y < c.ny;
+    // lanes outside the grid work on a valid node so that the whole warp can
+    // take part in the plane sums; they store nothing
+    if (!inside) {
+        x = x < c.nx ? x : c.nx - 1;
+        y = y < c.ny ? y : c.ny - 1;
+    }
     const int NX = c.nx, NY = c.ny, NZ = c.nz;
     const unsigned node = (unsigned)x + (unsigned)NX * ((unsigned)y + (unsigned)NY * z);
     const ZRef<R> zr = load_zref(zref, z);
@@ -142,24 +154,23 @@ lbm_step_kernel(const PopPtrs<T> pp, const R *__restrict__ phip,
     R f[Q], h[Q];
 #pragma unroll
     for (int d = 0; d < Q; ++d) {
-        f[d] = Store<T>::ld(pp.fa[d] + (LOCAL ? node : pull_src(P, d)));
-        if (!LOCAL && ez_of(d) != 0) f[d] += c.w[cls_of(d)] * zr.dr(ez_of(d));
+        f[d] = Store<T>::ld(pp.fa[d] + (LOCAL ? node : pull_src(P, d))) +
+               c.w[cls_of(d)] * zr.dr(LOCAL ? 0 : ez_of(d));
     }
     if (LOCAL) {
 #pragma unroll
-        for (int d = 0; d < Q; ++d) h[d] = Store<T>::ld(pp.ha[d] + node);
+        for (int d = 0; d < Q; ++d) h[d] = Store<T>::ld(pp.ha[d] + node) + c.w[cls_of(d)] * zr.dq0;
     } else if (z == 0) {
         // g_d = -g_opp(d) + 2 q0 w_d (LBM.cu:1320-1348), on deviations
-        h[0] = Store<T>::ld(pp.ha[0] + node);
-        const R inj = (R)2 * (c.q0 - zr.qref);
+        h[0] = Store<T>::ld(pp.ha[0] + node) + c.w[0] * zr.dq0;
+        const R inj = (R)2 * (c.q0 - zr.qref) - zr.dq0;
 #pragma unroll
         for (int d = 1; d < Q; ++d)
             h[d] = -Store<T>::ld(pp.ha[opp_of(d)] + node) + inj * c.w[cls_of(d)];
     } else {
 #pragma unroll
         for (int d = 0; d < Q; ++d) {
-            h[d] = Store<T>::ld(pp.ha[d] + pull_src(P, d));
-            if (ez_of(d) != 0) h[d] += c.w[cls_of(d)] * zr.dq(ez_of(d));
+            h[d] = Store<T>::ld(pp.ha[d] + pull_src(P, d)) + c.w[cls_of(d)] * zr.dq(ez_of(d));
         }
     }
 
@@ -175,6 +186,19 @@ lbm_step_kernel(const PopPtrs<T> pp, const R *__restrict__ phip,
     }
     const R rho = zr.rref + drho;
     const R charge = zr.qref + dq;
+
+    {  // per-warp sums of rho and q (fixed order) for the next references
+        float2 v = inside ? make_float2((float)rho, (float)charge) : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+            v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+        }
+        const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+        if ((tid & 31) == 0)
+            psum[(((size_t)z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) * 4 + (tid >> 5)] = v;
+    }
+    if (!inside) return;
 
     // ---- E at this node (and at z = 1 for the injector override) ----
     R Ex, Ey, Ez;
@@ -212,17 +236,14 @@ lbm_step_kernel(const PopPtrs<T> pp, const R *__restrict__ phip,
         PullIdx P1;
         make_pull(P1, x, y, 1, NX, NY, NZ);
         const unsigned node1 = node + c.nxy;
-        R dqm = Store<T>::ld(pp.ha[0] + node1);
+        R dqm = Store<T>::ld(pp.ha[0] + node1) + c.w[0] * z1.dq0;
         R mxm = 0, mym = 0, mzm = 0;
 #pragma unroll
         for (int d = 1; d < Q; ++d) {
             const unsigned s1 = LOCAL ? node1 : pull_src(P1, d);
-            R fm = Store<T>::ld(pp.fa[d] + s1);
-            R hm = Store<T>::ld(pp.ha[d] + s1);
-            if (!LOCAL && ez_of(d) != 0) {
-                fm += c.w[cls_of(d)] * z1.dr(ez_of(d));
-                hm += c.w[cls_of(d)] * z1.dq(ez_of(d));
-            }
+            const int e = LOCAL ? 0 : ez_of(d);
+            const R fm = Store<T>::ld(pp.fa[d] + s1) + c.w[cls_of(d)] * z1.dr(e);
+            const R hm = Store<T>::ld(pp.ha[d] + s1) + c.w[cls_of(d)] * z1.dq(e);
             dqm += hm;
             if (ex_of(d)) mxm += ex_of(d) > 0 ? fm : -fm;
             if (ey_of(d)) mym += ey_of(d) > 0 ? fm : -fm;
@@ -302,7 +323,7 @@ lbm_step_kernel(const PopPtrs<T> pp, const R *__restrict__ phip,
         const R tux = ucx * c.inv_cs2cfl, tuy = ucy * c.inv_cs2cfl, tuz = ucz * c.inv_cs2cfl;
         const bool dup = (z == NZ - 2);
         const unsigned nodeup = node + c.nxy;
-        const R up = -zr.dq(-1);  // q_ref(z) - q_ref(z+1)
+        const R up = zr.up;  // q_w(z) - q_w(z+1)
         R WQ[4], PQ[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -461,8 +482,8 @@ cudaError_t launch_lbm_step(const LbmArgs &a, const StepConst &c, int local_pops
     const bool general = local_pops || e_arrays;
 #define EHD_LAUNCH(G, M)                                                                     \
     lbm_step_kernel<T, R, G, M><<<grid, block, 0, s>>>(pp, phip, a.ez00, a.exa, a.eya, a.eza, \
-                                                       q, r, u, v, w, (const R *)a.zref, k,   \
-                                                       local_pops, e_arrays)
+                                                       q, r, u, v, w, (const R *)a.zref,      \
+                                                       a.psum, k, local_pops, e_arrays)
     if (general) {
         if (macros) EHD_LAUNCH(true, true);
         else EHD_LAUNCH(true, false);
@@ -545,11 +566,13 @@ template cudaError_t launch_fields_to_compute<float>(double *const *, void *, vo
 template cudaError_t launch_fields_to_compute<double>(double *const *, void *, void *, void *,
                                                       void *, void *, long long, cudaStream_t);
 
-// Per-plane reference state from the FP64 fields: ref[2z] = mean rho,
-// ref[2z+1] = mean q over the plane (one block per plane, fixed-order FP64
-// reduction), then the compute-type table of load_zref.
-__global__ void plane_mean_kernel(const double *__restrict__ rho, const double *__restrict__ q,
-                                  double *__restrict__ ref, long long nxy) {
+// ---- reference tables -------------------------------------------------------
+
+// Plane means of rho and q from the FP64 fields: m[2z] = mean rho, m[2z+1] =
+// mean q (one block per plane, fixed-order FP64 reduction).
+__global__ void fields_plane_mean_kernel(const double *__restrict__ rho,
+                                         const double *__restrict__ q, double *__restrict__ m,
+                                         long long nxy) {
     __shared__ double sr[256], sq[256];
     const int z = blockIdx.x;
     double a = 0.0, b = 0.0;
@@ -568,48 +591,96 @@ __global__ void plane_mean_kernel(const double *__restrict__ rho, const double *
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        ref[2 * z] = sr[0] / (double)nxy;
-        ref[2 * z + 1] = sq[0] / (double)nxy;
+        m[2 * z] = sr[0] / (double)nxy;
+        m[2 * z + 1] = sq[0] / (double)nxy;
     }
 }
 
-// The reference values only choose what the stored deviations are relative
-// to (any choice is exact in exact arithmetic); they are picked to keep the
-// deviations small: the collector plane holds copies of the g of the plane
-// below it (LBM.cu:1173-1200), so it takes that plane's references, and the
-// injector's charge alternates about q0 (LBM.cu:1320-1348), so q_ref(0) = q0.
-template <typename R>
-__global__ void build_zref_kernel(double *__restrict__ ref, R *__restrict__ zref, int nz,
-                                  double q0) {
+// Plane means from the step kernel's per-block sums (fixed order).
+__global__ void psum_reduce_kernel(const float2 *__restrict__ psum, double *__restrict__ m,
+                                   int nblk, long long nxy) {
+    __shared__ double sr[256], sq[256];
+    const int z = blockIdx.x;
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
+        const float2 v = psum[(size_t)z * nblk + i];
+        a += v.x;
+        b += v.y;
+    }
+    sr[threadIdx.x] = a;
+    sq[threadIdx.x] = b;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            sr[threadIdx.x] += sr[threadIdx.x + o];
+            sq[threadIdx.x] += sq[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
     if (threadIdx.x == 0) {
-        ref[2 * (nz - 1)] = ref[2 * (nz - 2)];
-        ref[2 * (nz - 1) + 1] = ref[2 * (nz - 2) + 1];
-        ref[1] = q0;
+        m[2 * z] = sr[0] / (double)nxy;
+        m[2 * z + 1] = sq[0] / (double)nxy;
+    }
+}
+
+// wdst := the plane means msrc, except that the collector plane takes the
+// values of the plane below it, whose g it holds as copies (LBM.cu:1173-1200);
+// then the step kernel's table for reading against wread and writing against
+// wdst (layout of load_zref).  The references only choose what the stored
+// deviations are relative to; any choice is exact in exact arithmetic.
+template <typename R>
+__global__ void build_tables_kernel(const double *__restrict__ msrc, double *wdst,
+                                    const double *wread, R *__restrict__ ktab, int nz) {
+    for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+        const int zs = z == nz - 1 ? nz - 2 : z;
+        wdst[2 * z] = msrc[2 * zs];
+        wdst[2 * z + 1] = msrc[2 * zs + 1];
     }
     __syncthreads();
     for (int z = threadIdx.x; z < nz; z += blockDim.x) {
         const int zm = z == 0 ? nz - 1 : z - 1, zp = z == nz - 1 ? 0 : z + 1;
-        zref[6 * z + 0] = (R)ref[2 * z];
-        zref[6 * z + 1] = (R)ref[2 * z + 1];
-        zref[6 * z + 2] = (R)(ref[2 * zm] - ref[2 * z]);
-        zref[6 * z + 3] = (R)(ref[2 * zp] - ref[2 * z]);
-        zref[6 * z + 4] = (R)(ref[2 * zm + 1] - ref[2 * z + 1]);
-        zref[6 * z + 5] = (R)(ref[2 * zp + 1] - ref[2 * z + 1]);
+        const double rw = wdst[2 * z], qw = wdst[2 * z + 1];
+        R *k = ktab + 10 * z;
+        k[0] = (R)rw;
+        k[1] = (R)qw;
+        k[2] = (R)(wread[2 * zm] - rw);      // e_z = +1: source z - 1
+        k[3] = (R)(wread[2 * z] - rw);       // e_z = 0
+        k[4] = (R)(wread[2 * zp] - rw);      // e_z = -1: source z + 1
+        k[5] = (R)(wread[2 * zm + 1] - qw);
+        k[6] = (R)(wread[2 * z + 1] - qw);
+        k[7] = (R)(wread[2 * zp + 1] - qw);
+        k[8] = (R)(qw - wdst[2 * zp + 1]);   // copy of g into the plane above
+        k[9] = (R)0;
     }
 }
 
-template <typename R>
-cudaError_t launch_plane_refs(const double *rho, const double *q, double *ref, void *zref,
-                              const StepConst &c, cudaStream_t s) {
-    plane_mean_kernel<<<c.nz, 256, 0, s>>>(rho, q, ref, c.nxy);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    build_zref_kernel<R><<<1, 256, 0, s>>>(ref, (R *)zref, c.nz, c.q0);
+cudaError_t launch_fields_plane_mean(const double *rho, const double *q, double *m,
+                                     const StepConst &c, cudaStream_t s) {
+    fields_plane_mean_kernel<<<c.nz, 256, 0, s>>>(rho, q, m, c.nxy);
     return cudaGetLastError();
 }
-template cudaError_t launch_plane_refs<float>(const double *, const double *, double *, void *,
-                                              const StepConst &, cudaStream_t);
-template cudaError_t launch_plane_refs<double>(const double *, const double *, double *, void *,
-                                               const StepConst &, cudaStream_t);
+
+cudaError_t launch_psum_reduce(const float2 *psum, double *m, int nblk, const StepConst &c,
+                               cudaStream_t s) {
+    psum_reduce_kernel<<<c.nz, 256, 0, s>>>(psum, m, nblk, c.nxy);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_build_tables(const double *msrc, double *wdst, const double *wread,
+                                void *ktab, const StepConst &c, cudaStream_t s) {
+    build_tables_kernel<R><<<1, 256, 0, s>>>(msrc, wdst, wread, (R *)ktab, c.nz);
+    return cudaGetLastError();
+}
+template cudaError_t launch_build_tables<float>(const double *, double *, const double *, void *,
+                                                const StepConst &, cudaStream_t);
+template cudaError_t launch_build_tables<double>(const double *, double *, const double *,
+                                                 void *, const StepConst &, cudaStream_t);
+
+// number of per-warp partial sums per plane written by the step kernel
+int lbm_blocks_per_plane(int nx, int ny) {
+    const int bx = nx >= 64 ? 64 : 32, by = nx >= 64 ? 2 : 4;
+    return ((nx + bx - 1) / bx) * ((ny + by - 1) / by) * 4;
+}
 
 }  // namespace ehd

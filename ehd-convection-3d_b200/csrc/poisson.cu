@@ -9,28 +9,35 @@
 // eigenvalues (4/dz^2) sin^2(kz dz/2).  This file solves the same discrete
 // problem without the doubled, complex z transform:
 //
-//   K1 rows_fwd : per x-row, s = -q/eps, complex FFT along x in shared memory,
-//                 keep kx = 0..NX/2 (real input); FP64 row sums of s.
-//   K2 cols     : per plane, FFT along y of tiles of kx columns; the block of
-//                 the first tile also reduces the FP64 row sums to the plane
-//                 sum.  Output in FP64.
-//   K3 zsolve   : per (kx, ky), the tridiagonal system
+//   K1 rows_fwd : per x-row, s' = -(q - q_m(z))/eps (q_m: the plane's reference
+//                 charge, taken out so the FP32 transform carries only the
+//                 fluctuation), FFT along x, keep kx = 0..NX/2 (real input);
+//                 FP64 row sums of s'.
+//   K2 cols     : per plane, FFT along y of tiles of kx columns, in place; the
+//                 block of the first tile reduces the FP64 row sums to the
+//                 plane sum.
+//   K3 zsolve   : per (kx, ky) != (0,0), the tridiagonal system
 //                 phi(z-1) - (2 + k^2 dz^2) phi(z) + phi(z+1) = dz^2 s(z),
-//                 phi(0) = phi(NZ-1) = 0, by the Thomas algorithm in FP64.
-//                 The electrode voltage enters as -V/dz^2 on the plane z = 1
-//                 (poisson.cu:97), i.e. only in the (0,0) mode, whose FP64
-//                 solution is the mean potential phi00(z) (plus V at z = 0);
-//                 the (0,0) mode of the fluctuation is zeroed.
-//   K2 cols     : inverse FFT along y, output in the compute type.
+//                 phi(0) = phi(NZ-1) = 0, by the Thomas algorithm in FP64
+//                 (pivots from a table built once per context; the forward
+//                 sweep kept in shared memory), in place.
+//   K3' mean    : the (0,0) mode in FP64 from the plane sums plus NX NY q_m,
+//                 with the electrode voltage entering as -V/dz^2 on the plane
+//                 z = 1 (poisson.cu:97): the mean potential phi00(z) (V at
+//                 z = 0) and its Ez; the (0,0) mode of the fluctuation is 0.
+//   K2 cols     : inverse FFT along y.
 //   K4 rows_inv : per x-row, Hermitian completion, inverse FFT along x,
 //                 phi' = Re / (NX NY).
 //
 // phi = phi00(z) + phi'(x,y,z).  E = -grad(phi) is not stored: the step kernel
 // takes central differences of phi' and adds ez00(z), the mean-field Ez.
 //
-// FFTs are radix-2/3/4/5 Stockham autosort passes in shared memory (any
-// NX, NY of the form 2^a 3^b 5^c), twiddles from an FP64-accurate table.
+// FFTs: for N = 64, 128, 256, 512 the x and y transforms use compile-time
+// Stockham passes of radix 8/16 (fft.cuh), two real x-rows packed into one
+// complex transform; other sizes of the form 2^a 3^b 5^c use run-time
+// radix-2/3/4/5 passes.  Twiddles come from an FP64-accurate table.
 #include "common.cuh"
+#include "fft.cuh"
 #include "kernels.h"
 
 namespace ehd {
@@ -131,23 +138,20 @@ __device__ typename Cplx<R>::T *fft_smem(typename Cplx<R>::T *a, typename Cplx<R
     return a;
 }
 
-template <typename R2> __device__ __forceinline__ R2 to_c(double2 v);
-template <> __device__ __forceinline__ float2 to_c<float2>(double2 v) {
-    return make_float2((float)v.x, (float)v.y);
-}
-template <> __device__ __forceinline__ double2 to_c<double2>(double2 v) { return v; }
-__device__ __forceinline__ double2 to_d(float2 v) { return make_double2(v.x, v.y); }
-__device__ __forceinline__ double2 to_d(double2 v) { return v; }
-
 }  // namespace
 
-// K1: s = -q/eps on the planes z = 1..NZ-2 (odd_extension's interior rows,
-// poisson.cu:96-106), FFT along x, half spectrum out; FP64 row sums.
+// ---------------------------------------------------------------------------
+// run-time radix kernels (any 2^a 3^b 5^c)
+// ---------------------------------------------------------------------------
+
+// K1: s' = -(q - q_m)/eps on the planes z = 1..NZ-2 (odd_extension's interior
+// rows, poisson.cu:96-106), FFT along x, half spectrum out; FP64 row sums.
 template <typename R>
 __global__ void __launch_bounds__(256)
 poisson_rows_fwd(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec,
                  double *__restrict__ rowsum, const typename Cplx<R>::T *__restrict__ tw,
-                 FftPlan pl, int nx, int ny, int nxh, int pitch, int rows, double eps) {
+                 const double *__restrict__ qmean, FftPlan pl, int nx, int ny, int nxh, int pitch,
+                 int rows, double eps) {
     using R2 = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R2 *a = reinterpret_cast<R2 *>(smem_raw);
@@ -156,23 +160,24 @@ poisson_rows_fwd(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec
     const int y0 = blockIdx.x * rows;
     const int tid = threadIdx.x;
     const R *qp = q + (size_t)nx * ny * (zi + 1);
+    const R qm = (R)qmean[2 * (zi + 1) + 1];
     for (int t = tid; t < rows * nx; t += blockDim.x) {
         const int r = t / nx, x = t - r * nx;
         const int y = y0 + r;
         R val = 0;
-        if (y < ny) val = -qp[(size_t)nx * y + x] / (R)eps;
+        if (y < ny) val = -(qp[(size_t)nx * y + x] - qm) / (R)eps;
         a[t] = R2{val, (R)0};
     }
-    // FP64 row sums: one warp per row, fixed order
     const int warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
     for (int r = warp; r < rows; r += nwarps) {
         const int y = y0 + r;
         if (y >= ny) continue;
-        double s = 0.0;
-        for (int x = lane; x < nx; x += 32) s += -(double)qp[(size_t)nx * y + x] / eps;
+        double sum = 0.0;
+        for (int x = lane; x < nx; x += 32)
+            sum += -((double)qp[(size_t)nx * y + x] - (double)qm) / eps;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) rowsum[(size_t)zi * ny + y] = s;
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (lane == 0) rowsum[(size_t)zi * ny + y] = sum;
     }
     __syncthreads();
     R2 *res = fft_smem<R>(a, b, pl, tw, (R)-1, rows);
@@ -184,15 +189,24 @@ poisson_rows_fwd(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec
     }
 }
 
-// K2: FFT along y of `cols` kx columns of one plane.  Forward: compute-type
-// spectrum in, FP64 out, plus the FP64 plane sum.  Inverse: FP64 in,
-// compute type out.
-template <typename R, typename SrcT, typename DstT>
+// FP64 plane sum of the row sums, fixed order (one warp).
+__device__ __forceinline__ void plane_sum_warp(const double *__restrict__ rowsum,
+                                               double *__restrict__ planesum, int zi, int ny) {
+    const int lane = threadIdx.x & 31;
+    double sum = 0.0;
+    for (int y = lane; y < ny; y += 32) sum += rowsum[(size_t)zi * ny + y];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) planesum[zi + 1] = sum;
+}
+
+// K2: FFT along y of `cols` kx columns of one plane, in place; the forward
+// pass also reduces the FP64 plane sum.
+template <typename R>
 __global__ void __launch_bounds__(256)
-poisson_cols(const SrcT *__restrict__ src, DstT *__restrict__ dst,
-             const typename Cplx<R>::T *__restrict__ tw, FftPlan pl, int ny, int nxh,
-             int pitch, int cols, R sign, const double *__restrict__ rowsum,
-             double *__restrict__ planesum) {
+poisson_cols(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::T *__restrict__ tw,
+             FftPlan pl, int ny, int nxh, int pitch, int cols, R sign,
+             const double *__restrict__ rowsum, double *__restrict__ planesum) {
     using R2 = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R2 *a = reinterpret_cast<R2 *>(smem_raw);
@@ -205,97 +219,16 @@ poisson_cols(const SrcT *__restrict__ src, DstT *__restrict__ dst,
         const int y = t / cols, cidx = t - y * cols;
         const int k = k0 + cidx;
         R2 v = R2{(R)0, (R)0};
-        if (k < nxh) v = to_c<R2>(to_d(src[off + (size_t)pitch * y + k]));
+        if (k < nxh) v = spec[off + (size_t)pitch * y + k];
         a[(size_t)cidx * ny + y] = v;
     }
-    if (planesum != nullptr && blockIdx.x == 0 && tid < 32) {
-        double s = 0.0;
-        for (int y = tid; y < ny; y += 32) s += rowsum[(size_t)zi * ny + y];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (tid == 0) planesum[zi + 1] = s;
-    }
+    if (planesum != nullptr && blockIdx.x == 0 && tid < 32) plane_sum_warp(rowsum, planesum, zi, ny);
     __syncthreads();
     R2 *res = fft_smem<R>(a, b, pl, tw, sign, cols);
     for (int t = tid; t < ny * cols; t += blockDim.x) {
         const int y = t / cols, cidx = t - y * cols;
         const int k = k0 + cidx;
-        if (k < nxh) {
-            const R2 v = res[(size_t)cidx * ny + y];
-            DstT o;
-            o.x = v.x;
-            o.y = v.y;
-            dst[off + (size_t)pitch * y + k] = o;
-        }
-    }
-}
-
-// K3: Thomas algorithm per (kx, ky) mode in FP64, in place on specd.
-__global__ void poisson_zsolve(double2 *__restrict__ specd, const double *__restrict__ kx2,
-                               const double *__restrict__ ky2,
-                               const double *__restrict__ planesum,
-                               double *__restrict__ phi00, double *__restrict__ ez00, int nx,
-                               int ny, int nz, int nxh, int pitch, double dz, double voltage) {
-    extern __shared__ double cps[];  // [z][thread]
-    const int tid = threadIdx.x;
-    const int nthr = blockDim.x;
-    const long long m = (long long)blockIdx.x * nthr + tid;
-    const int n = nz - 2;  // unknowns z = 1..nz-2
-    if (m >= (long long)nxh * ny) return;
-    const int ky = (int)(m / nxh), kx = (int)(m - (long long)ky * nxh);
-    const size_t plane = (size_t)ny * pitch;
-    const size_t off = (size_t)pitch * ky + kx;
-    const double dz2 = dz * dz;
-    if (kx == 0 && ky == 0) {
-        // mean mode: planesum (FP64) plus the Dirichlet lift -V/dz^2 on z = 1,
-        // unnormalised like the forward DFT (times NX*NY).
-        const double nxy = (double)nx * (double)ny;
-        double cp_prev = 0.0, dp_prev = 0.0;
-        for (int i = 0; i < n; ++i) {
-            double d = planesum[i + 1];
-            if (i == 0) d += -voltage / dz2 * nxy;
-            d *= dz2;
-            const double cp = 1.0 / (-2.0 - cp_prev);
-            const double dp = (d - dp_prev) * cp;
-            cps[(size_t)i * nthr + tid] = cp;
-            specd[(size_t)i * plane + off] = make_double2(dp, 0.0);
-            cp_prev = cp;
-            dp_prev = dp;
-        }
-        double xn = 0.0;
-        const double norm = 1.0 / nxy;
-        phi00[nz - 1] = 0.0;
-        phi00[0] = voltage;
-        for (int i = n - 1; i >= 0; --i) {
-            const double dp = specd[(size_t)i * plane + off].x;
-            const double xi = dp - cps[(size_t)i * nthr + tid] * xn;
-            phi00[i + 1] = xi * norm;
-            specd[(size_t)i * plane + off] = make_double2(0.0, 0.0);
-            xn = xi;
-        }
-        for (int z = 1; z <= nz - 2; ++z) ez00[z] = 0.5 * (phi00[z - 1] - phi00[z + 1]) / dz;
-        ez00[0] = ez00[1];
-        ez00[nz - 1] = ez00[nz - 2];
-        return;
-    }
-    const double beta = 2.0 + (kx2[kx] + ky2[ky]) * dz2;
-    double cp_prev = 0.0, dpr = 0.0, dpi = 0.0;
-    for (int i = 0; i < n; ++i) {
-        const double2 s = specd[(size_t)i * plane + off];
-        const double cp = 1.0 / (-beta - cp_prev);
-        dpr = (s.x * dz2 - dpr) * cp;
-        dpi = (s.y * dz2 - dpi) * cp;
-        cps[(size_t)i * nthr + tid] = cp;
-        specd[(size_t)i * plane + off] = make_double2(dpr, dpi);
-        cp_prev = cp;
-    }
-    double xr = 0.0, xi = 0.0;
-    for (int i = n - 1; i >= 0; --i) {
-        const double2 dp = specd[(size_t)i * plane + off];
-        const double cp = cps[(size_t)i * nthr + tid];
-        xr = dp.x - cp * xr;
-        xi = dp.y - cp * xi;
-        specd[(size_t)i * plane + off] = make_double2(xr, xi);
+        if (k < nxh) spec[off + (size_t)pitch * y + k] = res[(size_t)cidx * ny + y];
     }
 }
 
@@ -339,9 +272,256 @@ poisson_rows_inv(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ p
     }
 }
 
-size_t poisson_zsolve_smem(int nz, int threads) {
-    return (size_t)(nz > 2 ? nz - 2 : 1) * threads * sizeof(double);
+// ---------------------------------------------------------------------------
+// compile-time radix kernels (N = 64, 128, 256, 512)
+// ---------------------------------------------------------------------------
+
+// per-transform stride in shared memory: padded, and odd in 8-byte units so
+// the transposed (column-major) accesses do not collide on one bank
+template <int N> __host__ __device__ constexpr int tstride() { return fft::padded(N) + 1; }
+template <int N> constexpr int per_block() { return 256 / fft::Plan<N>::G; }
+
+template <typename R, int N>
+__device__ __forceinline__ void load_twiddles(typename Cplx<R>::T *tws,
+                                              const typename Cplx<R>::T *__restrict__ tw) {
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tws[i] = tw[i];
 }
+
+// K1, two real rows (y, y+1) per complex transform: z = a + i b, then
+// A[k] = (Z[k] + conj Z[N-k]) / 2, B[k] = (Z[k] - conj Z[N-k]) / (2i).
+template <typename R, int N>
+__global__ void __launch_bounds__(256)
+poisson_rows_fwd_fast(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec,
+                      double *__restrict__ rowsum, const typename Cplx<R>::T *__restrict__ tw,
+                      const double *__restrict__ qmean, int ny, int nxh, int pitch, double eps) {
+    using R2 = typename Cplx<R>::T;
+    constexpr int G = fft::Plan<N>::G, TB = per_block<N>(), P = tstride<N>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *tws = reinterpret_cast<R2 *>(smem_raw);
+    R2 *buf = tws + N;
+    const int zi = blockIdx.y;
+    const int y0 = blockIdx.x * 2 * TB;
+    const int tid = threadIdx.x;
+    const R *qp = q + (size_t)N * ny * (zi + 1);
+    const R qm = (R)qmean[2 * (zi + 1) + 1];
+    const R ieps = (R)(1.0 / eps);
+    load_twiddles<R, N>(tws, tw);
+    for (int i = tid; i < TB * N; i += 256) {
+        const int tr = i / N, x = i - tr * N;
+        const int ya = y0 + 2 * tr, yb = ya + 1;
+        R a = 0, b = 0;
+        if (ya < ny) a = -(qp[(size_t)N * ya + x] - qm) * ieps;
+        if (yb < ny) b = -(qp[(size_t)N * yb + x] - qm) * ieps;
+        buf[tr * P + fft::pad(x)] = R2{a, b};
+    }
+    {  // FP64 row sums, one warp per row, fixed order
+        const int warp = tid >> 5, lane = tid & 31;
+        for (int r = warp; r < 2 * TB; r += 8) {
+            const int y = y0 + r;
+            if (y >= ny) continue;
+            double sum = 0.0;
+            for (int x = lane; x < N; x += 32)
+                sum += -((double)qp[(size_t)N * y + x] - (double)qm) / eps;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            if (lane == 0) rowsum[(size_t)zi * ny + y] = sum;
+        }
+    }
+    __syncthreads();
+    const int tr = tid / G, j = tid - tr * G;
+    fft::Plan<N>::template run<-1>(buf + tr * P, tws, j);
+    R2 *sp = spec + (size_t)zi * ny * pitch;
+    for (int i = tid; i < TB * nxh; i += 256) {
+        const int t2 = i / nxh, k = i - t2 * nxh;
+        const int ya = y0 + 2 * t2, yb = ya + 1;
+        const R2 zk = buf[t2 * P + fft::pad(k)];
+        const R2 zn = buf[t2 * P + fft::pad((N - k) & (N - 1))];
+        const R2 A = R2{(R)0.5 * (zk.x + zn.x), (R)0.5 * (zk.y - zn.y)};
+        const R2 B = R2{(R)0.5 * (zk.y + zn.y), (R)0.5 * (zn.x - zk.x)};
+        if (ya < ny) sp[(size_t)pitch * ya + k] = A;
+        if (yb < ny) sp[(size_t)pitch * yb + k] = B;
+    }
+}
+
+// K2 for NY = N: tiles of TB kx columns, loaded transposed (coalesced along kx).
+template <typename R, int N, int S>
+__global__ void __launch_bounds__(256)
+poisson_cols_fast(typename Cplx<R>::T *__restrict__ spec,
+                  const typename Cplx<R>::T *__restrict__ tw, int nxh, int pitch,
+                  const double *__restrict__ rowsum, double *__restrict__ planesum) {
+    using R2 = typename Cplx<R>::T;
+    constexpr int G = fft::Plan<N>::G, TB = per_block<N>(), P = tstride<N>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *tws = reinterpret_cast<R2 *>(smem_raw);
+    R2 *buf = tws + N;
+    const int zi = blockIdx.y;
+    const int k0 = blockIdx.x * TB;
+    const int tid = threadIdx.x;
+    const size_t off = (size_t)zi * N * pitch;
+    load_twiddles<R, N>(tws, tw);
+    for (int i = tid; i < TB * N; i += 256) {
+        const int y = i / TB, c = i - y * TB;
+        const int k = k0 + c;
+        R2 v = R2{(R)0, (R)0};
+        if (k < nxh) v = spec[off + (size_t)pitch * y + k];
+        buf[c * P + fft::pad(y)] = v;
+    }
+    if (S < 0 && blockIdx.x == 0 && tid < 32) plane_sum_warp(rowsum, planesum, zi, N);
+    __syncthreads();
+    const int tr = tid / G, j = tid - tr * G;
+    fft::Plan<N>::template run<S>(buf + tr * P, tws, j);
+    for (int i = tid; i < TB * N; i += 256) {
+        const int y = i / TB, c = i - y * TB;
+        const int k = k0 + c;
+        if (k < nxh) spec[off + (size_t)pitch * y + k] = buf[c * P + fft::pad(y)];
+    }
+}
+
+// K4 for NX = N, two rows per transform: Z = A + i B over the full length
+// (A, B Hermitian-completed; the imaginary parts of the k = 0 and k = N/2
+// bins, which a real transform ignores, are dropped), inverse FFT,
+// phi'(y) = Re Z / (NX NY), phi'(y+1) = Im Z / (NX NY).
+template <typename R, int N>
+__global__ void __launch_bounds__(256)
+poisson_rows_inv_fast(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ phip,
+                      const typename Cplx<R>::T *__restrict__ tw, int ny, int nxh, int pitch) {
+    using R2 = typename Cplx<R>::T;
+    constexpr int G = fft::Plan<N>::G, TB = per_block<N>(), P = tstride<N>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *tws = reinterpret_cast<R2 *>(smem_raw);
+    R2 *buf = tws + N;
+    const int zi = blockIdx.y;
+    const int y0 = blockIdx.x * 2 * TB;
+    const int tid = threadIdx.x;
+    const R2 *sp = spec + (size_t)zi * ny * pitch;
+    load_twiddles<R, N>(tws, tw);
+    for (int i = tid; i < TB * N; i += 256) {
+        const int tr = i / N, k = i - tr * N;
+        const int ya = y0 + 2 * tr, yb = ya + 1;
+        const bool lo = k < nxh;
+        const int kk = lo ? k : N - k;
+        R2 A = R2{(R)0, (R)0}, B = R2{(R)0, (R)0};
+        if (ya < ny) A = sp[(size_t)pitch * ya + kk];
+        if (yb < ny) B = sp[(size_t)pitch * yb + kk];
+        if (kk == 0 || kk == N / 2) {
+            A.y = 0;
+            B.y = 0;
+        }
+        if (!lo) {
+            A.y = -A.y;
+            B.y = -B.y;
+        }
+        buf[tr * P + fft::pad(k)] = R2{A.x - B.y, A.y + B.x};
+    }
+    __syncthreads();
+    const int tr = tid / G, j = tid - tr * G;
+    fft::Plan<N>::template run<1>(buf + tr * P, tws, j);
+    const R norm = (R)(1.0 / ((double)N * (double)ny));
+    R *pp = phip + (size_t)N * ny * (zi + 1);
+    for (int i = tid; i < TB * N; i += 256) {
+        const int t2 = i / N, x = i - t2 * N;
+        const int ya = y0 + 2 * t2, yb = ya + 1;
+        const R2 zv = buf[t2 * P + fft::pad(x)];
+        if (ya < ny) pp[(size_t)N * ya + x] = zv.x * norm;
+        if (yb < ny) pp[(size_t)N * yb + x] = zv.y * norm;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// z solve
+// ---------------------------------------------------------------------------
+
+// K3: per mode (kx, ky) != (0,0), Thomas in FP64 with the pivots
+// cp_i = 1/(-beta - cp_{i-1}) read from cpt[i][mode]; the forward sweep d'
+// stays in shared memory; the result overwrites the spectrum.  The (0,0)
+// entries are set to 0 (the mean mode is K3').
+template <typename R>
+__global__ void __launch_bounds__(32)
+poisson_zsolve(typename Cplx<R>::T *__restrict__ spec, const double *__restrict__ cpt, int ny,
+               int nz, int nxh, int pitch, double dz2) {
+    using R2 = typename Cplx<R>::T;
+    extern __shared__ double2 dps[];  // [i][lane]
+    const int lane = threadIdx.x;
+    const int modes = nxh * ny;
+    const int m = blockIdx.x * 32 + lane;
+    if (m >= modes) return;
+    const int n = nz - 2;
+    const int ky = m / nxh, kx = m - ky * nxh;
+    const size_t plane = (size_t)ny * pitch;
+    R2 *sp = spec + (size_t)pitch * ky + kx;
+    if (m == 0) {
+        for (int i = 0; i < n; ++i) sp[(size_t)i * plane] = R2{(R)0, (R)0};
+        return;
+    }
+    double dr = 0.0, di = 0.0;
+#pragma unroll 4
+    for (int i = 0; i < n; ++i) {
+        const R2 s = sp[(size_t)i * plane];
+        const double cp = __ldg(cpt + (size_t)i * modes + m);
+        dr = ((double)s.x * dz2 - dr) * cp;
+        di = ((double)s.y * dz2 - di) * cp;
+        dps[i * 32 + lane] = make_double2(dr, di);
+    }
+    double xr = dr, xi = di;
+    sp[(size_t)(n - 1) * plane] = R2{(R)xr, (R)xi};
+#pragma unroll 4
+    for (int i = n - 2; i >= 0; --i) {
+        const double cp = __ldg(cpt + (size_t)i * modes + m);
+        const double2 d = dps[i * 32 + lane];
+        xr = d.x - cp * xr;
+        xi = d.y - cp * xi;
+        sp[(size_t)i * plane] = R2{(R)xr, (R)xi};
+    }
+}
+
+// K3': the (0,0) mode in FP64.  Right-hand side per plane: the FP64 plane sum
+// of s' plus NX NY (-q_m/eps), and the Dirichlet lift -V/dz^2 (NX NY) on
+// z = 1; solution phi00(z) = x / (NX NY), phi00(0) = V, phi00(NZ-1) = 0 and
+// its central-difference Ez with the electrode copy (poisson.cu:44-73).
+template <typename R>
+__global__ void __launch_bounds__(32)
+poisson_mean_mode(const double *__restrict__ planesum, const double *__restrict__ qmean,
+                  const double *__restrict__ cpt, double *__restrict__ phi00,
+                  double *__restrict__ ez00, int nx, int ny, int nz, int modes, double eps,
+                  double dz, double voltage) {
+    extern __shared__ double dd[];  // [n] right-hand side, then d'
+    const int n = nz - 2;
+    const double nxy = (double)nx * (double)ny;
+    const double dz2 = dz * dz;
+    for (int i = threadIdx.x; i < n; i += 32) {
+        double d = planesum[i + 1] + nxy * (-(double)(R)qmean[2 * (i + 1) + 1] / eps);
+        if (i == 0) d += -voltage / dz2 * nxy;
+        dd[i] = d * dz2;
+    }
+    __syncwarp();
+    if (threadIdx.x == 0) {
+        double dp = 0.0;
+        for (int i = 0; i < n; ++i) {
+            dp = (dd[i] - dp) * cpt[(size_t)i * modes];
+            dd[i] = dp;
+        }
+        double x = dp;
+        phi00[n] = x / nxy;
+        for (int i = n - 2; i >= 0; --i) {
+            x = dd[i] - cpt[(size_t)i * modes] * x;
+            phi00[i + 1] = x / nxy;
+        }
+        phi00[0] = voltage;
+        phi00[nz - 1] = 0.0;
+    }
+    __syncwarp();
+    for (int z = 1 + threadIdx.x; z <= nz - 2; z += 32)
+        ez00[z] = 0.5 * (phi00[z - 1] - phi00[z + 1]) / dz;
+    __syncwarp();
+    if (threadIdx.x == 0) {
+        ez00[0] = ez00[1];
+        ez00[nz - 1] = ez00[nz - 2];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launcher
+// ---------------------------------------------------------------------------
 
 // Opt in to more than 48 KB of dynamic shared memory.  Skipped while the
 // stream is being captured into a graph: the attribute is set by the first,
@@ -356,63 +536,131 @@ static cudaError_t set_smem(K kern, size_t bytes, cudaStream_t s) {
     return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+bool poisson_fast_size(int n) { return n == 64 || n == 128 || n == 256 || n == 512; }
+
+template <typename R, int N>
+static cudaError_t rows_fwd_fast(const PoissonArgs &a, cudaStream_t s) {
+    using R2 = typename Cplx<R>::T;
+    constexpr int TB = per_block<N>();
+    const size_t sm = sizeof(R2) * ((size_t)N + (size_t)TB * tstride<N>());
+    cudaError_t e = set_smem(poisson_rows_fwd_fast<R, N>, sm, s);
+    if (e != cudaSuccess) return e;
+    dim3 grid((a.ny + 2 * TB - 1) / (2 * TB), a.nz - 2);
+    poisson_rows_fwd_fast<R, N><<<grid, 256, sm, s>>>((const R *)a.q, (R2 *)a.spec, a.rowsum,
+                                                       (const R2 *)a.twx, a.qmean,
+                                                       a.ny, a.nxh, a.pitch, a.eps);
+    return cudaGetLastError();
+}
+template <typename R, int N>
+static cudaError_t rows_inv_fast(const PoissonArgs &a, cudaStream_t s) {
+    using R2 = typename Cplx<R>::T;
+    constexpr int TB = per_block<N>();
+    const size_t sm = sizeof(R2) * ((size_t)N + (size_t)TB * tstride<N>());
+    cudaError_t e = set_smem(poisson_rows_inv_fast<R, N>, sm, s);
+    if (e != cudaSuccess) return e;
+    dim3 grid((a.ny + 2 * TB - 1) / (2 * TB), a.nz - 2);
+    poisson_rows_inv_fast<R, N><<<grid, 256, sm, s>>>((const R2 *)a.spec, (R *)a.phip,
+                                                       (const R2 *)a.twx, a.ny, a.nxh, a.pitch);
+    return cudaGetLastError();
+}
+template <typename R, int N, int S>
+static cudaError_t cols_fast(const PoissonArgs &a, cudaStream_t s) {
+    using R2 = typename Cplx<R>::T;
+    constexpr int TB = per_block<N>();
+    const size_t sm = sizeof(R2) * ((size_t)N + (size_t)TB * tstride<N>());
+    cudaError_t e = set_smem(poisson_cols_fast<R, N, S>, sm, s);
+    if (e != cudaSuccess) return e;
+    dim3 grid((a.nxh + TB - 1) / TB, a.nz - 2);
+    poisson_cols_fast<R, N, S><<<grid, 256, sm, s>>>((R2 *)a.spec, (const R2 *)a.twy, a.nxh,
+                                                      a.pitch, a.rowsum, a.planesum);
+    return cudaGetLastError();
+}
+
+template <typename R>
+static cudaError_t rows_fwd(const PoissonArgs &a, cudaStream_t s) {
+    using R2 = typename Cplx<R>::T;
+    switch (a.nx) {
+        case 64: return rows_fwd_fast<R, 64>(a, s);
+        case 128: return rows_fwd_fast<R, 128>(a, s);
+        case 256: return rows_fwd_fast<R, 256>(a, s);
+        case 512: return rows_fwd_fast<R, 512>(a, s);
+        default: break;
+    }
+    const int rows = a.rows_per_block;
+    const size_t sm = (size_t)2 * rows * a.nx * sizeof(R2);
+    cudaError_t e = set_smem(poisson_rows_fwd<R>, sm, s);
+    if (e != cudaSuccess) return e;
+    dim3 grid((a.ny + rows - 1) / rows, a.nz - 2);
+    poisson_rows_fwd<R><<<grid, 256, sm, s>>>((const R *)a.q, (R2 *)a.spec, a.rowsum,
+                                               (const R2 *)a.twx, a.qmean, a.px,
+                                               a.nx, a.ny, a.nxh, a.pitch, rows, a.eps);
+    return cudaGetLastError();
+}
+template <typename R>
+static cudaError_t rows_inv(const PoissonArgs &a, cudaStream_t s) {
+    using R2 = typename Cplx<R>::T;
+    switch (a.nx) {
+        case 64: return rows_inv_fast<R, 64>(a, s);
+        case 128: return rows_inv_fast<R, 128>(a, s);
+        case 256: return rows_inv_fast<R, 256>(a, s);
+        case 512: return rows_inv_fast<R, 512>(a, s);
+        default: break;
+    }
+    const int rows = a.rows_per_block;
+    const size_t sm = (size_t)2 * rows * a.nx * sizeof(R2);
+    cudaError_t e = set_smem(poisson_rows_inv<R>, sm, s);
+    if (e != cudaSuccess) return e;
+    dim3 grid((a.ny + rows - 1) / rows, a.nz - 2);
+    poisson_rows_inv<R><<<grid, 256, sm, s>>>((const R2 *)a.spec, (R *)a.phip,
+                                               (const R2 *)a.twx, a.px, a.nx, a.ny, a.nxh,
+                                               a.pitch, rows);
+    return cudaGetLastError();
+}
+template <typename R, int S>
+static cudaError_t cols(const PoissonArgs &a, cudaStream_t s) {
+    using R2 = typename Cplx<R>::T;
+    switch (a.ny) {
+        case 64: return cols_fast<R, 64, S>(a, s);
+        case 128: return cols_fast<R, 128, S>(a, s);
+        case 256: return cols_fast<R, 256, S>(a, s);
+        case 512: return cols_fast<R, 512, S>(a, s);
+        default: break;
+    }
+    const int cc = a.cols_per_block;
+    const size_t sm = (size_t)2 * cc * a.ny * sizeof(R2);
+    cudaError_t e = set_smem(poisson_cols<R>, sm, s);
+    if (e != cudaSuccess) return e;
+    dim3 grid((a.nxh + cc - 1) / cc, a.nz - 2);
+    poisson_cols<R><<<grid, 256, sm, s>>>((R2 *)a.spec, (const R2 *)a.twy, a.py, a.ny, a.nxh,
+                                           a.pitch, cc, (R)S, S < 0 ? a.rowsum : nullptr,
+                                           S < 0 ? a.planesum : nullptr);
+    return cudaGetLastError();
+}
+
+size_t poisson_zsolve_smem(int nz, int threads) {
+    return (size_t)(nz > 2 ? nz - 2 : 1) * threads * sizeof(double2);
+}
+
 template <typename R>
 cudaError_t launch_poisson(const PoissonArgs &a, cudaStream_t s) {
     using R2 = typename Cplx<R>::T;
     cudaError_t e;
-    const int nzi = a.nz - 2;
-    const int rows = a.rows_per_block, cols = a.cols_per_block;
-    // K1
+    if ((e = rows_fwd<R>(a, s)) != cudaSuccess) return e;
+    if ((e = cols<R, -1>(a, s)) != cudaSuccess) return e;
     {
-        const size_t sm = (size_t)2 * rows * a.nx * sizeof(R2);
-        if ((e = set_smem(poisson_rows_fwd<R>, sm, s)) != cudaSuccess) return e;
-        dim3 grid((a.ny + rows - 1) / rows, nzi);
-        poisson_rows_fwd<R><<<grid, 256, sm, s>>>((const R *)a.q, (R2 *)a.spec, a.rowsum,
-                                                   (const R2 *)a.twx, a.px, a.nx, a.ny, a.nxh,
-                                                   a.pitch, rows, a.eps);
+        const size_t sm = poisson_zsolve_smem(a.nz, 32);
+        if ((e = set_smem(poisson_zsolve<R>, sm, s)) != cudaSuccess) return e;
+        const int modes = a.nxh * a.ny;
+        poisson_zsolve<R><<<(modes + 31) / 32, 32, sm, s>>>((R2 *)a.spec, a.cpt, a.ny, a.nz,
+                                                             a.nxh, a.pitch, a.dz * a.dz);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        poisson_mean_mode<R><<<1, 32, sizeof(double) * (a.nz - 2), s>>>(
+            a.planesum, a.qmean, a.cpt, a.phi00, a.ez00, a.nx, a.ny, a.nz, modes,
+            a.eps, a.dz, a.voltage);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    // K2 forward
-    {
-        const size_t sm = (size_t)2 * cols * a.ny * sizeof(R2);
-        auto kf = poisson_cols<R, R2, double2>;
-        if ((e = set_smem(kf, sm, s)) != cudaSuccess) return e;
-        dim3 grid((a.nxh + cols - 1) / cols, nzi);
-        kf<<<grid, 256, sm, s>>>((const R2 *)a.spec, a.specd, (const R2 *)a.twy, a.py, a.ny,
-                                 a.nxh, a.pitch, cols, (R)-1, a.rowsum, a.planesum);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    }
-    // K3
-    {
-        const int thr = 64;
-        const size_t sm = poisson_zsolve_smem(a.nz, thr);
-        if ((e = set_smem(poisson_zsolve, sm, s)) != cudaSuccess) return e;
-        const long long modes = (long long)a.nxh * a.ny;
-        poisson_zsolve<<<(unsigned)((modes + thr - 1) / thr), thr, sm, s>>>(
-            a.specd, a.kx2, a.ky2, a.planesum, a.phi00, a.ez00, a.nx, a.ny, a.nz, a.nxh,
-            a.pitch, a.dz, a.voltage);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    }
-    // K2 inverse
-    {
-        const size_t sm = (size_t)2 * cols * a.ny * sizeof(R2);
-        auto ki = poisson_cols<R, double2, R2>;
-        if ((e = set_smem(ki, sm, s)) != cudaSuccess) return e;
-        dim3 grid((a.nxh + cols - 1) / cols, nzi);
-        ki<<<grid, 256, sm, s>>>(a.specd, (R2 *)a.spec, (const R2 *)a.twy, a.py, a.ny, a.nxh,
-                                 a.pitch, cols, (R)1, nullptr, nullptr);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    }
-    // K4
-    {
-        const size_t sm = (size_t)2 * rows * a.nx * sizeof(R2);
-        if ((e = set_smem(poisson_rows_inv<R>, sm, s)) != cudaSuccess) return e;
-        dim3 grid((a.ny + rows - 1) / rows, nzi);
-        poisson_rows_inv<R><<<grid, 256, sm, s>>>((const R2 *)a.spec, (R *)a.phip,
-                                                   (const R2 *)a.twx, a.px, a.nx, a.ny, a.nxh,
-                                                   a.pitch, rows);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    }
+    if ((e = cols<R, 1>(a, s)) != cudaSuccess) return e;
+    if ((e = rows_inv<R>(a, s)) != cudaSuccess) return e;
     return cudaSuccess;
 }
 
