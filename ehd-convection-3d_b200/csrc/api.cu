@@ -70,6 +70,11 @@ FftPlan make_plan(int n) {
 
 }  // namespace
 
+namespace ehd {
+// The thread's last-error message, for entry points outside this file.
+int set_error(int code, const char *msg) { return fail(code, "%s", msg); }
+}  // namespace ehd
+
 struct ehd_ctx {
     ehd_params p{};
     ehd_config cfg{};

@@ -103,4 +103,7 @@ struct DiagArgs {
 template <typename R>
 cudaError_t launch_diag(const DiagArgs &a, cudaStream_t s);
 
+// sets the calling thread's ehd_last_error message; returns code
+int set_error(int code, const char *msg);
+
 }  // namespace ehd

@@ -95,6 +95,7 @@ SIGNATURES = {
     "ehd_device_bytes": (_i, [_vp, ctypes.POINTER(ctypes.c_size_t)]),
     "ehd_params_from_groups": (_i, [ctypes.POINTER(Params)] + [ctypes.c_double] * 4),
     "ehd_groups_from_params": (_i, [ctypes.POINTER(Params)] + [_dp] * 4),
+    "ehd_poisson_noalloc": (_i, [ctypes.POINTER(Params), _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None
@@ -137,6 +138,13 @@ def params_from_groups(nx, ny, nz, lx, ly, T, M, C, Fe, lambda_f=0.25, lambda_g=
     for k, v in over.items():
         setattr(p, k, v)
     return p
+
+
+def poisson_noalloc(p: Params, q, phi, ex, ey, ez, stream=None):
+    """ehd_poisson_noalloc on device buffers given as integer device addresses
+    (e.g. torch ``tensor.data_ptr()``): q in; phi, ex, ey, ez out.  For callers
+    that cannot allocate device memory; asynchronous on `stream`."""
+    _check(lib().ehd_poisson_noalloc(ctypes.byref(p), q, phi, ex, ey, ez, stream))
 
 
 def groups_of(p: Params):

@@ -171,6 +171,30 @@ int ehd_groups_from_params(const ehd_params *p, double *T, double *M, double *C,
 
 int ehd_abi_version(void);
 
+/* --- no device allocation -------------------------------------------------- */
+
+/* Bytes of device memory held, on every GPU that loads this library, by the
+ * file-scope working array of ehd_poisson_noalloc, until the process exits. */
+#define EHD_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory (their GPU memory is owned by another framework's pool, or an
+ * allocation would synchronise a pipeline they run inside): the Poisson solve
+ * and E = -grad(phi) of one time step, FP64, on device arrays the caller owns
+ * -- q in; phi, ex, ey, ez out; NX*NY*NZ doubles each in the reference layout
+ * -- with the same discrete solution as ehd_poisson.  It calls no cudaMalloc,
+ * cudaFree or other allocating routine; its working storage is one
+ * file-scope device array of EHD_NOALLOC_SCRATCH_BYTES, so grids whose
+ * working set exceeds it are rejected with EHD_ERR_INVALID (about
+ * 128 x 128 x 129 nodes fit).  The first call on each device looks up the
+ * array's device address; make that first call before any stream capture.
+ * All calls on a device share the array and each call leaves its contents
+ * behind: calls whose GPU work overlaps (different streams, host threads)
+ * race on it.  Runs on `stream` (NULL: the legacy default stream) on the
+ * current device; asynchronous. */
+int ehd_poisson_noalloc(const ehd_params *params, const double *q, double *phi, double *ex,
+                        double *ey, double *ez, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
