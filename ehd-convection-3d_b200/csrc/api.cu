@@ -462,6 +462,7 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
     const size_t nmodes = (size_t)pa.nxh * ny;
     double *cpt = nullptr;
     if ((r = dalloc(c, (void **)&cpt, sizeof(double) * nmodes * (size_t)(nz - 2)))) return bail(r);
+    if ((r = dalloc(c, (void **)&pa.dpw, sizeof(double2) * nmodes * (size_t)(nz - 2)))) return bail(r);
     pa.twx = twx;
     pa.twy = twy;
     pa.cpt = cpt;

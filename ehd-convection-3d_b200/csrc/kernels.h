@@ -71,6 +71,7 @@ struct PoissonArgs {
     FftPlan px, py;
     const void *twx, *twy;   // exp(-2 pi i k/N) tables in the compute type
     const double *cpt;       // Thomas pivots [z-1][ky*nxh + kx], FP64
+    double2 *dpw;            // FP64 scratch of the forward sweep, same layout
     void *spec;              // complex compute type
     double *rowsum;          // [z-1][y] FP64 sums of the source
     double *planesum;        // [z] FP64 sums of the source
@@ -84,7 +85,6 @@ struct PoissonArgs {
 template <typename R>
 cudaError_t launch_poisson(const PoissonArgs &a, cudaStream_t s);
 
-size_t poisson_zsolve_smem(int nz, int threads);
 bool poisson_fast_size(int n);
 
 // ---- diagnostics ---------------------------------------------------------

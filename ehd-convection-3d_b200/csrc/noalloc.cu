@@ -130,11 +130,12 @@ extern "C" int ehd_poisson_noalloc(const ehd_params *p, const double *q, double 
     // scratch layout
     const size_t b_spec = align256(sizeof(double2) * (size_t)(nz - 2) * ny * pitch);
     const size_t b_cpt = align256(sizeof(double) * modes * (size_t)(nz - 2));
+    const size_t b_dpw = align256(sizeof(double2) * modes * (size_t)(nz - 2));
     const size_t b_twx = align256(sizeof(double2) * nx), b_twy = align256(sizeof(double2) * ny);
     const size_t b_row = align256(sizeof(double) * (size_t)(nz - 2) * ny);
     const size_t b_z = align256(sizeof(double) * nz);
     const size_t b_qm = align256(sizeof(double) * 2 * nz);
-    const size_t total = b_spec + b_cpt + b_twx + b_twy + b_row + 3 * b_z + b_qm;
+    const size_t total = b_spec + b_cpt + b_dpw + b_twx + b_twy + b_row + 3 * b_z + b_qm;
     if (total > EHD_NOALLOC_SCRATCH_BYTES || (long long)nx * ny * nz > (1LL << 31))
         return set_error(EHD_ERR_INVALID,
                          "ehd_poisson_noalloc: the grid needs more working storage than the "
@@ -178,6 +179,7 @@ extern "C" int ehd_poisson_noalloc(const ehd_params *p, const double *q, double 
     unsigned char *cur = base;
     a.spec = cur;                       cur += b_spec;
     double *cpt = (double *)cur;        cur += b_cpt;
+    a.dpw = (double2 *)cur;             cur += b_dpw;
     double2 *twx = (double2 *)cur;      cur += b_twx;
     double2 *twy = (double2 *)cur;      cur += b_twy;
     a.rowsum = (double *)cur;           cur += b_row;

@@ -19,12 +19,12 @@
 //   K3 zsolve   : per (kx, ky) != (0,0), the tridiagonal system
 //                 phi(z-1) - (2 + k^2 dz^2) phi(z) + phi(z+1) = dz^2 s(z),
 //                 phi(0) = phi(NZ-1) = 0, by the Thomas algorithm in FP64
-//                 (pivots from a table built once per context; the forward
-//                 sweep kept in shared memory), in place.
-//   K3' mean    : the (0,0) mode in FP64 from the plane sums plus NX NY q_m,
-//                 with the electrode voltage entering as -V/dz^2 on the plane
-//                 z = 1 (poisson.cu:97): the mean potential phi00(z) (V at
-//                 z = 0) and its Ez; the (0,0) mode of the fluctuation is 0.
+//                 (pivots from a table built once per context, the forward
+//                 sweep in an FP64 scratch), in place.  The (0,0) mode in
+//                 FP64 from the plane sums plus NX NY q_m, with the electrode
+//                 voltage entering as -V/dz^2 on the plane z = 1
+//                 (poisson.cu:97): the mean potential phi00(z) (V at z = 0)
+//                 and its Ez; the (0,0) mode of the fluctuation is 0.
 //   K2 cols     : inverse FFT along y.
 //   K4 rows_inv : per x-row, Hermitian completion, inverse FFT along x,
 //                 phi' = Re / (NX NY).
@@ -173,11 +173,10 @@ poisson_rows_fwd(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec
         const int y = y0 + r;
         if (y >= ny) continue;
         double sum = 0.0;
-        for (int x = lane; x < nx; x += 32)
-            sum += -((double)qp[(size_t)nx * y + x] - (double)qm) / eps;
+        for (int x = lane; x < nx; x += 32) sum += (double)qp[(size_t)nx * y + x] - (double)qm;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-        if (lane == 0) rowsum[(size_t)zi * ny + y] = sum;
+        if (lane == 0) rowsum[(size_t)zi * ny + y] = -sum / eps;
     }
     __syncthreads();
     R2 *res = fft_smem<R>(a, b, pl, tw, (R)-1, rows);
@@ -320,11 +319,10 @@ poisson_rows_fwd_fast(const R *__restrict__ q, typename Cplx<R>::T *__restrict__
             const int y = y0 + r;
             if (y >= ny) continue;
             double sum = 0.0;
-            for (int x = lane; x < N; x += 32)
-                sum += -((double)qp[(size_t)N * y + x] - (double)qm) / eps;
+            for (int x = lane; x < N; x += 32) sum += (double)qp[(size_t)N * y + x] - (double)qm;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-            if (lane == 0) rowsum[(size_t)zi * ny + y] = sum;
+            if (lane == 0) rowsum[(size_t)zi * ny + y] = -sum / eps;
         }
     }
     __syncthreads();
@@ -431,91 +429,95 @@ poisson_rows_inv_fast(const typename Cplx<R>::T *__restrict__ spec, R *__restric
 // z solve
 // ---------------------------------------------------------------------------
 
-// K3: per mode (kx, ky) != (0,0), Thomas in FP64 with the pivots
-// cp_i = 1/(-beta - cp_{i-1}) read from cpt[i][mode]; the forward sweep d'
-// stays in shared memory; the result overwrites the spectrum.  The (0,0)
-// entries are set to 0 (the mean mode is K3').
+// K3: per mode (kx, ky), the Thomas algorithm in FP64 with the pivots
+// cp_i = 1/(-beta - cp_{i-1}) read from cpt[i][mode] and the forward sweep d'
+// kept in the FP64 scratch dpw[i][mode]; loads are issued in register batches
+// of kZB planes ahead of the dependent chain.  The result overwrites the
+// spectrum.  The thread of the (0,0) mode solves the mean mode instead:
+// right-hand side per plane the FP64 plane sum of s' plus NX NY (-q_m/eps),
+// with the electrode voltage entering as -V/dz^2 (NX NY) on z = 1
+// (poisson.cu:97); phi00(z) = x / (NX NY), phi00(0) = V, phi00(NZ-1) = 0,
+// and its central-difference Ez with the electrode copy (poisson.cu:44-73).
+// The (0,0) entries of the spectrum are set to 0.
+constexpr int kZB = 8;
+
 template <typename R>
-__global__ void __launch_bounds__(32)
-poisson_zsolve(typename Cplx<R>::T *__restrict__ spec, const double *__restrict__ cpt, int ny,
-               int nz, int nxh, int pitch, double dz2) {
+__global__ void __launch_bounds__(128)
+poisson_zsolve(typename Cplx<R>::T *__restrict__ spec, const double *__restrict__ cpt,
+               double2 *__restrict__ dpw, const double *__restrict__ planesum,
+               const double *__restrict__ qmean, double *__restrict__ phi00,
+               double *__restrict__ ez00, int nx, int ny, int nz, int nxh, int pitch,
+               double dz, double eps, double voltage) {
     using R2 = typename Cplx<R>::T;
-    extern __shared__ double2 dps[];  // [i][lane]
-    const int lane = threadIdx.x;
     const int modes = nxh * ny;
-    const int m = blockIdx.x * 32 + lane;
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= modes) return;
     const int n = nz - 2;
     const int ky = m / nxh, kx = m - ky * nxh;
     const size_t plane = (size_t)ny * pitch;
     R2 *sp = spec + (size_t)pitch * ky + kx;
-    if (m == 0) {
-        for (int i = 0; i < n; ++i) sp[(size_t)i * plane] = R2{(R)0, (R)0};
-        return;
-    }
-    double dr = 0.0, di = 0.0;
-#pragma unroll 4
-    for (int i = 0; i < n; ++i) {
-        const R2 s = sp[(size_t)i * plane];
-        const double cp = __ldg(cpt + (size_t)i * modes + m);
-        dr = ((double)s.x * dz2 - dr) * cp;
-        di = ((double)s.y * dz2 - di) * cp;
-        dps[i * 32 + lane] = make_double2(dr, di);
-    }
-    double xr = dr, xi = di;
-    sp[(size_t)(n - 1) * plane] = R2{(R)xr, (R)xi};
-#pragma unroll 4
-    for (int i = n - 2; i >= 0; --i) {
-        const double cp = __ldg(cpt + (size_t)i * modes + m);
-        const double2 d = dps[i * 32 + lane];
-        xr = d.x - cp * xr;
-        xi = d.y - cp * xi;
-        sp[(size_t)i * plane] = R2{(R)xr, (R)xi};
-    }
-}
-
-// K3': the (0,0) mode in FP64.  Right-hand side per plane: the FP64 plane sum
-// of s' plus NX NY (-q_m/eps), and the Dirichlet lift -V/dz^2 (NX NY) on
-// z = 1; solution phi00(z) = x / (NX NY), phi00(0) = V, phi00(NZ-1) = 0 and
-// its central-difference Ez with the electrode copy (poisson.cu:44-73).
-template <typename R>
-__global__ void __launch_bounds__(32)
-poisson_mean_mode(const double *__restrict__ planesum, const double *__restrict__ qmean,
-                  const double *__restrict__ cpt, double *__restrict__ phi00,
-                  double *__restrict__ ez00, int nx, int ny, int nz, int modes, double eps,
-                  double dz, double voltage) {
-    extern __shared__ double dd[];  // [n] right-hand side, then d'
-    const int n = nz - 2;
-    const double nxy = (double)nx * (double)ny;
     const double dz2 = dz * dz;
-    for (int i = threadIdx.x; i < n; i += 32) {
-        double d = planesum[i + 1] + nxy * (-(double)(R)qmean[2 * (i + 1) + 1] / eps);
-        if (i == 0) d += -voltage / dz2 * nxy;
-        dd[i] = d * dz2;
-    }
-    __syncwarp();
-    if (threadIdx.x == 0) {
+    if (m == 0) {
+        const double nxy = (double)nx * (double)ny;
         double dp = 0.0;
         for (int i = 0; i < n; ++i) {
-            dp = (dd[i] - dp) * cpt[(size_t)i * modes];
-            dd[i] = dp;
+            double d = planesum[i + 1] + nxy * (-(double)(R)qmean[2 * (i + 1) + 1] / eps);
+            if (i == 0) d += -voltage / dz2 * nxy;
+            dp = (d * dz2 - dp) * cpt[(size_t)i * modes];
+            dpw[(size_t)i * modes] = make_double2(dp, 0.0);
+            sp[(size_t)i * plane] = R2{(R)0, (R)0};
         }
         double x = dp;
         phi00[n] = x / nxy;
         for (int i = n - 2; i >= 0; --i) {
-            x = dd[i] - cpt[(size_t)i * modes] * x;
+            x = dpw[(size_t)i * modes].x - cpt[(size_t)i * modes] * x;
             phi00[i + 1] = x / nxy;
         }
         phi00[0] = voltage;
         phi00[nz - 1] = 0.0;
-    }
-    __syncwarp();
-    for (int z = 1 + threadIdx.x; z <= nz - 2; z += 32)
-        ez00[z] = 0.5 * (phi00[z - 1] - phi00[z + 1]) / dz;
-    __syncwarp();
-    if (threadIdx.x == 0) {
+        for (int z = 1; z <= nz - 2; ++z) ez00[z] = 0.5 * (phi00[z - 1] - phi00[z + 1]) / dz;
         ez00[0] = ez00[1];
         ez00[nz - 1] = ez00[nz - 2];
+        return;
+    }
+    double dr = 0.0, di = 0.0;
+    for (int i0 = 0; i0 < n; i0 += kZB) {
+        R2 sv[kZB];
+        double cv[kZB];
+#pragma unroll
+        for (int j = 0; j < kZB; ++j) {
+            const int i = i0 + j < n ? i0 + j : n - 1;
+            sv[j] = sp[(size_t)i * plane];
+            cv[j] = __ldg(cpt + (size_t)i * modes + m);
+        }
+#pragma unroll
+        for (int j = 0; j < kZB; ++j) {
+            if (i0 + j < n) {
+                dr = ((double)sv[j].x * dz2 - dr) * cv[j];
+                di = ((double)sv[j].y * dz2 - di) * cv[j];
+                dpw[(size_t)(i0 + j) * modes + m] = make_double2(dr, di);
+            }
+        }
+    }
+    double xr = dr, xi = di;
+    sp[(size_t)(n - 1) * plane] = R2{(R)xr, (R)xi};
+    for (int i1 = n - 2; i1 >= 0; i1 -= kZB) {
+        double2 dv[kZB];
+        double cv[kZB];
+#pragma unroll
+        for (int j = 0; j < kZB; ++j) {
+            const int i = i1 - j >= 0 ? i1 - j : 0;
+            dv[j] = dpw[(size_t)i * modes + m];
+            cv[j] = __ldg(cpt + (size_t)i * modes + m);
+        }
+#pragma unroll
+        for (int j = 0; j < kZB; ++j) {
+            if (i1 - j >= 0) {
+                xr = dv[j].x - cv[j] * xr;
+                xi = dv[j].y - cv[j] * xi;
+                sp[(size_t)(i1 - j) * plane] = R2{(R)xr, (R)xi};
+            }
+        }
     }
 }
 
@@ -637,10 +639,6 @@ static cudaError_t cols(const PoissonArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-size_t poisson_zsolve_smem(int nz, int threads) {
-    return (size_t)(nz > 2 ? nz - 2 : 1) * threads * sizeof(double2);
-}
-
 template <typename R>
 cudaError_t launch_poisson(const PoissonArgs &a, cudaStream_t s) {
     using R2 = typename Cplx<R>::T;
@@ -648,15 +646,10 @@ cudaError_t launch_poisson(const PoissonArgs &a, cudaStream_t s) {
     if ((e = rows_fwd<R>(a, s)) != cudaSuccess) return e;
     if ((e = cols<R, -1>(a, s)) != cudaSuccess) return e;
     {
-        const size_t sm = poisson_zsolve_smem(a.nz, 32);
-        if ((e = set_smem(poisson_zsolve<R>, sm, s)) != cudaSuccess) return e;
         const int modes = a.nxh * a.ny;
-        poisson_zsolve<R><<<(modes + 31) / 32, 32, sm, s>>>((R2 *)a.spec, a.cpt, a.ny, a.nz,
-                                                             a.nxh, a.pitch, a.dz * a.dz);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        poisson_mean_mode<R><<<1, 32, sizeof(double) * (a.nz - 2), s>>>(
-            a.planesum, a.qmean, a.cpt, a.phi00, a.ez00, a.nx, a.ny, a.nz, modes,
-            a.eps, a.dz, a.voltage);
+        poisson_zsolve<R><<<(modes + 127) / 128, 128, 0, s>>>(
+            (R2 *)a.spec, a.cpt, a.dpw, a.planesum, a.qmean, a.phi00, a.ez00, a.nx, a.ny, a.nz,
+            a.nxh, a.pitch, a.dz, a.eps, a.voltage);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if ((e = cols<R, 1>(a, s)) != cudaSuccess) return e;
