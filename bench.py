@@ -48,9 +48,26 @@ def lbm_bytes_per_node(s: int, p: int) -> int:
     return 2 * 27 * 2 * s + p * (1 + 1 + 4)
 
 
-# DRAM traffic per lbm_step launch from ncu (profiles/lbm_step_fp32.md), scaled
-# to one full 256x256x129 launch; None until captured.
-NCU_TRAFFIC_BYTES = None
+# DRAM traffic (read + write) of one lbm_step launch on the full 256x256x129 grid:
+# an ncu capture of the 256x256x33 case (profiles/lbm_step_fp32_256x256x33.md)
+# scaled by the node count.
+NCU_TRAFFIC_BYTES = 3.663e9
+
+
+def reduce_max(x: float, dist=None, device="cpu") -> float:
+    """Max of x over the ranks of the process group (x itself on one rank)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mlups(world: int, steps: int, nodes: int, ms: float) -> float:
+    """Whole-job MLUPS of `world` replicas that each advanced `nodes` nodes by
+    `steps` steps, timed as the slowest rank's `ms`."""
+    return world * steps * nodes / (ms * 1e-3) / 1e6
 
 
 def load_ehd():
@@ -163,11 +180,7 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, "cuda")
 
     def device_mlups(prec, sampler_gpu=None):
         sim = ehd.Simulation(p, prec, device=local_rank, stream=stream.cuda_stream)
@@ -207,7 +220,7 @@ def run_ours(args, rank, world, local_rank):
             sim.close()
 
     ms, lbm_ms, clocks, diag = device_mlups(args.precision, sampler_gpu=local_rank)
-    value = world * K * NODES / (ms * 1e-3) / 1e6
+    value = job_mlups(world, K, NODES, ms)
     if args.no_e2e:
         if rank == 0:
             print(json.dumps({"profile_run": True, "value": round(value, 1),
@@ -247,7 +260,7 @@ def run_ours(args, rank, world, local_rank):
     sim.close()
     if rc != 0:
         raise RuntimeError("e2e API call failed: " + L.ehd_last_error().decode())
-    e2e = world * K * NODES / e2e_s / 1e6
+    e2e = job_mlups(world, K, NODES, e2e_s * 1e3)
     field_bytes = 9 * NODES * 8
 
     # ---- storage variants, same workload ----
@@ -258,7 +271,7 @@ def run_ours(args, rank, world, local_rank):
             s = {"fp16": 2, "bf16": 2, "fp64": 8}[prec]
             pf = 8 if prec == "fp64" else 4
             variants[prec] = {
-                "value": round(world * K * NODES / (vms * 1e-3) / 1e6, 1),
+                "value": round(job_mlups(world, K, NODES, vms), 1),
                 "ms_per_step": round(vms / K, 4),
                 "lbm_kernel_ms": round(vlbm, 4),
                 "lbm_kernel_gbs": round(lbm_bytes_per_node(s, pf) * NODES / (vlbm * 1e-3) / 1e9, 1),
@@ -297,7 +310,8 @@ def run_ours(args, rank, world, local_rank):
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "bytes_per_node": lbm_bytes_per_node(4, 4),
-                     "kernel_ms": round(lbm_ms, 4), "traffic": NCU_TRAFFIC_BYTES},
+                     "kernel_ms": round(lbm_ms, 4),
+                     "traffic": NCU_TRAFFIC_BYTES if (NX, NY, NZ) == (256, 256, 129) else None},
         "gpu_launches": K * KERNELS_PER_STEP,
         "clocks": clocks,
         "variants": variants,

@@ -3,6 +3,7 @@
 
 #include <cmath>
 #include <cstdarg>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -75,6 +76,12 @@ namespace ehd {
 int set_error(int code, const char *msg) { return fail(code, "%s", msg); }
 }  // namespace ehd
 
+struct ehd_ctx;
+namespace ehd {
+const ehd_params *ctx_params(const ehd_ctx *c);
+double *ctx_time(ehd_ctx *c);
+}  // namespace ehd
+
 struct ehd_ctx {
     ehd_params p{};
     ehd_config cfg{};
@@ -103,6 +110,7 @@ struct ehd_ctx {
     int psum_blocks = 0;
     double *out[9] = {};
     double **out_dev = nullptr;
+    double *prof_dev = nullptr;  // 9 x NZ profile for ehd_set_state_seeded
     PoissonArgs pa{};
     double *diag_partial = nullptr, *diag_result = nullptr, *host_diag = nullptr;
     int diag_blocks = 0;
@@ -118,6 +126,11 @@ struct ehd_ctx {
     bool use_graphs = true;
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [cur][macros]
 };
+
+namespace ehd {
+const ehd_params *ctx_params(const ehd_ctx *c) { return &c->p; }
+double *ctx_time(ehd_ctx *c) { return &c->t; }
+}  // namespace ehd
 
 namespace {
 
@@ -430,6 +443,7 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
     for (int i = 0; i < 9; ++i)
         if ((r = dalloc(c, (void **)&c->out[i], sizeof(double) * n))) return bail(r);
     if ((r = dalloc(c, (void **)&c->out_dev, sizeof(double *) * 9))) return bail(r);
+    if ((r = dalloc(c, (void **)&c->prof_dev, sizeof(double) * 9 * nz))) return bail(r);
 
     // Poisson solver set-up: replaces cufftPlan3d and the wavenumber tables
     // (main.cu:104-143)
@@ -694,6 +708,192 @@ int ehd_current(ehd_ctx *c, double *current) {
     int r = ehd_diagnostics(c, &d);
     if (r != EHD_OK) return r;
     *current = d.current;
+    return EHD_OK;
+}
+
+int ehd_set_state_seeded(ehd_ctx *c, const double *profile, uint64_t seed, double amp) {
+    if (!c || !profile) return fail(EHD_ERR_INVALID, "NULL argument");
+    if (!std::isfinite(amp)) return fail(EHD_ERR_INVALID, "amp not finite");
+    DeviceGuard dg(c->device);
+    EHD_CK(cudaMemcpyAsync(c->prof_dev, profile, sizeof(double) * 9 * c->p.nz,
+                           cudaMemcpyHostToDevice, c->stream));
+    cudaError_t e = launch_seeded_state(c->out_dev, c->prof_dev, (unsigned long long)seed, amp,
+                                        c->sc, c->stream);
+    if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "seeded state: %s", cudaGetErrorString(e));
+    return after_upload(c);
+}
+
+int ehd_hydrostatic_profile(const ehd_params *params, const ehd_config *config, int nsteps,
+                            double *profile, double *i0) {
+    if (!params || !profile) return fail(EHD_ERR_INVALID, "NULL argument");
+    if (nsteps < 0) return fail(EHD_ERR_INVALID, "nsteps < 0");
+    ehd_params q = *params;
+    q.nx = 1;
+    q.ny = 1;
+    q.lx = params->dx;
+    q.ly = params->dy;
+    ehd_ctx *col = nullptr;
+    int r = ehd_create(&q, config, &col);
+    if (r != EHD_OK) return r;
+    const int nz = q.nz;
+    std::vector<double> f(9 * (size_t)nz);
+    double *fp[9];
+    for (int k = 0; k < 9; ++k) fp[k] = f.data() + (size_t)k * nz;
+    ehd_diag d{};
+    if ((r = ehd_initialize(col)) == EHD_OK && (r = ehd_step(col, nsteps)) == EHD_OK &&
+        (r = ehd_get_fields(col, fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7],
+                            fp[8])) == EHD_OK)
+        r = ehd_diagnostics(col, &d);
+    ehd_destroy(col);
+    if (r != EHD_OK) return r;
+    std::memcpy(profile, f.data(), sizeof(double) * 9 * nz);
+    if (i0) *i0 = d.current * (double)params->nx * (double)params->ny;
+    return EHD_OK;
+}
+
+int ehd_run_to_saturation(ehd_ctx *c, int sample_every, double tol, int hold, int64_t max_steps,
+                          double *nu_e, int64_t *steps, int *saturated) {
+    if (!c || sample_every < 1 || hold < 1 || !(tol > 0) || max_steps < 0)
+        return fail(EHD_ERR_INVALID, "bad arguments");
+    if (c->i0 == 0.0) return fail(EHD_ERR_STATE, "reference current I0 not set");
+    double prev = 0.0;
+    int held = 0, ok = 0;
+    int64_t done = 0;
+    ehd_diag d{};
+    bool first = true;
+    while (done < max_steps) {
+        const int n = (int)std::min<int64_t>(sample_every, max_steps - done);
+        int r = ehd_step(c, n);
+        if (r == EHD_OK) r = ehd_diagnostics(c, &d);
+        if (r != EHD_OK) return r;
+        done += n;
+        if (d.nonfinite) return fail(EHD_ERR_NUMERIC, "non-finite field after %lld steps", (long long)done);
+        if (!first && std::fabs(d.nu_e - prev) <= tol * std::fabs(d.nu_e)) {
+            if (++held >= hold) {
+                ok = 1;
+                break;
+            }
+        } else {
+            held = 0;
+        }
+        prev = d.nu_e;
+        first = false;
+    }
+    if (nu_e) *nu_e = d.nu_e;
+    if (steps) *steps = done;
+    if (saturated) *saturated = ok;
+    return EHD_OK;
+}
+
+namespace {
+const char kCkptMagic[8] = {'E', 'H', 'D', 'C', 'K', 'P', 'T', '1'};
+
+struct CkptHeader {
+    char magic[8];
+    uint32_t version, precision;
+    ehd_params params;
+    int64_t step;
+    double t, i0;
+    int32_t cur, pops_local, e_arrays, pad_;
+};
+
+// device buffers of the state, in file order
+struct Blob {
+    void *ptr;
+    size_t bytes;
+};
+std::vector<Blob> state_blobs(ehd_ctx *c) {
+    const size_t n = (size_t)c->sc.n, nz = (size_t)c->p.nz;
+    std::vector<Blob> b = {
+        {c->f[c->cur], (size_t)Q * n * c->tsize}, {c->h[c->cur], (size_t)Q * n * c->tsize},
+        {c->phip, n * c->rsize}, {c->q, n * c->rsize}, {c->rho, n * c->rsize},
+        {c->u, n * c->rsize}, {c->v, n * c->rsize}, {c->w, n * c->rsize},
+        {c->phi00, nz * 8}, {c->ez00, nz * 8},
+        {c->wref[0], 2 * nz * 8}, {c->wref[1], 2 * nz * 8},
+        {c->mean[0], 2 * nz * 8}, {c->mean[1], 2 * nz * 8},
+        {c->ktab[0], 10 * nz * c->rsize}, {c->ktab[1], 10 * nz * c->rsize}};
+    if (c->e_arrays)  // the uploaded phi and E are still in use
+        for (int k = 5; k < 9; ++k) b.push_back({c->out[k], n * 8});
+    return b;
+}
+}  // namespace
+
+int ehd_checkpoint(ehd_ctx *c, const char *path) {
+    if (!c || !path) return fail(EHD_ERR_INVALID, "NULL argument");
+    if (!c->have_state) return fail(EHD_ERR_STATE, "no state to checkpoint");
+    DeviceGuard dg(c->device);
+    EHD_CK(cudaStreamSynchronize(c->stream));
+    FILE *fp = std::fopen(path, "wb");
+    if (!fp) return fail(EHD_ERR_IO, "cannot open %s for writing", path);
+    CkptHeader h{};
+    std::memcpy(h.magic, kCkptMagic, 8);
+    h.version = 1;
+    h.precision = (uint32_t)c->prec;
+    h.params = c->p;
+    h.step = c->step;
+    h.t = c->t;
+    h.i0 = c->i0;
+    h.cur = c->cur;
+    h.pops_local = c->pops_local;
+    h.e_arrays = c->e_arrays;
+    bool ok = std::fwrite(&h, sizeof(h), 1, fp) == 1;
+    std::vector<unsigned char> buf;
+    for (const Blob &b : state_blobs(c)) {
+        if (!ok) break;
+        buf.resize(b.bytes);
+        if (cudaMemcpy(buf.data(), b.ptr, b.bytes, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            std::fclose(fp);
+            return fail(EHD_ERR_CUDA, "checkpoint: device read failed");
+        }
+        const uint64_t sz = b.bytes;
+        ok = std::fwrite(&sz, sizeof(sz), 1, fp) == 1 && std::fwrite(buf.data(), 1, b.bytes, fp) == b.bytes;
+    }
+    ok = (std::fclose(fp) == 0) && ok;
+    if (!ok) return fail(EHD_ERR_IO, "checkpoint: write to %s failed", path);
+    return EHD_OK;
+}
+
+int ehd_restore(ehd_ctx *c, const char *path) {
+    if (!c || !path) return fail(EHD_ERR_INVALID, "NULL argument");
+    DeviceGuard dg(c->device);
+    FILE *fp = std::fopen(path, "rb");
+    if (!fp) return fail(EHD_ERR_IO, "cannot open %s", path);
+    CkptHeader h{};
+    if (std::fread(&h, sizeof(h), 1, fp) != 1 || std::memcmp(h.magic, kCkptMagic, 8) != 0 ||
+        h.version != 1) {
+        std::fclose(fp);
+        return fail(EHD_ERR_IO, "%s is not an ehd checkpoint", path);
+    }
+    if ((int)h.precision != c->prec || std::memcmp(&h.params, &c->p, sizeof(ehd_params)) != 0) {
+        std::fclose(fp);
+        return fail(EHD_ERR_INVALID, "checkpoint parameters or precision differ from the context's");
+    }
+    EHD_CK(cudaStreamSynchronize(c->stream));
+    c->cur = h.cur & 1;
+    c->e_arrays = h.e_arrays != 0;
+    std::vector<unsigned char> buf;
+    for (const Blob &b : state_blobs(c)) {
+        uint64_t sz = 0;
+        buf.resize(b.bytes);
+        if (std::fread(&sz, sizeof(sz), 1, fp) != 1 || sz != b.bytes ||
+            std::fread(buf.data(), 1, b.bytes, fp) != b.bytes) {
+            std::fclose(fp);
+            c->have_state = false;
+            return fail(EHD_ERR_IO, "checkpoint %s is truncated or corrupt", path);
+        }
+        if (cudaMemcpy(b.ptr, buf.data(), b.bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+            std::fclose(fp);
+            c->have_state = false;
+            return fail(EHD_ERR_CUDA, "restore: device write failed");
+        }
+    }
+    std::fclose(fp);
+    c->pops_local = h.pops_local != 0;
+    c->step = h.step;
+    c->t = h.t;
+    c->i0 = h.i0;
+    c->have_state = true;
+    c->out_valid = false;
     return EHD_OK;
 }
 

@@ -52,6 +52,12 @@ cudaError_t launch_build_tables(const double *msrc, double *wdst, const double *
                                 void *ktab, const StepConst &c, cudaStream_t s);
 int lbm_blocks_per_plane(int nx, int ny);
 
+// The nine FP64 fields from a per-plane profile [k][z] plus a seeded velocity
+// perturbation (ehd_set_state_seeded).
+cudaError_t launch_seeded_state(double *const *out_dev, const double *prof_dev,
+                                unsigned long long seed, double amp, const StepConst &c,
+                                cudaStream_t s);
+
 // ---- Poisson solve ---------------------------------------------------------
 
 constexpr int kMaxRadix = 24;
@@ -105,5 +111,13 @@ cudaError_t launch_diag(const DiagArgs &a, cudaStream_t s);
 
 // sets the calling thread's ehd_last_error message; returns code
 int set_error(int code, const char *msg);
+}  // namespace ehd
+
+struct ehd_ctx;
+struct ehd_params;
+namespace ehd {
+// a context's parameters and its physical time (for the text writers)
+const ::ehd_params *ctx_params(const ::ehd_ctx *c);
+double *ctx_time(::ehd_ctx *c);
 
 }  // namespace ehd

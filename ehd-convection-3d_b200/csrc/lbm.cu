@@ -683,4 +683,46 @@ int lbm_blocks_per_plane(int nx, int ny) {
     return ((nx + bx - 1) / bx) * ((ny + by - 1) / by) * 4;
 }
 
+// ---- seeded initial state ------------------------------------------------------
+
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long x) {
+    unsigned long long z = x + 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// out[k][i] = prof[k][z]; u, v, w at rest plus amp (2 r - 1) on the interior
+// planes, r = splitmix64(seed * 2^32 + 3 i + c) / 2^64 (53 bits).
+__global__ void seeded_state_kernel(double *const *out, const double *__restrict__ prof,
+                                    unsigned long long seed, double amp, StepConst c) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const int z = (int)(i / c.nxy);
+    const int nz = c.nz;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        double v = prof[k * nz + z];
+        if (k >= 1 && k <= 3) {
+            v = 0.0;
+            if (z > 0 && z < nz - 1 && amp != 0.0) {
+                const unsigned long long ctr =
+                    (seed << 32) + 3ULL * (unsigned long long)i + (unsigned long long)(k - 1);
+                const double r = (double)(splitmix64(ctr) >> 11) * (1.0 / 9007199254740992.0);
+                v = amp * (2.0 * r - 1.0);
+            }
+        }
+        out[k][i] = v;
+    }
+}
+
+cudaError_t launch_seeded_state(double *const *out_dev, const double *prof_dev,
+                                unsigned long long seed, double amp, const StepConst &c,
+                                cudaStream_t s) {
+    const int bs = 256;
+    seeded_state_kernel<<<(unsigned)((c.n + bs - 1) / bs), bs, 0, s>>>(out_dev, prof_dev, seed,
+                                                                       amp, c);
+    return cudaGetLastError();
+}
+
 }  // namespace ehd

@@ -96,6 +96,15 @@ SIGNATURES = {
     "ehd_params_from_groups": (_i, [ctypes.POINTER(Params)] + [ctypes.c_double] * 4),
     "ehd_groups_from_params": (_i, [ctypes.POINTER(Params)] + [_dp] * 4),
     "ehd_poisson_noalloc": (_i, [ctypes.POINTER(Params), _vp, _vp, _vp, _vp, _vp, _vp]),
+    "ehd_hydrostatic_profile": (_i, [ctypes.POINTER(Params), ctypes.POINTER(Config), _i, _dp, _dp]),
+    "ehd_set_state_seeded": (_i, [_vp, _dp, ctypes.c_uint64, ctypes.c_double]),
+    "ehd_run_to_saturation": (_i, [_vp, _i, ctypes.c_double, _i, ctypes.c_int64, _dp,
+                                   ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(_i)]),
+    "ehd_checkpoint": (_i, [_vp, ctypes.c_char_p]),
+    "ehd_restore": (_i, [_vp, ctypes.c_char_p]),
+    "ehd_write_data_end": (_i, [_vp, ctypes.c_char_p]),
+    "ehd_read_data_end": (_i, [_vp, ctypes.c_char_p]),
+    "ehd_write_tecplot": (_i, [_vp, ctypes.c_char_p, _i]),
 }
 
 _lib = None
@@ -145,6 +154,17 @@ def poisson_noalloc(p: Params, q, phi, ex, ey, ez, stream=None):
     (e.g. torch ``tensor.data_ptr()``): q in; phi, ex, ey, ez out.  For callers
     that cannot allocate device memory; asynchronous on `stream`."""
     _check(lib().ehd_poisson_noalloc(ctypes.byref(p), q, phi, ex, ey, ez, stream))
+
+
+def hydrostatic_profile(p: Params, nsteps: int, precision: str = "fp64", device: int = 0):
+    """The u = 0 steady state of the step on a 1 x 1 x NZ column after nsteps
+    steps: (profile dict of per-z arrays, I0 on the full NX x NY plane)."""
+    prof = np.empty(9 * p.nz, np.float64)
+    i0 = ctypes.c_double()
+    cfg = Config(precision=PRECISIONS[precision], device=device)
+    _check(lib().ehd_hydrostatic_profile(ctypes.byref(p), ctypes.byref(cfg), int(nsteps),
+                                         _ptr(prof), ctypes.byref(i0)))
+    return {k: prof[i * p.nz:(i + 1) * p.nz].copy() for i, k in enumerate(FIELDS)}, i0.value
 
 
 def groups_of(p: Params):
@@ -221,6 +241,35 @@ class Simulation:
         d = Diag()
         _check(lib().ehd_diagnostics(self.h, ctypes.byref(d)))
         return d.as_dict()
+
+    def set_state_seeded(self, profile: dict, seed: int = 0, amp: float = 1e-3):
+        prof = np.ascontiguousarray(np.concatenate([np.asarray(profile[k], np.float64)
+                                                    for k in FIELDS]))
+        _check(lib().ehd_set_state_seeded(self.h, _ptr(prof), int(seed), float(amp)))
+
+    def run_to_saturation(self, sample_every=1000, tol=1e-3, hold=3, max_steps=10**7):
+        nu = ctypes.c_double()
+        steps = ctypes.c_int64()
+        sat = ctypes.c_int()
+        _check(lib().ehd_run_to_saturation(self.h, int(sample_every), float(tol), int(hold),
+                                           int(max_steps), ctypes.byref(nu), ctypes.byref(steps),
+                                           ctypes.byref(sat)))
+        return {"nu_e": nu.value, "steps": steps.value, "saturated": bool(sat.value)}
+
+    def checkpoint(self, path):
+        _check(lib().ehd_checkpoint(self.h, str(path).encode()))
+
+    def restore(self, path):
+        _check(lib().ehd_restore(self.h, str(path).encode()))
+
+    def write_data_end(self, path):
+        _check(lib().ehd_write_data_end(self.h, str(path).encode()))
+
+    def read_data_end(self, path):
+        _check(lib().ehd_read_data_end(self.h, str(path).encode()))
+
+    def write_tecplot(self, path, first=True):
+        _check(lib().ehd_write_tecplot(self.h, str(path).encode(), int(bool(first))))
 
     def device_bytes(self) -> int:
         b = ctypes.c_size_t()

@@ -153,6 +153,50 @@ int ehd_set_reference_current(ehd_ctx *ctx, double i0);
 /* All scalar diagnostics, reduced on the device (blocks until done). */
 int ehd_diagnostics(ehd_ctx *ctx, ehd_diag *out);
 
+/* --- initial state, saturation, restart ----------------------------------- */
+
+/* The hydrostatic state: the u = 0 steady state of the same discrete step,
+ * found by running it on a 1 x 1 x NZ column of the grid's geometry from the
+ * reference's initialization (LBM.cu:69-96) for nsteps steps (even; the
+ * injector alternates with period 2).  profile receives 9*NZ doubles, field
+ * k at profile[k*NZ + z] in the order rho, u, v, w, q, phi, ex, ey, ez;
+ * *i0 the current of that state on the full NX x NY plane (the Nu_e
+ * normaliser).  Not in the reference, which starts from q = 0. */
+int ehd_hydrostatic_profile(const ehd_params *params, const ehd_config *config, int nsteps,
+                            double *profile, double *i0);
+
+/* Sets the state to a per-plane profile (layout of ehd_hydrostatic_profile)
+ * broadcast over x, y, at rest, plus a seeded velocity perturbation of
+ * amplitude amp on the interior planes: component c of node i is
+ * amp (2 r - 1) with r from splitmix64 of the counter seed * 2^32 + 3 i + c.
+ * Builds the equilibrium populations like ehd_set_fields.  Not in the
+ * reference (its perturbation, LBM.cu:389-415, is a disabled sinusoid). */
+int ehd_set_state_seeded(ehd_ctx *ctx, const double *profile, uint64_t seed, double amp);
+
+/* Steps until the electric Nusselt number Nu_e = I / I0 (I0 from
+ * ehd_set_reference_current) changes by less than tol relative between
+ * consecutive samples every sample_every steps, hold times in a row, or until
+ * max_steps.  *saturated tells which; *nu_e is the last sample. */
+int ehd_run_to_saturation(ehd_ctx *ctx, int sample_every, double tol, int hold,
+                          int64_t max_steps, double *nu_e, int64_t *steps, int *saturated);
+
+/* Binary checkpoint of the complete state (populations of both sets,
+ * reference tables, potential, fields, step and time) for a bit-exact
+ * resume in a context with the same parameters and precision.  Replaces the
+ * lossy save_data_end / read_data restart (LBM.cu:1506-1643), which restarts
+ * from equilibrium populations. */
+int ehd_checkpoint(ehd_ctx *ctx, const char *path);
+int ehd_restore(ehd_ctx *ctx, const char *path);
+
+/* The reference's text formats, on the host: data_end.dat (save_data_end,
+ * LBM.cu:1506-1566: ten %10.6f columns t u v w rho q phi Ex Ey Ez, rho q u v w
+ * extrapolated onto the walls), and its reader (read_data, LBM.cu:1597-1643)
+ * followed by the equilibrium rebuild; the Tecplot writer (save_data_tecplot,
+ * LBM.cu:1427-1503; first != 0 writes the VARIABLES header). */
+int ehd_write_data_end(ehd_ctx *ctx, const char *path);
+int ehd_read_data_end(ehd_ctx *ctx, const char *path);
+int ehd_write_tecplot(ehd_ctx *ctx, const char *path, int first);
+
 /* --- information -------------------------------------------------------- */
 
 /* Message of the last failed call on this thread ("" if none). */

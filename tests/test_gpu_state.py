@@ -1,0 +1,136 @@
+"""Initial state, saturation and restart through the C ABI (GPU)."""
+import numpy as np
+import pytest
+
+from conftest import O, ehd, golden, relerr
+
+pytestmark = pytest.mark.gpu
+
+
+def to_ehd(p):
+    return ehd.Params.from_dict(p.as_dict())
+
+
+def config0():
+    import make_golden as M
+    return M, M.case_params("config0"), golden("config0")
+
+
+def test_hydrostatic_profile_matches_oracle():
+    """The u = 0 steady state of the step on a 1 x 1 x NZ column, run on the
+    GPU in FP64, against the oracle's column run over the same steps
+    (stored in the config-0 fixture)."""
+    M, p, g = config0()
+    prof, i0 = ehd.hydrostatic_profile(to_ehd(p), M.hydrostatic_steps(p))
+    for k in ("rho", "q", "phi", "ez"):
+        assert relerr(prof[k], g[f"prof_{k}"]) < 1e-8, k
+    ref_i0 = O.current_of(p, np.broadcast_to(g["prof_q"][:, None, None], (p.nz, p.ny, p.nx)),
+                          np.broadcast_to(g["prof_ez"][:, None, None], (p.nz, p.ny, p.nx)))
+    assert i0 == pytest.approx(ref_i0, rel=1e-8)
+
+
+@pytest.mark.parametrize("seed", [0, 7])
+def test_seeded_state_matches_oracle_generator(seed):
+    M, p, g = config0()
+    prof = {k: g[f"prof_{k}"] for k in O.FIELDS}
+    ref = O.state_from_profile(p, prof, seed=seed, amp=1e-3)
+    with ehd.Simulation(to_ehd(p), "fp32") as sim:
+        sim.set_state_seeded(prof, seed=seed, amp=1e-3)
+        got = sim.get_fields()
+    for k in O.FIELDS:
+        assert np.array_equal(got[k], ref[k]), k
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_checkpoint_resume_is_bitexact(prec, tmp_path):
+    M, p, g = config0()
+    prof = {k: g[f"prof_{k}"] for k in O.FIELDS}
+    path = tmp_path / "state.ckpt"
+    with ehd.Simulation(to_ehd(p), prec) as a:
+        a.set_state_seeded(prof, seed=3)
+        a.step(37)
+        a.checkpoint(path)
+        a.step(25)
+        fa, da = a.get_fields(), a.diagnostics()
+    with ehd.Simulation(to_ehd(p), prec) as b:
+        b.restore(path)
+        b.step(25)
+        fb, db = b.get_fields(), b.diagnostics()
+    for k in O.FIELDS:
+        assert np.array_equal(fa[k], fb[k]), k
+    assert da == db
+
+
+def test_checkpoint_rejects_other_parameters(tmp_path):
+    M, p, g = config0()
+    prof = {k: g[f"prof_{k}"] for k in O.FIELDS}
+    path = tmp_path / "state.ckpt"
+    with ehd.Simulation(to_ehd(p), "fp32") as a:
+        a.set_state_seeded(prof)
+        a.checkpoint(path)
+    q = to_ehd(p)
+    q.nu = q.nu * 2
+    with ehd.Simulation(q, "fp32") as b:
+        with pytest.raises(ehd.EhdError):
+            b.restore(path)
+    path.write_bytes(path.read_bytes()[:1000])
+    with ehd.Simulation(to_ehd(p), "fp32") as b:
+        with pytest.raises(ehd.EhdError):
+            b.restore(path)
+
+
+def test_data_end_text_roundtrip(tmp_path):
+    """save_data_end / read_data formats (LBM.cu:1506-1643)."""
+    M, p, g = config0()
+    prof = {k: g[f"prof_{k}"] for k in O.FIELDS}
+    path = tmp_path / "data_end.dat"
+    with ehd.Simulation(to_ehd(p), "fp64") as sim:
+        sim.set_state_seeded(prof, seed=1)
+        sim.step(10)
+        ref = O.data_end_view(sim.get_fields())
+        sim.write_data_end(path)
+        a = np.loadtxt(path)
+        assert a.shape == (p.nx * p.ny * p.nz, 10)
+        assert np.allclose(a[:, 0], 10 * p.dt, atol=1e-6)
+        cols = ("u", "v", "w", "rho", "q", "phi", "ex", "ey", "ez")
+        for j, k in enumerate(cols):
+            assert np.allclose(a[:, j + 1], ref[k].ravel(), atol=6e-7, rtol=0), k
+        sim.read_data_end(path)
+        back = sim.get_fields()
+        for j, k in enumerate(cols):
+            assert np.array_equal(back[k].ravel(), a[:, j + 1]), k
+
+
+def test_tecplot_writer(tmp_path):
+    M, p, g = config0()
+    prof = {k: g[f"prof_{k}"] for k in O.FIELDS}
+    path = tmp_path / "data.dat"
+    with ehd.Simulation(to_ehd(p), "fp32") as sim:
+        sim.set_state_seeded(prof)
+        sim.write_tecplot(path, first=True)
+        sim.step(2)
+        sim.write_tecplot(path, first=False)
+    lines = path.read_text().splitlines()
+    assert lines[0].startswith('VARIABLES="x","y","z","u","v","w","p","charge","phi"')
+    assert sum(1 for s in lines if s.startswith("ZONE T=")) == 2
+    assert len(lines) == 1 + 2 * (2 + p.nx * p.ny * p.nz)
+
+
+def test_run_to_saturation_mechanics():
+    """Sampling, hold count and the step budget of ehd_run_to_saturation."""
+    M, p, g = config0()
+    prof = {k: g[f"prof_{k}"] for k in O.FIELDS}
+    i0 = O.current_of(p, np.broadcast_to(g["prof_q"][:, None, None], (p.nz, p.ny, p.nx)),
+                      np.broadcast_to(g["prof_ez"][:, None, None], (p.nz, p.ny, p.nx)))
+    with ehd.Simulation(to_ehd(p), "fp32") as sim:
+        sim.set_state_seeded(prof, amp=0.0)
+        with pytest.raises(ehd.EhdError):  # I0 not set yet
+            sim.run_to_saturation(sample_every=20, max_steps=40)
+        sim.set_reference_current(i0)
+        # a loose tolerance holds from the second sample on: 1 + 3 samples
+        r = sim.run_to_saturation(sample_every=20, tol=10.0, hold=3, max_steps=2000)
+        assert r["saturated"] and r["steps"] == 80
+        assert np.isfinite(r["nu_e"]) and r["nu_e"] > 0
+        # an impossible tolerance runs out the budget
+        r = sim.run_to_saturation(sample_every=20, tol=1e-300, hold=3, max_steps=60)
+        assert not r["saturated"] and r["steps"] == 60
