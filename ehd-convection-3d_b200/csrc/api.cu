@@ -1,6 +1,7 @@
 // api.cu -- the C ABI (include/ehd.h): context, buffers, the time step, graphs.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdint>
@@ -107,7 +108,9 @@ struct ehd_ctx {
     double *mean[2] = {nullptr, nullptr};
     void *ktab[2] = {nullptr, nullptr};
     float2 *psum = nullptr;
-    int psum_blocks = 0;
+    int psum_blocks = 0;   // psum slots per plane of the per-node kernel
+    int rows_grid = 0;     // CTAs of the bulk-copy row kernel, 0: not used
+    int *err = nullptr;    // device flag set by a row-kernel wait that gave up
     double *out[9] = {};
     double **out_dev = nullptr;
     double *prof_dev = nullptr;  // 9 x NZ profile for ehd_set_state_seeded
@@ -234,7 +237,10 @@ int lbm(ehd_ctx *c, bool macros) {
     a.w = c->w;
     a.zref = c->ktab[c->cur];
     a.psum = c->psum;
+    a.err = c->err;
     const int loc = c->pops_local ? 1 : 0, ea = c->e_arrays ? 1 : 0;
+    const bool rows = c->rows_grid > 0 && !loc && !ea;
+    a.rows_grid = rows ? c->rows_grid : 0;
     cudaError_t e = cudaErrorInvalidValue;
     switch (c->prec) {
         case EHD_PREC_FP64: e = launch_lbm_step<double, double>(a, c->sc, loc, ea, macros, c->stream); break;
@@ -247,7 +253,8 @@ int lbm(ehd_ctx *c, bool macros) {
     // buffer p will next be written against the means of the state it holds
     // now (the same phase of the injector's two-step alternation)
     const int p = c->cur;
-    e = launch_psum_reduce(c->psum, c->mean[p ^ 1], c->psum_blocks, c->sc, c->stream);
+    const int nblk = rows ? lbm_rows_slots_per_plane(c->p.nx, c->p.ny) : c->psum_blocks;
+    e = launch_psum_reduce(c->psum, c->mean[p ^ 1], nblk, c->sc, c->stream);
     if (e == cudaSuccess)
         e = c->rsize == 8 ? launch_build_tables<double>(c->mean[p], c->wref[p], c->wref[p ^ 1], c->ktab[p ^ 1], c->sc, c->stream)
                           : launch_build_tables<float>(c->mean[p], c->wref[p], c->wref[p ^ 1], c->ktab[p ^ 1], c->sc, c->stream);
@@ -273,6 +280,17 @@ void drop_graphs(ehd_ctx *c) {
                 cudaGraphExecDestroy(g);
                 g = nullptr;
             }
+}
+
+// After a stream synchronisation: a row-kernel wait that gave up leaves the
+// state invalid; report it on every later call that returns results.
+int check_device_error(ehd_ctx *c) {
+    int flag = 0;
+    EHD_CK(cudaMemcpy(&flag, c->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag)
+        return fail(EHD_ERR_CUDA,
+                    "LBM row kernel: a bulk-copy wait did not complete; the state is invalid");
+    return EHD_OK;
 }
 
 // One steady-state step (pull, E from phi) as a CUDA graph, captured once per
@@ -439,7 +457,22 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
         if ((r = dalloc(c, &c->ktab[i], c->rsize * 10 * nz))) return bail(r);
     }
     c->psum_blocks = lbm_blocks_per_plane(nx, ny);
-    if ((r = dalloc(c, (void **)&c->psum, sizeof(float2) * (size_t)c->psum_blocks * nz))) return bail(r);
+    if (!(cfg.flags & EHD_FLAG_NODE_KERNEL)) {
+        // the bulk-copy row kernel for steady-state steps, where it applies
+        cudaError_t e = cudaSuccess;
+        switch (c->prec) {
+            case EHD_PREC_FP64: e = prepare_lbm_rows<double, double>(nx, ny, nz, &c->rows_grid); break;
+            case EHD_PREC_FP32: e = prepare_lbm_rows<float, float>(nx, ny, nz, &c->rows_grid); break;
+            case EHD_PREC_FP16: e = prepare_lbm_rows<__half, float>(nx, ny, nz, &c->rows_grid); break;
+            default: e = prepare_lbm_rows<__nv_bfloat16, float>(nx, ny, nz, &c->rows_grid); break;
+        }
+        if (e != cudaSuccess) return bail(fail(EHD_ERR_CUDA, "row kernel set-up: %s", cudaGetErrorString(e)));
+    }
+    {
+        const int slots = std::max(c->psum_blocks, c->rows_grid > 0 ? lbm_rows_slots_per_plane(nx, ny) : 0);
+        if ((r = dalloc(c, (void **)&c->psum, sizeof(float2) * (size_t)slots * nz))) return bail(r);
+    }
+    if ((r = dalloc(c, (void **)&c->err, sizeof(int)))) return bail(r);
     for (int i = 0; i < 9; ++i)
         if ((r = dalloc(c, (void **)&c->out[i], sizeof(double) * n))) return bail(r);
     if ((r = dalloc(c, (void **)&c->out_dev, sizeof(double *) * 9))) return bail(r);
@@ -474,11 +507,23 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
     if ((r = dalloc(c, &twx, (size_t)nx * c2))) return bail(r);
     if ((r = dalloc(c, &twy, (size_t)ny * c2))) return bail(r);
     const size_t nmodes = (size_t)pa.nxh * ny;
+    // z solve: sine transform where 2 (nz - 1) is a compile-time FFT size,
+    // else the Thomas solve with its pivot table and sweep scratch
+    const int lz2 = 2 * (nz - 1);
+    const bool zdst = poisson_fast_size(lz2);
     double *cpt = nullptr;
-    if ((r = dalloc(c, (void **)&cpt, sizeof(double) * nmodes * (size_t)(nz - 2)))) return bail(r);
-    if ((r = dalloc(c, (void **)&pa.dpw, sizeof(double2) * nmodes * (size_t)(nz - 2)))) return bail(r);
+    void *twz = nullptr;
+    if (zdst) {
+        if ((r = dalloc(c, &twz, c->rsize * (size_t)(2 * lz2 + lz2 / 2 + 1)))) return bail(r);
+    } else {
+        if ((r = dalloc(c, (void **)&cpt, sizeof(double) * nmodes * (size_t)(nz - 2)))) return bail(r);
+        if ((r = dalloc(c, (void **)&pa.dpw, sizeof(double2) * nmodes * (size_t)(nz - 2)))) return bail(r);
+    }
     pa.twx = twx;
     pa.twy = twy;
+    pa.twz = twz;
+    pa.lx = params->lx;
+    pa.ly = params->ly;
     pa.cpt = cpt;
     pa.phi00 = c->phi00;
     pa.ez00 = c->ez00;
@@ -502,35 +547,56 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
         };
         EHD_CK(table(nx, twx));
         EHD_CK(table(ny, twy));
-        // Thomas pivots per mode (kx, ky): beta = 2 + (kx^2 + ky^2) dz^2 with
-        // the wavenumbers of main.cu:110-129, cp_0 = -1/beta,
-        // cp_i = 1/(-beta - cp_{i-1}); layout [i][ky*nxh + kx].
-        std::vector<double> hx(pa.nxh), hy(ny);
-        for (int i = 0; i < pa.nxh; ++i) {
-            const double k = (double)i * 2.0 * M_PI / params->lx;
-            hx[i] = k * k;
-        }
-        for (int j = 0; j < ny; ++j) {
-            const double k = (j <= ny / 2 ? (double)j : (double)j - ny) * 2.0 * M_PI / params->ly;
-            hy[j] = k * k;
-        }
-        const int n = nz - 2;
-        const double dz2 = params->dz * params->dz;
-        std::vector<double> cp(nmodes * (size_t)n);
-        for (int j = 0; j < ny; ++j)
-            for (int i = 0; i < pa.nxh; ++i) {
-                const size_t m = (size_t)j * pa.nxh + i;
-                const double beta = 2.0 + (hx[i] + hy[j]) * dz2;
-                double prev = 0.0;
-                for (int z = 0; z < n; ++z) {
-                    prev = 1.0 / (-beta - prev);
-                    cp[(size_t)z * nmodes + m] = prev;
-                }
+        if (zdst) {
+            // twiddles, then the z eigenvalues 4 sin^2(pi k / L), k = 0..L/2
+            std::vector<double> t(2 * (size_t)lz2 + lz2 / 2 + 1);
+            for (int k = 0; k < lz2; ++k) {
+                const double a = -2.0 * M_PI * (double)k / (double)lz2;
+                t[2 * k] = std::cos(a);
+                t[2 * k + 1] = std::sin(a);
             }
-        EHD_CK(cudaMemcpy(cpt, cp.data(), sizeof(double) * cp.size(), cudaMemcpyHostToDevice));
+            for (int k = 0; k <= lz2 / 2; ++k) {
+                const double sn = std::sin(M_PI * (double)k / (double)lz2);
+                t[2 * (size_t)lz2 + k] = 4.0 * sn * sn;
+            }
+            if (c->rsize == 8) {
+                EHD_CK(cudaMemcpy(twz, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice));
+            } else {
+                std::vector<float> tf(t.begin(), t.end());
+                EHD_CK(cudaMemcpy(twz, tf.data(), sizeof(float) * tf.size(), cudaMemcpyHostToDevice));
+            }
+        } else {
+            // Thomas pivots per mode (kx, ky): beta = 2 + (kx^2 + ky^2) dz^2 with
+            // the wavenumbers of main.cu:110-129, cp_0 = -1/beta,
+            // cp_i = 1/(-beta - cp_{i-1}); layout [i][ky*nxh + kx].
+            std::vector<double> hx(pa.nxh), hy(ny);
+            for (int i = 0; i < pa.nxh; ++i) {
+                const double k = (double)i * 2.0 * M_PI / params->lx;
+                hx[i] = k * k;
+            }
+            for (int j = 0; j < ny; ++j) {
+                const double k = (j <= ny / 2 ? (double)j : (double)j - ny) * 2.0 * M_PI / params->ly;
+                hy[j] = k * k;
+            }
+            const int n = nz - 2;
+            const double dz2 = params->dz * params->dz;
+            std::vector<double> cp(nmodes * (size_t)n);
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < pa.nxh; ++i) {
+                    const size_t m = (size_t)j * pa.nxh + i;
+                    const double beta = 2.0 + (hx[i] + hy[j]) * dz2;
+                    double prev = 0.0;
+                    for (int z = 0; z < n; ++z) {
+                        prev = 1.0 / (-beta - prev);
+                        cp[(size_t)z * nmodes + m] = prev;
+                    }
+                }
+            EHD_CK(cudaMemcpy(cpt, cp.data(), sizeof(double) * cp.size(), cudaMemcpyHostToDevice));
+        }
     }
     EHD_CK(cudaMemcpy(c->out_dev, c->out, sizeof(double *) * 9, cudaMemcpyHostToDevice));
     EHD_CK(cudaMemset(c->phip, 0, n * c->rsize));
+    EHD_CK(cudaMemset(c->err, 0, sizeof(int)));
     EHD_CK(cudaMemset(c->phi00, 0, sizeof(double) * nz));
     EHD_CK(cudaMemset(c->ez00, 0, sizeof(double) * nz));
     // diagnostics scratch
@@ -599,7 +665,7 @@ int ehd_get_fields(ehd_ctx *c, double *rho, double *u, double *v, double *w, dou
     for (int i = 0; i < 9; ++i)
         if (dst[i]) EHD_CK(cudaMemcpyAsync(dst[i], c->out[i], b, cudaMemcpyDeviceToHost, c->stream));
     EHD_CK(cudaStreamSynchronize(c->stream));
-    return EHD_OK;
+    return check_device_error(c);
 }
 
 int ehd_step(ehd_ctx *c, int nsteps) {
@@ -653,7 +719,7 @@ int ehd_synchronize(ehd_ctx *c) {
     if (!c) return fail(EHD_ERR_INVALID, "ctx is NULL");
     DeviceGuard dg(c->device);
     EHD_CK(cudaStreamSynchronize(c->stream));
-    return EHD_OK;
+    return check_device_error(c);
 }
 
 int ehd_set_reference_current(ehd_ctx *c, double i0) {
@@ -688,6 +754,7 @@ int ehd_diagnostics(ehd_ctx *c, ehd_diag *o) {
     EHD_CK(cudaMemcpyAsync(c->host_diag, c->diag_result, sizeof(double) * 5,
                            cudaMemcpyDeviceToHost, c->stream));
     EHD_CK(cudaStreamSynchronize(c->stream));
+    if (int rc = check_device_error(c)) return rc;
     const double *r = c->host_diag;
     const double dv = c->p.dx * c->p.dy * c->p.dz;
     std::memset(o, 0, sizeof(*o));

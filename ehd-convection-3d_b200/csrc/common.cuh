@@ -98,19 +98,25 @@ struct KConst {
 template <typename T> struct Store;
 template <> struct Store<double> {
     __device__ __forceinline__ static double ld(const double *p) { return __ldg(p); }
+    __device__ __forceinline__ static double lds(const double *p) { return *p; }
     __device__ __forceinline__ static void st(double *p, double v) { *p = v; }
 };
 template <> struct Store<float> {
     __device__ __forceinline__ static float ld(const float *p) { return __ldg(p); }
+    __device__ __forceinline__ static float lds(const float *p) { return *p; }
     __device__ __forceinline__ static void st(float *p, float v) { *p = v; }
 };
 template <> struct Store<__half> {
     __device__ __forceinline__ static float ld(const __half *p) { return __half2float(__ldg(p)); }
+    __device__ __forceinline__ static float lds(const __half *p) { return __half2float(*p); }
     __device__ __forceinline__ static void st(__half *p, float v) { *p = __float2half_rn(v); }
 };
 template <> struct Store<__nv_bfloat16> {
     __device__ __forceinline__ static float ld(const __nv_bfloat16 *p) {
         return __bfloat162float(__ldg(p));
+    }
+    __device__ __forceinline__ static float lds(const __nv_bfloat16 *p) {
+        return __bfloat162float(*p);
     }
     __device__ __forceinline__ static void st(__nv_bfloat16 *p, float v) {
         *p = __float2bfloat16_rn(v);

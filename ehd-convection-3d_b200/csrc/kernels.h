@@ -15,7 +15,10 @@ struct LbmArgs {
     const double *exa, *eya, *eza;  // explicit E (first step after set_fields)
     void *q, *rho, *u, *v, *w;      // macroscopic outputs (compute type)
     const void *zref;               // step kernel's reference table (compute type, 10 per plane)
-    float2 *psum;                   // per-warp sums of rho and q [z][block][warp]
+    float2 *psum;                   // per-warp sums of rho and q
+    int *err;                       // device flag: a bounded wait gave up
+    int rows_grid;                  // > 0: steady-state steps run the bulk-copy
+                                    // row kernel on this many CTAs
 };
 
 template <typename T, typename R>
@@ -51,6 +54,14 @@ template <typename R>
 cudaError_t launch_build_tables(const double *msrc, double *wdst, const double *wread,
                                 void *ktab, const StepConst &c, cudaStream_t s);
 int lbm_blocks_per_plane(int nx, int ny);
+// whether the bulk-copy row kernel serves this grid and storage type
+bool lbm_rows_usable(int nx, size_t tsize);
+// sets the row kernel's shared-memory attribute (before any stream capture)
+// and returns its persistent grid size in *grid, 0 when it does not apply
+template <typename T, typename R>
+cudaError_t prepare_lbm_rows(int nx, int ny, int nz, int *grid);
+// psum slots per plane: per-node kernel / row kernel
+int lbm_rows_slots_per_plane(int nx, int ny);
 
 // The nine FP64 fields from a per-plane profile [k][z] plus a seeded velocity
 // perturbation (ehd_set_state_seeded).
@@ -76,6 +87,10 @@ struct PoissonArgs {
     int cols_per_block;  // y-column FFT batch per block (run-time radix path)
     FftPlan px, py;
     const void *twx, *twy;   // exp(-2 pi i k/N) tables in the compute type
+    const void *twz;         // sine-transform z solve, L = 2 (nz - 1), compute type:
+                             // exp(-2 pi i k/L) (L complex), then 4 sin^2(pi k/L)
+                             // (L/2 + 1 real); nullptr: Thomas solve
+    double lx, ly;           // domain lengths (wavenumbers 2 pi k / l)
     const double *cpt;       // Thomas pivots [z-1][ky*nxh + kx], FP64
     double2 *dpw;            // FP64 scratch of the forward sweep, same layout
     void *spec;              // complex compute type

@@ -30,6 +30,8 @@
 //                 populations while z = 1 threads overwrite them; here the
 //                 rest populations are double-buffered, so the z = 0 node
 //                 always sees the pre-collision value.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -107,57 +109,32 @@ __device__ __forceinline__ ZRef<R> load_zref(const R *__restrict__ t, int z) {
 
 }  // namespace
 
-// GENERAL = false: the steady-state step (pull, E from phi).  GENERAL = true
-// adds two run-time switches used right after ehd_set_fields:
-//   local_pops: the buffers hold the pre-collision populations of each node
-//               (the reference's f1/h1 after init_equilibrium), so they are
-//               read in place, without pull or injection rule;
-//   e_arrays:   E comes from the uploaded FP64 arrays instead of phi.
-//
-// Collision algebra (LBM.cu:519-1089 rewritten on deviations, per opposite
-// pair d, o = d+1 of weight class k, s = f_d + f_o):
-//   fp - feq+  = s/2 + P_k - (w_k rho / 2) cu^2,  P_k = w_k rho usq - w_k drho
-//   fm - feq-  = (f_d - f_o)/2 - w_k rho cu
-//   A = rate+ (fp - feq+) + dt sp (w_k/cs2) uF - dt sp w_k cflinv2 CFL cu eF
-//   B = rate- (fm - feq-) - dt sm (w_k/cs2) cflinv eF
-//   f_d' = f_d - A - B,  f_o' = f_o - A + B
-// (e.u = cu cs2 CFL); the same with q, u + K E and no source for g.
-template <typename T, typename R, bool GENERAL, bool MACROS>
-__global__ void __launch_bounds__(128, sizeof(R) == 8 ? 2 : 4)
-lbm_step_kernel(const PopPtrs<T> pp, const R *__restrict__ phip,
-                const double *__restrict__ ez00, const double *__restrict__ exa,
-                const double *__restrict__ eya, const double *__restrict__ eza,
-                R *__restrict__ qout, R *__restrict__ rout, R *__restrict__ uout,
-                R *__restrict__ vout, R *__restrict__ wout, const R *__restrict__ zref,
-                float2 *__restrict__ psum, const KConst<R> c, int local_pops, int e_arrays) {
-    const bool LOCAL = GENERAL && local_pops;
-    const bool EARR = GENERAL && e_arrays;
-    int x = blockIdx.x * blockDim.x + threadIdx.x;
-    int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z;
-    const bool inside = x < c.nx && y < c.ny;
-    // lanes outside the grid work on a valid node so that the whole warp can
-    // take part in the plane sums; they store nothing
-    if (!inside) {
-        x = x < c.nx ? x : c.nx - 1;
-        y = y < c.ny ? y : c.ny - 1;
-    }
-    const int NX = c.nx, NY = c.ny, NZ = c.nz;
-    const unsigned node = (unsigned)x + (unsigned)NX * ((unsigned)y + (unsigned)NY * z);
-    const ZRef<R> zr = load_zref(zref, z);
+// Kernel arguments shared by both step kernels.
+template <typename T, typename R>
+struct StepArgs {
+    PopPtrs<T> pp;
+    const R *phip;                    // phi', zero on both electrodes
+    const double *ez00;               // mean-field Ez per plane
+    const double *exa, *eya, *eza;    // uploaded E (first step after set_fields)
+    R *qout, *rout, *uout, *vout, *wout;
+    const R *zref;                    // reference table (load_zref)
+    float2 *psum;                     // per-warp plane sums
+    int *err;                         // set to 1 if a bounded wait gives up
+};
 
-    PullIdx P;
-    make_pull(P, x, y, z, NX, NY, NZ);
-
-    // ---- pull (the reference's stream + injection rule), as deviations
-    // ft_d = f_d - w_d rho_ref(z), ht_d = g_d - w_d q_ref(z) ----
-    R f[Q], h[Q];
+// Pull of node (x, y, z) from global memory (the reference's stream and
+// injection rule), as deviations ft_d = f_d - w_d rho_w(z), ht_d = g_d -
+// w_d q_w(z).  local: the buffers hold each node's own pre-collision values.
+template <typename T, typename R>
+__device__ __forceinline__ void pull_global(R (&f)[Q], R (&h)[Q], const PopPtrs<T> &pp,
+                                            const PullIdx &P, unsigned node, int z,
+                                            const ZRef<R> &zr, const KConst<R> &c, bool local) {
 #pragma unroll
     for (int d = 0; d < Q; ++d) {
-        f[d] = Store<T>::ld(pp.fa[d] + (LOCAL ? node : pull_src(P, d))) +
-               c.w[cls_of(d)] * zr.dr(LOCAL ? 0 : ez_of(d));
+        f[d] = Store<T>::ld(pp.fa[d] + (local ? node : pull_src(P, d))) +
+               c.w[cls_of(d)] * zr.dr(local ? 0 : ez_of(d));
     }
-    if (LOCAL) {
+    if (local) {
 #pragma unroll
         for (int d = 0; d < Q; ++d) h[d] = Store<T>::ld(pp.ha[d] + node) + c.w[cls_of(d)] * zr.dq0;
     } else if (z == 0) {
@@ -169,37 +146,62 @@ lbm_step_kernel(const PopPtrs<T> pp, const R *__restrict__ phip,
             h[d] = -Store<T>::ld(pp.ha[opp_of(d)] + node) + inj * c.w[cls_of(d)];
     } else {
 #pragma unroll
-        for (int d = 0; d < Q; ++d) {
+        for (int d = 0; d < Q; ++d)
             h[d] = Store<T>::ld(pp.ha[d] + pull_src(P, d)) + c.w[cls_of(d)] * zr.dq(ez_of(d));
-        }
     }
+}
 
-    // ---- moments ----
-    R drho = 0, dq = 0, mx = 0, my = 0, mz = 0;
+template <typename R>
+struct Moments {
+    R drho, dq, mx, my, mz, rho, charge;
+};
+
+template <typename R>
+__device__ __forceinline__ Moments<R> moments(const R (&f)[Q], const R (&h)[Q], const ZRef<R> &zr) {
+    Moments<R> m{0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int d = 0; d < Q; ++d) {
-        drho += f[d];
-        dq += h[d];
-        if (ex_of(d)) mx += ex_of(d) > 0 ? f[d] : -f[d];
-        if (ey_of(d)) my += ey_of(d) > 0 ? f[d] : -f[d];
-        if (ez_of(d)) mz += ez_of(d) > 0 ? f[d] : -f[d];
+        m.drho += f[d];
+        m.dq += h[d];
+        if (ex_of(d)) m.mx += ex_of(d) > 0 ? f[d] : -f[d];
+        if (ey_of(d)) m.my += ey_of(d) > 0 ? f[d] : -f[d];
+        if (ez_of(d)) m.mz += ez_of(d) > 0 ? f[d] : -f[d];
     }
-    const R rho = zr.rref + drho;
-    const R charge = zr.qref + dq;
+    m.rho = zr.rref + m.drho;
+    m.charge = zr.qref + m.dq;
+    return m;
+}
 
-    {  // per-warp sums of rho and q (fixed order) for the next references
-        float2 v = inside ? make_float2((float)rho, (float)charge) : make_float2(0.f, 0.f);
+// Warp sum of rho and q into psum[slot] (fixed order; all 32 lanes take part).
+__device__ __forceinline__ void warp_plane_sum(float rho, float charge, float2 *psum, size_t slot) {
+    float2 v = make_float2(rho, charge);
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
-            v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
-        }
-        const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-        if ((tid & 31) == 0)
-            psum[(((size_t)z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) * 4 + (tid >> 5)] = v;
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
     }
-    if (!inside) return;
+    if ((threadIdx.x & 31) == 0) psum[slot] = v;
+}
 
+// Everything after the moments: E, the injector override, the macroscopic
+// outputs, the TRT collisions of f and g and the wall rules on store.
+//
+// Collision algebra (LBM.cu:519-1089 rewritten on deviations, per opposite
+// pair d, o = d+1 of weight class k, s = f_d + f_o):
+//   fp - feq+  = s/2 + P_k - (w_k rho / 2) cu^2,  P_k = w_k rho usq - w_k drho
+//   fm - feq-  = (f_d - f_o)/2 - w_k rho cu
+//   A = rate+ (fp - feq+) + dt sp (w_k/cs2) uF - dt sp w_k cflinv2 CFL cu eF
+//   B = rate- (fm - feq-) - dt sm (w_k/cs2) cflinv eF
+//   f_d' = f_d - A - B,  f_o' = f_o - A + B
+// (e.u = cu cs2 CFL); the same with q, u + K E and no source for g.
+template <typename T, typename R, bool MACROS>
+__device__ __forceinline__ void finish_node(R (&f)[Q], R (&h)[Q], const Moments<R> &mo, int x,
+                                            int y, int z, unsigned node, const ZRef<R> &zr,
+                                            const StepArgs<T, R> &a, const KConst<R> &c,
+                                            bool local, bool earr) {
+    const int NX = c.nx, NY = c.ny, NZ = c.nz;
+    const R drho = mo.drho, dq = mo.dq, mx = mo.mx, my = mo.my, mz = mo.mz;
+    const R rho = mo.rho, charge = mo.charge;
     // ---- E at this node (and at z = 1 for the injector override) ----
     R Ex, Ey, Ez;
     const unsigned row = (unsigned)NX * ((unsigned)y + (unsigned)NY * z);
@@ -207,21 +209,21 @@ lbm_step_kernel(const PopPtrs<T> pp, const R *__restrict__ phip,
     const int ym = y == 0 ? NY - 1 : y - 1, yp = y == NY - 1 ? 0 : y + 1;
     const unsigned rym = (unsigned)NX * ((unsigned)ym + (unsigned)NY * z);
     const unsigned ryp = (unsigned)NX * ((unsigned)yp + (unsigned)NY * z);
-    if (!EARR) {
+    if (!earr) {
         // E = -grad(phi), central differences (gpu_efield, poisson.cu:44-60);
         // phi = phi00(z) + phi'(x,y,z) with phi' = 0 on both electrodes, and
         // Ez on the electrodes copied from the planes inside (gpu_bc,
         // poisson.cu:61-73).
-        Ex = (__ldg(phip + row + xm) - __ldg(phip + row + xp)) * c.inv2dx;
-        Ey = (__ldg(phip + rym + x) - __ldg(phip + ryp + x)) * c.inv2dy;
+        Ex = (__ldg(a.phip + row + xm) - __ldg(a.phip + row + xp)) * c.inv2dx;
+        Ey = (__ldg(a.phip + rym + x) - __ldg(a.phip + ryp + x)) * c.inv2dy;
         const int zc = z < 1 ? 1 : (z > NZ - 2 ? NZ - 2 : z);
         const unsigned rzc = (unsigned)NX * ((unsigned)y + (unsigned)NY * zc);
-        Ez = (R)__ldg(ez00 + zc) +
-             (__ldg(phip + rzc - c.nxy + x) - __ldg(phip + rzc + c.nxy + x)) * c.inv2dz;
+        Ez = (R)__ldg(a.ez00 + zc) +
+             (__ldg(a.phip + rzc - c.nxy + x) - __ldg(a.phip + rzc + c.nxy + x)) * c.inv2dz;
     } else {
-        Ex = (R)__ldg(exa + node);
-        Ey = (R)__ldg(eya + node);
-        Ez = (R)__ldg(eza + node);
+        Ex = (R)__ldg(a.exa + node);
+        Ey = (R)__ldg(a.eya + node);
+        Ez = (R)__ldg(a.eza + node);
     }
 
     const R fx = charge * Ex + c.exf, fy = charge * Ey, fz = charge * Ez;
@@ -232,18 +234,18 @@ lbm_step_kernel(const PopPtrs<T> pp, const R *__restrict__ phip,
 
     if (z == 0) {
         // LBM.cu:417-492
-        const ZRef<R> z1 = load_zref(zref, 1);
+        const ZRef<R> z1 = load_zref(a.zref, 1);
         PullIdx P1;
         make_pull(P1, x, y, 1, NX, NY, NZ);
         const unsigned node1 = node + c.nxy;
-        R dqm = Store<T>::ld(pp.ha[0] + node1) + c.w[0] * z1.dq0;
+        R dqm = Store<T>::ld(a.pp.ha[0] + node1) + c.w[0] * z1.dq0;
         R mxm = 0, mym = 0, mzm = 0;
 #pragma unroll
         for (int d = 1; d < Q; ++d) {
-            const unsigned s1 = LOCAL ? node1 : pull_src(P1, d);
-            const int e = LOCAL ? 0 : ez_of(d);
-            const R fm = Store<T>::ld(pp.fa[d] + s1) + c.w[cls_of(d)] * z1.dr(e);
-            const R hm = Store<T>::ld(pp.ha[d] + s1) + c.w[cls_of(d)] * z1.dq(e);
+            const unsigned s1 = local ? node1 : pull_src(P1, d);
+            const int e = local ? 0 : ez_of(d);
+            const R fm = Store<T>::ld(a.pp.fa[d] + s1) + c.w[cls_of(d)] * z1.dr(e);
+            const R hm = Store<T>::ld(a.pp.ha[d] + s1) + c.w[cls_of(d)] * z1.dq(e);
             dqm += hm;
             if (ex_of(d)) mxm += ex_of(d) > 0 ? fm : -fm;
             if (ey_of(d)) mym += ey_of(d) > 0 ? fm : -fm;
@@ -251,16 +253,16 @@ lbm_step_kernel(const PopPtrs<T> pp, const R *__restrict__ phip,
         }
         const R chargem = z1.qref + dqm;
         R Exm, Eym, Ezm;
-        if (!EARR) {
+        if (!earr) {
             const unsigned row1 = row + c.nxy;
-            Exm = (__ldg(phip + row1 + xm) - __ldg(phip + row1 + xp)) * c.inv2dx;
-            Eym = (__ldg(phip + rym + c.nxy + x) - __ldg(phip + ryp + c.nxy + x)) * c.inv2dy;
-            Ezm = (R)__ldg(ez00 + 1) +
-                  (__ldg(phip + row + x) - __ldg(phip + row + 2 * c.nxy + x)) * c.inv2dz;
+            Exm = (__ldg(a.phip + row1 + xm) - __ldg(a.phip + row1 + xp)) * c.inv2dx;
+            Eym = (__ldg(a.phip + rym + c.nxy + x) - __ldg(a.phip + ryp + c.nxy + x)) * c.inv2dy;
+            Ezm = (R)__ldg(a.ez00 + 1) +
+                  (__ldg(a.phip + row + x) - __ldg(a.phip + row + 2 * c.nxy + x)) * c.inv2dz;
         } else {
-            Exm = (R)__ldg(exa + node1);
-            Eym = (R)__ldg(eya + node1);
-            Ezm = (R)__ldg(eza + node1);
+            Exm = (R)__ldg(a.exa + node1);
+            Eym = (R)__ldg(a.eya + node1);
+            Ezm = (R)__ldg(a.eza + node1);
         }
         const R fxm = chargem * Exm + c.exf, fym = chargem * Eym, fzm = chargem * Ezm;
         ux = -rhoinv * (mxm * c.cflinv + fxm * c.dt_half);
@@ -268,22 +270,22 @@ lbm_step_kernel(const PopPtrs<T> pp, const R *__restrict__ phip,
         uz = -rhoinv * (mzm * c.cflinv + fzm * c.dt_half);
     }
 
-    qout[node] = charge;
+    a.qout[node] = charge;
     if (MACROS) {
-        rout[node] = rho;
-        uout[node] = ux;
-        vout[node] = uy;
-        wout[node] = uz;
+        a.rout[node] = rho;
+        a.uout[node] = ux;
+        a.vout[node] = uy;
+        a.wout[node] = uz;
     }
 
     // ---- f: collide (interior) or wall rule ----
     if (z == 0 || z == NZ - 1) {
-        Store<T>::st(pp.fb[0] + node, f[0]);
+        Store<T>::st(a.pp.fb[0] + node, f[0]);
 #pragma unroll
         for (int d = 1; d < Q; ++d) {
             R v = f[opp_of(d)];
             if (z == NZ - 1 && mw_sign_of(d) != 0) v += c.mw[d];
-            Store<T>::st(pp.fb[d] + node, v);
+            Store<T>::st(a.pp.fb[d] + node, v);
         }
     } else {
         const R rp_hi = c.rate_hi[0], rp_lo = c.rate_lo[0];
@@ -298,7 +300,7 @@ lbm_step_kernel(const PopPtrs<T> pp, const R *__restrict__ phip,
             PK[k] = WR[k] * usq - c.w[k] * drho;
             QK[k] = c.c3[k] * uF;
         }
-        Store<T>::st(pp.fb[0] + node, f[0] - relax(rp_hi, rp_lo, f[0] + PK[0]) - QK[0]);
+        Store<T>::st(a.pp.fb[0] + node, f[0] - relax(rp_hi, rp_lo, f[0] + PK[0]) - QK[0]);
 #pragma unroll
         for (int d = 1; d < Q; d += 2) {
             const int o = d + 1, k = cls_of(d);
@@ -308,8 +310,8 @@ lbm_step_kernel(const PopPtrs<T> pp, const R *__restrict__ phip,
             const R A = relax(rp_hi, rp_lo, X) + QK[k] - c.c1[k] * cu * eF;
             const R Y = (R)0.5 * (f[d] - f[o]) - WR[k] * cu;
             const R B = relax(rm_hi, rm_lo, Y) - c.c2[k] * eF;
-            Store<T>::st(pp.fb[d] + node, f[d] - A - B);
-            Store<T>::st(pp.fb[o] + node, f[o] - A + B);
+            Store<T>::st(a.pp.fb[d] + node, f[d] - A - B);
+            Store<T>::st(a.pp.fb[o] + node, f[o] - A + B);
         }
     }
 
@@ -332,8 +334,8 @@ lbm_step_kernel(const PopPtrs<T> pp, const R *__restrict__ phip,
         }
         {
             const R out = h[0] - relax(cp_hi, cp_lo, h[0] + PQ[0]);
-            Store<T>::st(pp.hb[0] + node, z == 0 ? -out + (R)2 * (c.q0 - zr.qref) * c.w[0] : out);
-            if (dup) Store<T>::st(pp.hb[0] + nodeup, out + c.w[0] * up);
+            Store<T>::st(a.pp.hb[0] + node, z == 0 ? -out + (R)2 * (c.q0 - zr.qref) * c.w[0] : out);
+            if (dup) Store<T>::st(a.pp.hb[0] + nodeup, out + c.w[0] * up);
         }
 #pragma unroll
         for (int d = 1; d < Q; d += 2) {
@@ -345,11 +347,224 @@ lbm_step_kernel(const PopPtrs<T> pp, const R *__restrict__ phip,
             const R B = relax(cm_hi, cm_lo, Y);
             const R outd = h[d] - A - B;
             const R outo = h[o] - A + B;
-            Store<T>::st(pp.hb[d] + node, outd);
-            Store<T>::st(pp.hb[o] + node, outo);
+            Store<T>::st(a.pp.hb[d] + node, outd);
+            Store<T>::st(a.pp.hb[o] + node, outo);
             if (dup) {
-                Store<T>::st(pp.hb[d] + nodeup, outd + c.w[k] * up);
-                Store<T>::st(pp.hb[o] + nodeup, outo + c.w[k] * up);
+                Store<T>::st(a.pp.hb[d] + nodeup, outd + c.w[k] * up);
+                Store<T>::st(a.pp.hb[o] + nodeup, outo + c.w[k] * up);
+            }
+        }
+    }
+}
+
+// GENERAL = false: the steady-state step (pull, E from phi).  GENERAL = true
+// adds two run-time switches used right after ehd_set_fields:
+//   local_pops: the buffers hold the pre-collision populations of each node
+//               (the reference's f1/h1 after init_equilibrium), so they are
+//               read in place, without pull or injection rule;
+//   e_arrays:   E comes from the uploaded FP64 arrays instead of phi.
+// One thread per node, 128-thread blocks.
+template <typename T, typename R, bool GENERAL, bool MACROS>
+__global__ void __launch_bounds__(128, sizeof(R) == 8 ? 2 : 4)
+lbm_step_kernel(const StepArgs<T, R> a, const KConst<R> c, int local_pops, int e_arrays) {
+    const bool local = GENERAL && local_pops;
+    const bool earr = GENERAL && e_arrays;
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    const bool inside = x < c.nx && y < c.ny;
+    // lanes outside the grid work on a valid node so that the whole warp can
+    // take part in the plane sums; they store nothing
+    if (!inside) {
+        x = x < c.nx ? x : c.nx - 1;
+        y = y < c.ny ? y : c.ny - 1;
+    }
+    const unsigned node = (unsigned)x + (unsigned)c.nx * ((unsigned)y + (unsigned)c.ny * z);
+    const ZRef<R> zr = load_zref(a.zref, z);
+    PullIdx P;
+    make_pull(P, x, y, z, c.nx, c.ny, c.nz);
+    R f[Q], h[Q];
+    pull_global<T, R>(f, h, a.pp, P, node, z, zr, c, local);
+    const Moments<R> mo = moments(f, h, zr);
+    {
+        const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+        warp_plane_sum(inside ? (float)mo.rho : 0.f, inside ? (float)mo.charge : 0.f, a.psum,
+                       (((size_t)z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) * 4 +
+                           (tid >> 5));
+    }
+    if (!inside) return;
+    finish_node<T, R, MACROS>(f, h, mo, x, y, z, node, zr, a, c, local, earr);
+}
+
+// ---- bulk-copy row kernel ------------------------------------------------------
+
+namespace {
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned phase) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+// one contiguous global -> shared copy completing on the barrier; both
+// addresses 16-byte aligned and the size a multiple of 16
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes,
+                                         unsigned long long *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+constexpr unsigned kWaitLimit = 1u << 24;  // try_wait polls before giving up
+
+// e_y + 1 and e_z + 1 of all directions, 2 bits per direction, for lookups
+// with a run-time d (a constexpr table indexed at run time lands in local
+// memory)
+constexpr unsigned long long pack_e(int comp) {
+    unsigned long long v = 0;
+    for (int d = 0; d < Q; ++d)
+        v |= (unsigned long long)((comp == 1 ? ey_of(d) : ez_of(d)) + 1) << (2 * d);
+    return v;
+}
+constexpr unsigned long long kEyPack = pack_e(1), kEzPack = pack_e(2);
+__device__ __forceinline__ int ey_rt(int d) { return (int)((kEyPack >> (2 * d)) & 3u) - 1; }
+__device__ __forceinline__ int ez_rt(int d) { return (int)((kEzPack >> (2 * d)) & 3u) - 1; }
+
+}  // namespace
+
+// Persistent variant of the steady-state step for rows of NX nodes: one CTA
+// of NX threads walks the x-rows (y, z), and for every row lane d of warp 0
+// issues the bulk copies of the source rows (y - e_y, z - e_z) of f_d and g_d
+// into shared memory, one row ahead (two stages).  The x shift -e_x and its
+// periodic wrap are applied when reading shared memory.  Rows of the injector
+// plane z = 0 (which need their own node's g and the z = 1 populations) are
+// pulled from global memory instead.  A wait that does not complete within
+// kWaitLimit polls sets *err, waits (bounded) for the copies still in flight,
+// and returns.
+template <typename T, typename R, bool MACROS>
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 1 : 2)
+lbm_rows_kernel(const StepArgs<T, R> a, const KConst<R> c) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ unsigned long long bar[2];
+    __shared__ int ok_flag;
+    const int NX = c.nx, NY = c.ny, NZ = c.nz;
+    const size_t stage_elems = (size_t)2 * Q * NX;
+    T *const smem = reinterpret_cast<T *>(smem_raw);  // stage s at smem + s * stage_elems
+    const unsigned row_bytes = (unsigned)(NX * sizeof(T));
+    const int x = threadIdx.x;
+    const long long rows = (long long)NY * NZ;
+    const int nw = NX / 32;
+
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    // issue the 54 row copies of row r into stage s (warp 0, lanes 0..26)
+    auto issue = [&](long long r, int s) {
+        const int yy = (int)(r % NY), zz = (int)(r / NY);
+        if (threadIdx.x == 0) mbar_expect_tx(&bar[s], 2u * Q * row_bytes);
+        __syncwarp();
+        const int d = threadIdx.x;
+        if (d < Q) {
+            const int ys = (yy - ey_rt(d) + NY) % NY, zs = (zz - ez_rt(d) + NZ) % NZ;
+            // direction d's array starts d * NX * NY * NZ after direction 0's
+            const size_t off = (size_t)d * NX * NY * NZ + (size_t)NX * ((size_t)ys + (size_t)NY * zs);
+            T *dst = smem + (size_t)s * stage_elems + (size_t)d * NX;
+            bulk_g2s(dst, a.pp.fa[0] + off, row_bytes, &bar[s]);
+            bulk_g2s(dst + (size_t)Q * NX, a.pp.ha[0] + off, row_bytes, &bar[s]);
+        }
+    };
+    auto needs_copy = [&](long long r) { return r < rows && r / NY != 0; };
+
+    unsigned phases = 0u;  // bit s: parity of the next phase of bar[s]
+    long long r0 = blockIdx.x;
+    if (threadIdx.x < 32) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        if (needs_copy(r0)) issue(r0, 0);
+        if (needs_copy(r0 + gridDim.x)) issue(r0 + gridDim.x, 1);
+    }
+    int it = 0;
+    for (long long r = r0; r < rows; r += gridDim.x, ++it) {
+        const int s = it & 1;
+        const int y = (int)(r % NY), z = (int)(r / NY);
+        const unsigned node = (unsigned)x + (unsigned)NX * ((unsigned)y + (unsigned)NY * z);
+        const ZRef<R> zr = load_zref(a.zref, z);
+        PullIdx P;
+        make_pull(P, x, y, z, NX, NY, NZ);
+        R f[Q], h[Q];
+        if (z != 0) {
+            if (threadIdx.x == 0) {
+                unsigned n = 0;
+                while (!mbar_try_wait(&bar[s], (phases >> s) & 1u) && ++n < kWaitLimit) {
+                }
+                ok_flag = n < kWaitLimit;
+            }
+            __syncthreads();
+            if (!ok_flag) {
+                if (threadIdx.x == 0) {
+                    atomicExch(a.err, 1);
+                    // copies may still be landing in this stage and in the
+                    // other one (row r + gridDim.x): bounded waits for both
+                    unsigned n = 0;
+                    while (!mbar_try_wait(&bar[s], (phases >> s) & 1u) && ++n < kWaitLimit) {
+                    }
+                    if (needs_copy(r + gridDim.x)) {
+                        n = 0;
+                        while (!mbar_try_wait(&bar[s ^ 1], (phases >> (s ^ 1)) & 1u) &&
+                               ++n < kWaitLimit) {
+                        }
+                    }
+                }
+                __syncthreads();
+                return;
+            }
+            (void)mbar_try_wait(&bar[s], (phases >> s) & 1u);  // acquire for this thread
+            phases ^= 1u << s;
+            const T *sf = smem + (size_t)s * stage_elems;
+            const T *sh = sf + (size_t)Q * NX;
+#pragma unroll
+            for (int d = 0; d < Q; ++d) {
+                const int xs = P.xs[ex_of(d) + 1];
+                f[d] = Store<T>::lds(sf + (size_t)d * NX + xs) + c.w[cls_of(d)] * zr.dr(ez_of(d));
+                h[d] = Store<T>::lds(sh + (size_t)d * NX + xs) + c.w[cls_of(d)] * zr.dq(ez_of(d));
+            }
+        } else {
+            pull_global<T, R>(f, h, a.pp, P, node, z, zr, c, false);
+        }
+        const Moments<R> mo = moments(f, h, zr);
+        warp_plane_sum((float)mo.rho, (float)mo.charge, a.psum,
+                       ((size_t)z * NY + y) * nw + (threadIdx.x >> 5));
+        finish_node<T, R, MACROS>(f, h, mo, x, y, z, node, zr, a, c, false, false);
+        // the stage is free once every thread has read it: refill it with the
+        // row two iterations ahead
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            const long long rn = r + 2LL * gridDim.x;
+            if (needs_copy(rn)) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                issue(rn, s);
             }
         }
     }
@@ -464,26 +679,79 @@ __global__ void fields_to_compute_kernel(const double *const *out, R *rho, R *u,
 
 // ---- launchers ---------------------------------------------------------------
 
+size_t lbm_rows_smem(int nx, size_t tsize) { return (size_t)2 * 2 * Q * nx * tsize; }
+
+// FP32 and FP64 storage only: with 2-byte populations the per-node kernel
+// measured faster (0.73 vs 0.76 ms at 256 x 256 x 129, FP16)
+bool lbm_rows_usable(int nx, size_t tsize) {
+    return tsize >= 4 && nx >= 32 && nx <= 256 && nx % 32 == 0 && (nx * tsize) % 16 == 0 &&
+           lbm_rows_smem(nx, tsize) <= 220 * 1024;
+}
+
 template <typename T, typename R>
-cudaError_t launch_lbm_step(const LbmArgs &a, const StepConst &c, int local_pops, int e_arrays,
+cudaError_t prepare_lbm_rows(int nx, int ny, int nz, int *grid) {
+    *grid = 0;
+    if (!lbm_rows_usable(nx, sizeof(T))) return cudaSuccess;
+    const int sm = (int)lbm_rows_smem(nx, sizeof(T));
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(lbm_rows_kernel<T, R, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, sm)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(lbm_rows_kernel<T, R, false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, sm)) != cudaSuccess)
+        return e;
+    int dev = 0, nsm = 0, occ_a = 0, occ_b = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, lbm_rows_kernel<T, R, true>, nx,
+                                                           sm)) != cudaSuccess ||
+        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, lbm_rows_kernel<T, R, false>, nx,
+                                                           sm)) != cudaSuccess)
+        return e;
+    const long long rows = (long long)ny * nz;
+    *grid = (int)std::min<long long>(rows, (long long)nsm * std::min(occ_a, occ_b));
+    return cudaSuccess;
+}
+
+template cudaError_t prepare_lbm_rows<double, double>(int, int, int, int *);
+template cudaError_t prepare_lbm_rows<float, float>(int, int, int, int *);
+template cudaError_t prepare_lbm_rows<__half, float>(int, int, int, int *);
+template cudaError_t prepare_lbm_rows<__nv_bfloat16, float>(int, int, int, int *);
+
+template <typename T, typename R>
+cudaError_t launch_lbm_step(const LbmArgs &la, const StepConst &c, int local_pops, int e_arrays,
                             bool macros, cudaStream_t s) {
+    StepArgs<T, R> a;
+    for (int d = 0; d < Q; ++d) {
+        a.pp.fa[d] = (const T *)la.fa + (size_t)d * c.n;
+        a.pp.ha[d] = (const T *)la.ha + (size_t)d * c.n;
+        a.pp.fb[d] = (T *)la.fb + (size_t)d * c.n;
+        a.pp.hb[d] = (T *)la.hb + (size_t)d * c.n;
+    }
+    a.phip = (const R *)la.phip;
+    a.ez00 = la.ez00;
+    a.exa = la.exa;
+    a.eya = la.eya;
+    a.eza = la.eza;
+    a.qout = (R *)la.q;
+    a.rout = (R *)la.rho;
+    a.uout = (R *)la.u;
+    a.vout = (R *)la.v;
+    a.wout = (R *)la.w;
+    a.zref = (const R *)la.zref;
+    a.psum = la.psum;
+    a.err = la.err;
+    const KConst<R> k = make_kconst<R>(c);
+    const bool general = local_pops || e_arrays;
+    if (!general && la.rows_grid > 0) {
+        // the shared-memory attribute was set by prepare_lbm_rows
+        const size_t sm = lbm_rows_smem(c.nx, sizeof(T));
+        if (macros) lbm_rows_kernel<T, R, true><<<la.rows_grid, c.nx, sm, s>>>(a, k);
+        else lbm_rows_kernel<T, R, false><<<la.rows_grid, c.nx, sm, s>>>(a, k);
+        return cudaGetLastError();
+    }
     dim3 block(c.nx >= 64 ? 64 : 32, c.nx >= 64 ? 2 : 4, 1);
     dim3 grid((c.nx + block.x - 1) / block.x, (c.ny + block.y - 1) / block.y, c.nz);
-    PopPtrs<T> pp;
-    for (int d = 0; d < Q; ++d) {
-        pp.fa[d] = (const T *)a.fa + (size_t)d * c.n;
-        pp.ha[d] = (const T *)a.ha + (size_t)d * c.n;
-        pp.fb[d] = (T *)a.fb + (size_t)d * c.n;
-        pp.hb[d] = (T *)a.hb + (size_t)d * c.n;
-    }
-    const KConst<R> k = make_kconst<R>(c);
-    const R *phip = (const R *)a.phip;
-    R *q = (R *)a.q, *r = (R *)a.rho, *u = (R *)a.u, *v = (R *)a.v, *w = (R *)a.w;
-    const bool general = local_pops || e_arrays;
-#define EHD_LAUNCH(G, M)                                                                     \
-    lbm_step_kernel<T, R, G, M><<<grid, block, 0, s>>>(pp, phip, a.ez00, a.exa, a.eya, a.eza, \
-                                                       q, r, u, v, w, (const R *)a.zref,      \
-                                                       a.psum, k, local_pops, e_arrays)
+#define EHD_LAUNCH(G, M) lbm_step_kernel<T, R, G, M><<<grid, block, 0, s>>>(a, k, local_pops, e_arrays)
     if (general) {
         if (macros) EHD_LAUNCH(true, true);
         else EHD_LAUNCH(true, false);
@@ -682,6 +950,8 @@ int lbm_blocks_per_plane(int nx, int ny) {
     const int bx = nx >= 64 ? 64 : 32, by = nx >= 64 ? 2 : 4;
     return ((nx + bx - 1) / bx) * ((ny + by - 1) / by) * 4;
 }
+
+int lbm_rows_slots_per_plane(int nx, int ny) { return ny * (nx / 32); }
 
 // ---- seeded initial state ------------------------------------------------------
 

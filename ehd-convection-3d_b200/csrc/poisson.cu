@@ -36,6 +36,8 @@
 // Stockham passes of radix 8/16 (fft.cuh), two real x-rows packed into one
 // complex transform; other sizes of the form 2^a 3^b 5^c use run-time
 // radix-2/3/4/5 passes.  Twiddles come from an FP64-accurate table.
+#include <cmath>
+
 #include "common.cuh"
 #include "fft.cuh"
 #include "kernels.h"
@@ -521,6 +523,123 @@ poisson_zsolve(typename Cplx<R>::T *__restrict__ spec, const double *__restrict_
     }
 }
 
+// K3 (fast sizes): the same z solve by the sine transform the reference's
+// odd extension amounts to, for L = 2 (NZ - 1) in the compile-time FFT sizes,
+// in the compute type.  Per mode the interior column x_1..x_n (n = NZ - 2) is
+// extended oddly to length L, y = [0, x_1..x_n, 0, -x_n..-x_1], so that its
+// DFT is Y_k = -2i S_k with S_k = sum_j x_j sin(pi j k / (n + 1)) (DST-I).
+// The 3-point operator x_{j-1} - beta x_j + x_{j+1} has the eigenvalues
+// -(lambda_k + h dz^2), lambda_k = 4 sin^2(pi k / L), on sin(pi j k / (n+1)),
+// and the same DFT applied to the scaled, still odd, spectrum gives
+//   x_j = (dz^2 / L) DFT[ Y_k / (lambda_k + h dz^2) ]_j,
+// with h = kx^2 + ky^2 (main.cu:110-129) and the terms k = 0, L/2 zero.
+// lambda_k comes from an FP64 table: 2 - 2 cos(2 pi k / L) in the compute type
+// would cancel for small k.  TB modes per block, consecutive in the flattened
+// index m = ky nxh + kx.
+//
+// The (0,0) mode is solved by the block holding m = 0 in FP64 and apart from
+// the transforms: right-hand side as in poisson_zsolve, and with beta = 2 the
+// inverse of the Dirichlet operator is known in closed form,
+//   x_i = -sum_j min(i, j) (n + 1 - max(i, j)) / (n + 1) d_j dz^2,
+// one thread per plane.  That block writes phi00 and its Ez.
+template <typename R, int L>
+__global__ void __launch_bounds__(256)
+poisson_zdst(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::T *__restrict__ twz,
+             const R *__restrict__ lamz, const double *__restrict__ planesum,
+             const double *__restrict__ qmean, double *__restrict__ phi00,
+             double *__restrict__ ez00, int nx, int ny, int nxh, int pitch, double dz,
+             double eps, double voltage, double kx0, double ky0) {
+    using R2 = typename Cplx<R>::T;
+    constexpr int G = fft::Plan<L>::G, TB = 256 / G, P = tstride<L>();
+    constexpr int n = L / 2 - 1, nz = n + 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *tws = reinterpret_cast<R2 *>(smem_raw);
+    R2 *buf = tws + L;
+    __shared__ double mrhs[n > 0 ? n : 1], mphi[nz];
+    const int tid = threadIdx.x;
+    const int modes = nxh * ny;
+    const int m0 = blockIdx.x * TB;
+    const size_t plane = (size_t)ny * pitch;
+    const double dz2 = dz * dz;
+    const R rdz2 = (R)dz2;
+    for (int i = tid; i < L; i += 256) tws[i] = twz[i];
+#pragma unroll 4
+    for (int i = tid; i < TB * n; i += 256) {
+        const int zi = i / TB, t = i - zi * TB;
+        const int m = m0 + t;
+        R2 v = R2{(R)0, (R)0};
+        if (m != 0 && m < modes) {
+            const int ky = m / nxh, kx = m - ky * nxh;
+            v = spec[(size_t)zi * plane + (size_t)ky * pitch + kx];
+        }
+        buf[t * P + fft::pad(zi + 1)] = v;
+        buf[t * P + fft::pad(L - 1 - zi)] = R2{-v.x, -v.y};
+    }
+    if (tid < TB) {
+        buf[tid * P + fft::pad(0)] = R2{(R)0, (R)0};
+        buf[tid * P + fft::pad(L / 2)] = R2{(R)0, (R)0};
+    }
+    if (m0 == 0) {
+        const double nxy = (double)nx * (double)ny;
+        for (int i = tid; i < n; i += 256) {
+            double d = planesum[i + 1] + nxy * (-(double)(R)qmean[2 * (i + 1) + 1] / eps);
+            if (i == 0) d += -voltage / dz2 * nxy;
+            mrhs[i] = d * dz2;
+        }
+    }
+    __syncthreads();
+    const int tr = tid / G, j = tid - tr * G;
+    fft::Plan<L>::template run<-1>(buf + tr * P, tws, j);
+#pragma unroll 4
+    for (int i = tid; i < TB * L; i += 256) {
+        const int t = i / L, k = i - t * L;
+        const int m = m0 + t;
+        R2 &y = buf[t * P + fft::pad(k)];
+        if (k == 0 || k == L / 2 || m >= modes || m == 0) {
+            y = R2{(R)0, (R)0};
+        } else {
+            const int ky = m / nxh, kx = m - ky * nxh;
+            const R wx = (R)(kx * kx0), wy = (R)((ky <= ny / 2 ? ky : ky - ny) * ky0);
+            const R f = (R)1 / (lamz[k < L / 2 ? k : L - k] + (wx * wx + wy * wy) * rdz2);
+            y = R2{y.x * f, y.y * f};
+        }
+    }
+    __syncthreads();
+    fft::Plan<L>::template run<-1>(buf + tr * P, tws, j);
+    const R sc = (R)(dz2 / (double)L);
+#pragma unroll 4
+    for (int i = tid; i < TB * n; i += 256) {
+        const int zi = i / TB, t = i - zi * TB;
+        const int m = m0 + t;
+        if (m >= modes) continue;
+        const int ky = m / nxh, kx = m - ky * nxh;
+        const R2 w = buf[t * P + fft::pad(zi + 1)];
+        spec[(size_t)zi * plane + (size_t)ky * pitch + kx] = R2{w.x * sc, w.y * sc};
+    }
+    if (m0 == 0) {
+        const double nxy = (double)nx * (double)ny;
+        for (int i = tid; i < nz; i += 256) {
+            double x = 0.0;
+            if (i == 0) {
+                x = voltage;
+            } else if (i < nz - 1) {
+                for (int jj = 1; jj <= n; ++jj) {
+                    const int lo = i < jj ? i : jj, hi = i < jj ? jj : i;
+                    x -= (double)(lo * (n + 1 - hi)) * mrhs[jj - 1];
+                }
+                x = x / (double)(n + 1) / nxy;
+            }
+            mphi[i] = x;
+            phi00[i] = x;
+        }
+        __syncthreads();
+        for (int z = tid; z < nz; z += 256) {
+            const int zc = z < 1 ? 1 : (z > nz - 2 ? nz - 2 : z);
+            ez00[z] = 0.5 * (mphi[zc - 1] - mphi[zc + 1]) / dz;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // launcher
 // ---------------------------------------------------------------------------
@@ -639,13 +758,36 @@ static cudaError_t cols(const PoissonArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <typename R, int L>
+static cudaError_t zdst(const PoissonArgs &a, cudaStream_t s) {
+    using R2 = typename Cplx<R>::T;
+    constexpr int TB = per_block<L>();
+    const size_t sm = sizeof(R2) * ((size_t)L + (size_t)TB * tstride<L>());
+    cudaError_t e = set_smem(poisson_zdst<R, L>, sm, s);
+    if (e != cudaSuccess) return e;
+    const int modes = a.nxh * a.ny;
+    const R2 *tw = (const R2 *)a.twz;
+    poisson_zdst<R, L><<<(modes + TB - 1) / TB, 256, sm, s>>>(
+        (R2 *)a.spec, tw, (const R *)(tw + L), a.planesum, a.qmean, a.phi00, a.ez00, a.nx, a.ny,
+        a.nxh, a.pitch, a.dz, a.eps, a.voltage, 2.0 * M_PI / a.lx, 2.0 * M_PI / a.ly);
+    return cudaGetLastError();
+}
+
 template <typename R>
 cudaError_t launch_poisson(const PoissonArgs &a, cudaStream_t s) {
     using R2 = typename Cplx<R>::T;
     cudaError_t e;
     if ((e = rows_fwd<R>(a, s)) != cudaSuccess) return e;
     if ((e = cols<R, -1>(a, s)) != cudaSuccess) return e;
-    {
+    if (a.twz && poisson_fast_size(2 * (a.nz - 1))) {
+        switch (2 * (a.nz - 1)) {
+            case 64: e = zdst<R, 64>(a, s); break;
+            case 128: e = zdst<R, 128>(a, s); break;
+            case 256: e = zdst<R, 256>(a, s); break;
+            default: e = zdst<R, 512>(a, s); break;
+        }
+        if (e != cudaSuccess) return e;
+    } else {
         const int modes = a.nxh * a.ny;
         poisson_zsolve<R><<<(modes + 127) / 128, 128, 0, s>>>(
             (R2 *)a.spec, a.cpt, a.dpw, a.planesum, a.qmean, a.phi00, a.ez00, a.nx, a.ny, a.nz,

@@ -20,6 +20,7 @@ LIB_PATH = HERE / "libehd.so"
 FIELDS = ("rho", "u", "v", "w", "q", "phi", "ex", "ey", "ez")
 PRECISIONS = {"fp64": 0, "fp32": 1, "fp16": 2, "bf16": 3}
 FLAG_NO_GRAPH = 0x1
+FLAG_NODE_KERNEL = 0x2
 
 
 class EhdError(RuntimeError):
@@ -177,11 +178,12 @@ class Simulation:
     """One simulation instance (ehd_ctx) on one GPU."""
 
     def __init__(self, params: Params, precision: str = "fp32", device: int = 0,
-                 stream: int | None = None, graphs: bool = True):
+                 stream: int | None = None, graphs: bool = True, row_kernel: bool = True):
         self.p = params
         self.shape = (params.nz, params.ny, params.nx)
+        flags = (0 if graphs else FLAG_NO_GRAPH) | (0 if row_kernel else FLAG_NODE_KERNEL)
         cfg = Config(precision=PRECISIONS[precision], device=device, stream=stream,
-                     flags=0 if graphs else FLAG_NO_GRAPH)
+                     flags=flags)
         h = _vp()
         _check(lib().ehd_create(ctypes.byref(params), ctypes.byref(cfg), ctypes.byref(h)))
         self.h = h

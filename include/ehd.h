@@ -74,6 +74,8 @@ typedef struct ehd_config {
 } ehd_config;
 
 #define EHD_FLAG_NO_GRAPH 0x1u /* launch kernels one by one, no CUDA graphs   */
+#define EHD_FLAG_NODE_KERNEL 0x2u /* every step on the one-thread-per-node
+                                     kernel (no bulk-copy row kernel)       */
 
 typedef struct ehd_ctx ehd_ctx;
 

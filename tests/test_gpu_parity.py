@@ -146,6 +146,31 @@ def test_poisson_fft_sizes_match_oracle(shape, prec, tol):
         assert relerr(a[k], b[k]) < tol, (k, relerr(a[k], b[k]))
 
 
+@pytest.mark.parametrize("shape", [(64, 48, 33), (96, 64, 65), (32, 20, 129), (16, 12, 257)])
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("fp32", 2e-6)])
+def test_poisson_sine_transform_z_solve_matches_oracle(shape, prec, tol):
+    """2 (NZ - 1) = 64..512: the z solve runs as a sine transform (odd
+    extension, FFT, spectral division, FFT) instead of the Thomas sweep;
+    against the oracle's odd-extension DFT solve on random charge.  The z
+    operator's condition number grows as NZ^2 (about 3e4 at NZ = 257), which
+    sets the FP64 tolerance."""
+    nx, ny, nz = shape
+    dz = 1.0 / (nz - 1)
+    p = O.params_from_groups(nx, ny, nz, nx * dz, ny * dz, T=200, M=10, C=10, Fe=4000)
+    f = random_fields(p, 4)
+    o = O.Oracle(p)
+    o.set_fields(f)
+    o.poisson()
+    o.efield()
+    b = o.get_fields()
+    with ehd.Simulation(to_ehd(p), prec) as sim:
+        sim.set_fields(f)
+        sim.poisson()
+        a = sim.get_fields()
+    for k in ("phi", "ex", "ey", "ez"):
+        assert relerr(a[k], b[k]) < tol, (k, relerr(a[k], b[k]))
+
+
 def test_graphs_and_direct_launches_agree_bitwise():
     _, p, _, f = config0_inputs()
     out = []
