@@ -307,13 +307,24 @@ poisson_rows_fwd_fast(const R *__restrict__ q, typename Cplx<R>::T *__restrict__
     const R qm = (R)qmean[2 * (zi + 1) + 1];
     const R ieps = (R)(1.0 / eps);
     load_twiddles<R, N>(tws, tw);
-    for (int i = tid; i < TB * N; i += 256) {
-        const int tr = i / N, x = i - tr * N;
-        const int ya = y0 + 2 * tr, yb = ya + 1;
-        R a = 0, b = 0;
-        if (ya < ny) a = -(qp[(size_t)N * ya + x] - qm) * ieps;
-        if (yb < ny) b = -(qp[(size_t)N * yb + x] - qm) * ieps;
-        buf[tr * P + fft::pad(x)] = R2{a, b};
+    {
+        // every load of the tile in flight before the first shared store
+        constexpr int IT = TB * N / 256;
+        R va[IT], vb[IT];
+#pragma unroll
+        for (int r = 0; r < IT; ++r) {
+            const int i = tid + 256 * r;
+            const int tr = i / N, x = i - tr * N;
+            const int ya = y0 + 2 * tr, yb = ya + 1;
+            va[r] = ya < ny ? qp[(size_t)N * ya + x] : qm;
+            vb[r] = yb < ny ? qp[(size_t)N * yb + x] : qm;
+        }
+#pragma unroll
+        for (int r = 0; r < IT; ++r) {
+            const int i = tid + 256 * r;
+            const int tr = i / N, x = i - tr * N;
+            buf[tr * P + fft::pad(x)] = R2{-(va[r] - qm) * ieps, -(vb[r] - qm) * ieps};
+        }
     }
     {  // FP64 row sums, one warp per row, fixed order
         const int warp = tid >> 5, lane = tid & 31;
@@ -359,21 +370,27 @@ poisson_cols_fast(typename Cplx<R>::T *__restrict__ spec,
     const int tid = threadIdx.x;
     const size_t off = (size_t)zi * N * pitch;
     load_twiddles<R, N>(tws, tw);
-    for (int i = tid; i < TB * N; i += 256) {
-        const int y = i / TB, c = i - y * TB;
-        const int k = k0 + c;
-        R2 v = R2{(R)0, (R)0};
-        if (k < nxh) v = spec[off + (size_t)pitch * y + k];
-        buf[c * P + fft::pad(y)] = v;
+    // thread tid serves column c = tid % TB and rows y = tid / TB + (256 / TB) r
+    constexpr int IT = TB * N / 256, YS = 256 / TB;
+    const int c = tid % TB, yt = tid / TB;
+    const bool valid = k0 + c < nxh;
+    R2 *col = spec + off + k0 + c;
+    {
+        R2 v[IT];
+#pragma unroll
+        for (int r = 0; r < IT; ++r)
+            v[r] = valid ? col[(size_t)pitch * (yt + YS * r)] : R2{(R)0, (R)0};
+#pragma unroll
+        for (int r = 0; r < IT; ++r) buf[c * P + fft::pad(yt + YS * r)] = v[r];
     }
     if (S < 0 && blockIdx.x == 0 && tid < 32) plane_sum_warp(rowsum, planesum, zi, N);
     __syncthreads();
     const int tr = tid / G, j = tid - tr * G;
     fft::Plan<N>::template run<S>(buf + tr * P, tws, j);
-    for (int i = tid; i < TB * N; i += 256) {
-        const int y = i / TB, c = i - y * TB;
-        const int k = k0 + c;
-        if (k < nxh) spec[off + (size_t)pitch * y + k] = buf[c * P + fft::pad(y)];
+    if (valid) {
+#pragma unroll
+        for (int r = 0; r < IT; ++r)
+            col[(size_t)pitch * (yt + YS * r)] = buf[c * P + fft::pad(yt + YS * r)];
     }
 }
 
@@ -395,23 +412,34 @@ poisson_rows_inv_fast(const typename Cplx<R>::T *__restrict__ spec, R *__restric
     const int tid = threadIdx.x;
     const R2 *sp = spec + (size_t)zi * ny * pitch;
     load_twiddles<R, N>(tws, tw);
-    for (int i = tid; i < TB * N; i += 256) {
-        const int tr = i / N, k = i - tr * N;
-        const int ya = y0 + 2 * tr, yb = ya + 1;
-        const bool lo = k < nxh;
-        const int kk = lo ? k : N - k;
-        R2 A = R2{(R)0, (R)0}, B = R2{(R)0, (R)0};
-        if (ya < ny) A = sp[(size_t)pitch * ya + kk];
-        if (yb < ny) B = sp[(size_t)pitch * yb + kk];
-        if (kk == 0 || kk == N / 2) {
-            A.y = 0;
-            B.y = 0;
+    {
+        constexpr int IT = TB * N / 256;
+        R2 va[IT], vb[IT];
+#pragma unroll
+        for (int r = 0; r < IT; ++r) {
+            const int i = tid + 256 * r;
+            const int tr = i / N, k = i - tr * N;
+            const int ya = y0 + 2 * tr, yb = ya + 1;
+            const int kk = k < nxh ? k : N - k;
+            va[r] = ya < ny ? sp[(size_t)pitch * ya + kk] : R2{(R)0, (R)0};
+            vb[r] = yb < ny ? sp[(size_t)pitch * yb + kk] : R2{(R)0, (R)0};
         }
-        if (!lo) {
-            A.y = -A.y;
-            B.y = -B.y;
+#pragma unroll
+        for (int r = 0; r < IT; ++r) {
+            const int i = tid + 256 * r;
+            const int tr = i / N, k = i - tr * N;
+            const int kk = k < nxh ? k : N - k;
+            R2 A = va[r], B = vb[r];
+            if (kk == 0 || kk == N / 2) {
+                A.y = 0;
+                B.y = 0;
+            }
+            if (k >= nxh) {
+                A.y = -A.y;
+                B.y = -B.y;
+            }
+            buf[tr * P + fft::pad(k)] = R2{A.x - B.y, A.y + B.x};
         }
-        buf[tr * P + fft::pad(k)] = R2{A.x - B.y, A.y + B.x};
     }
     __syncthreads();
     const int tr = tid / G, j = tid - tr * G;
@@ -523,6 +551,10 @@ poisson_zsolve(typename Cplx<R>::T *__restrict__ spec, const double *__restrict_
     }
 }
 
+// correctly rounded reciprocal
+__device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
+
 // K3 (fast sizes): the same z solve by the sine transform the reference's
 // odd extension amounts to, for L = 2 (NZ - 1) in the compile-time FFT sizes,
 // in the compute type.  Per mode the interior column x_1..x_n (n = NZ - 2) is
@@ -556,24 +588,44 @@ poisson_zdst(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::T *
     R2 *tws = reinterpret_cast<R2 *>(smem_raw);
     R2 *buf = tws + L;
     __shared__ double mrhs[n > 0 ? n : 1], mphi[nz];
+    __shared__ R hdz2[TB];  // (kx^2 + ky^2) dz^2 of transform t, < 0: no mode
     const int tid = threadIdx.x;
     const int modes = nxh * ny;
     const int m0 = blockIdx.x * TB;
     const size_t plane = (size_t)ny * pitch;
     const double dz2 = dz * dz;
-    const R rdz2 = (R)dz2;
     for (int i = tid; i < L; i += 256) tws[i] = twz[i];
-#pragma unroll 4
-    for (int i = tid; i < TB * n; i += 256) {
-        const int zi = i / TB, t = i - zi * TB;
-        const int m = m0 + t;
-        R2 v = R2{(R)0, (R)0};
-        if (m != 0 && m < modes) {
-            const int ky = m / nxh, kx = m - ky * nxh;
-            v = spec[(size_t)zi * plane + (size_t)ky * pitch + kx];
+    // thread tid serves transform t = tid % TB and planes zi = tid / TB + (256 / TB) r
+    constexpr int YS = 256 / TB, IT = (n + YS - 1) / YS;
+    const int t = tid % TB, zt = tid / TB;
+    const int m = m0 + t;
+    const bool valid = m < modes && m != 0;
+    size_t goff = 0;
+    if (m < modes) {
+        const int ky = m / nxh, kx = m - ky * nxh;
+        goff = (size_t)ky * pitch + kx;
+        if (zt == 0) {
+            const double wx = kx * kx0, wy = (ky <= ny / 2 ? ky : ky - ny) * ky0;
+            hdz2[t] = m == 0 ? (R)-1 : (R)((wx * wx + wy * wy) * dz2);
         }
-        buf[t * P + fft::pad(zi + 1)] = v;
-        buf[t * P + fft::pad(L - 1 - zi)] = R2{-v.x, -v.y};
+    } else if (zt == 0) {
+        hdz2[t] = (R)-1;
+    }
+    {
+        R2 v[IT];
+#pragma unroll
+        for (int r = 0; r < IT; ++r) {
+            const int zi = zt + YS * r;
+            v[r] = valid && zi < n ? spec[(size_t)zi * plane + goff] : R2{(R)0, (R)0};
+        }
+#pragma unroll
+        for (int r = 0; r < IT; ++r) {
+            const int zi = zt + YS * r;
+            if (zi < n) {
+                buf[t * P + fft::pad(zi + 1)] = v[r];
+                buf[t * P + fft::pad(L - 1 - zi)] = R2{-v[r].x, -v[r].y};
+            }
+        }
     }
     if (tid < TB) {
         buf[tid * P + fft::pad(0)] = R2{(R)0, (R)0};
@@ -590,31 +642,31 @@ poisson_zdst(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::T *
     __syncthreads();
     const int tr = tid / G, j = tid - tr * G;
     fft::Plan<L>::template run<-1>(buf + tr * P, tws, j);
-#pragma unroll 4
-    for (int i = tid; i < TB * L; i += 256) {
-        const int t = i / L, k = i - t * L;
-        const int m = m0 + t;
-        R2 &y = buf[t * P + fft::pad(k)];
-        if (k == 0 || k == L / 2 || m >= modes || m == 0) {
+    // transform tr, bins k = j + G u
+#pragma unroll
+    for (int u = 0; u < L / G; ++u) {
+        const int k = j + G * u;
+        R2 &y = buf[tr * P + fft::pad(k)];
+        const R h = hdz2[tr];
+        if (k == 0 || k == L / 2 || h < (R)0) {
             y = R2{(R)0, (R)0};
         } else {
-            const int ky = m / nxh, kx = m - ky * nxh;
-            const R wx = (R)(kx * kx0), wy = (R)((ky <= ny / 2 ? ky : ky - ny) * ky0);
-            const R f = (R)1 / (lamz[k < L / 2 ? k : L - k] + (wx * wx + wy * wy) * rdz2);
+            const R f = rcp(lamz[k < L / 2 ? k : L - k] + h);
             y = R2{y.x * f, y.y * f};
         }
     }
     __syncthreads();
     fft::Plan<L>::template run<-1>(buf + tr * P, tws, j);
     const R sc = (R)(dz2 / (double)L);
-#pragma unroll 4
-    for (int i = tid; i < TB * n; i += 256) {
-        const int zi = i / TB, t = i - zi * TB;
-        const int m = m0 + t;
-        if (m >= modes) continue;
-        const int ky = m / nxh, kx = m - ky * nxh;
-        const R2 w = buf[t * P + fft::pad(zi + 1)];
-        spec[(size_t)zi * plane + (size_t)ky * pitch + kx] = R2{w.x * sc, w.y * sc};
+    if (m < modes) {
+#pragma unroll
+        for (int r = 0; r < IT; ++r) {
+            const int zi = zt + YS * r;
+            if (zi < n) {
+                const R2 w = buf[t * P + fft::pad(zi + 1)];
+                spec[(size_t)zi * plane + goff] = R2{w.x * sc, w.y * sc};
+            }
+        }
     }
     if (m0 == 0) {
         const double nxy = (double)nx * (double)ny;
