@@ -388,8 +388,9 @@ lbm_step_kernel(const StepArgs<T, R> a, const KConst<R> c, int local_pops, int e
     const Moments<R> mo = moments(f, h, zr);
     {
         const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+        const int wpb = (blockDim.x * blockDim.y) >> 5;
         warp_plane_sum(inside ? (float)mo.rho : 0.f, inside ? (float)mo.charge : 0.f, a.psum,
-                       (((size_t)z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) * 4 +
+                       (((size_t)z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) * wpb +
                            (tid >> 5));
     }
     if (!inside) return;
@@ -452,96 +453,109 @@ __device__ __forceinline__ int ez_rt(int d) { return (int)((kEzPack >> (2 * d)) 
 }  // namespace
 
 // Persistent variant of the steady-state step for rows of NX nodes: one CTA
-// of NX threads walks the x-rows (y, z), and for every row lane d of warp 0
-// issues the bulk copies of the source rows (y - e_y, z - e_z) of f_d and g_d
-// into shared memory, one row ahead (two stages).  The x shift -e_x and its
-// periodic wrap are applied when reading shared memory.  Rows of the injector
-// plane z = 0 (which need their own node's g and the z = 1 populations) are
-// pulled from global memory instead.  A wait that does not complete within
-// kWaitLimit polls sets *err, waits (bounded) for the copies still in flight,
-// and returns.
+// of NX threads walks the x-rows (y, z) of the planes z >= 1, and the source
+// rows (y - e_y, z - e_z) of f_d and g_d of each row arrive in shared memory
+// by bulk copies, two rows ahead (two stages).  The x shift -e_x and its
+// periodic wrap are applied when reading shared memory.
+//
+// No block-wide barrier in the loop: each warp waits for its stage on the
+// stage's mbarrier, reads its 54 values into registers and counts itself out
+// of the stage (shared counter); the warp that counts last refills the stage
+// with the row two iterations ahead while the others compute.  The rows of
+// the injector plane z = 0 (own-node g and z = 1 populations) follow at the
+// end, pulled from global memory.  A wait that does not complete within
+// kWaitLimit polls sets *err, waits (bounded) for the copies that may still
+// be landing, and ends the warp.
 template <typename T, typename R, bool MACROS>
 __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 1 : 2)
 lbm_rows_kernel(const StepArgs<T, R> a, const KConst<R> c) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ unsigned long long bar[2];
-    __shared__ int ok_flag;
+    __shared__ unsigned cnt[2];
     const int NX = c.nx, NY = c.ny, NZ = c.nz;
     const size_t stage_elems = (size_t)2 * Q * NX;
     T *const smem = reinterpret_cast<T *>(smem_raw);  // stage s at smem + s * stage_elems
     const unsigned row_bytes = (unsigned)(NX * sizeof(T));
     const int x = threadIdx.x;
-    const long long rows = (long long)NY * NZ;
-    const int nw = NX / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned nw = (unsigned)(NX / 32);
 
     if (threadIdx.x == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
+        cnt[0] = 0u;
+        cnt[1] = 0u;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
 
-    // issue the 54 row copies of row r into stage s (warp 0, lanes 0..26)
-    auto issue = [&](long long r, int s) {
-        const int yy = (int)(r % NY), zz = (int)(r / NY);
-        if (threadIdx.x == 0) mbar_expect_tx(&bar[s], 2u * Q * row_bytes);
+    // the calling warp issues the 54 row copies of row (yy, zz) into stage s;
+    // lane d < 27 copies direction d
+    auto issue = [&](int yy, int zz, int s) {
+        if (lane == 0) mbar_expect_tx(&bar[s], 2u * Q * row_bytes);
         __syncwarp();
-        const int d = threadIdx.x;
-        if (d < Q) {
-            const int ys = (yy - ey_rt(d) + NY) % NY, zs = (zz - ez_rt(d) + NZ) % NZ;
+        if (lane < Q) {
+            int ys = yy - ey_rt(lane), zs = zz - ez_rt(lane);
+            ys += ys < 0 ? NY : (ys >= NY ? -NY : 0);
+            zs += zs < 0 ? NZ : (zs >= NZ ? -NZ : 0);
             // direction d's array starts d * NX * NY * NZ after direction 0's
-            const size_t off = (size_t)d * NX * NY * NZ + (size_t)NX * ((size_t)ys + (size_t)NY * zs);
-            T *dst = smem + (size_t)s * stage_elems + (size_t)d * NX;
+            const size_t off = (size_t)lane * NX * NY * NZ + (size_t)NX * ((size_t)ys + (size_t)NY * zs);
+            T *dst = smem + (size_t)s * stage_elems + (size_t)lane * NX;
             bulk_g2s(dst, a.pp.fa[0] + off, row_bytes, &bar[s]);
             bulk_g2s(dst + (size_t)Q * NX, a.pp.ha[0] + off, row_bytes, &bar[s]);
         }
     };
-    auto needs_copy = [&](long long r) { return r < rows && r / NY != 0; };
+    // bounded wait of the calling thread for the phase `parity` of bar[s]
+    auto wait_stage = [&](int s, unsigned parity) {
+        unsigned n = 0;
+        while (!mbar_try_wait(&bar[s], parity) && ++n < kWaitLimit) {
+        }
+        return n < kWaitLimit;
+    };
+    // rows r = NY + blockIdx.x + k gridDim.x, r < NY NZ, as (y, z); a step of
+    // gridDim.x rows advances y by gy and z by gz (plus the carry)
+    const int g = (int)gridDim.x, gy = g % NY, gz = g / NY;
+    auto advance = [&](int &yy, int &zz) {
+        yy += gy;
+        zz += gz;
+        if (yy >= NY) {
+            yy -= NY;
+            ++zz;
+        }
+    };
 
     unsigned phases = 0u;  // bit s: parity of the next phase of bar[s]
-    long long r0 = blockIdx.x;
-    if (threadIdx.x < 32) {
+    int y = (int)(blockIdx.x % NY), z = 1 + (int)(blockIdx.x / NY);
+    if (warp == 0) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        if (needs_copy(r0)) issue(r0, 0);
-        if (needs_copy(r0 + gridDim.x)) issue(r0 + gridDim.x, 1);
+        int y1 = y, z1 = z;
+        advance(y1, z1);
+        if (z < NZ) issue(y, z, 0);
+        if (z1 < NZ) issue(y1, z1, 1);
     }
-    int it = 0;
-    for (long long r = r0; r < rows; r += gridDim.x, ++it) {
+    for (int it = 0; z < NZ; ++it) {
         const int s = it & 1;
-        const int y = (int)(r % NY), z = (int)(r / NY);
         const unsigned node = (unsigned)x + (unsigned)NX * ((unsigned)y + (unsigned)NY * z);
         const ZRef<R> zr = load_zref(a.zref, z);
         PullIdx P;
         make_pull(P, x, y, z, NX, NY, NZ);
         R f[Q], h[Q];
-        if (z != 0) {
-            if (threadIdx.x == 0) {
-                unsigned n = 0;
-                while (!mbar_try_wait(&bar[s], (phases >> s) & 1u) && ++n < kWaitLimit) {
-                }
-                ok_flag = n < kWaitLimit;
+        const unsigned par = (phases >> s) & 1u;
+        if (!__all_sync(0xffffffffu, wait_stage(s, par))) {
+            if (lane == 0) {
+                atomicExch(a.err, 1);
+                // this stage's copies and the other stage's (the next row)
+                // may still be landing: bounded waits for both
+                (void)wait_stage(s, par);
+                int y1 = y, z1 = z;
+                advance(y1, z1);
+                if (z1 < NZ) (void)wait_stage(s ^ 1, (phases >> (s ^ 1)) & 1u);
             }
-            __syncthreads();
-            if (!ok_flag) {
-                if (threadIdx.x == 0) {
-                    atomicExch(a.err, 1);
-                    // copies may still be landing in this stage and in the
-                    // other one (row r + gridDim.x): bounded waits for both
-                    unsigned n = 0;
-                    while (!mbar_try_wait(&bar[s], (phases >> s) & 1u) && ++n < kWaitLimit) {
-                    }
-                    if (needs_copy(r + gridDim.x)) {
-                        n = 0;
-                        while (!mbar_try_wait(&bar[s ^ 1], (phases >> (s ^ 1)) & 1u) &&
-                               ++n < kWaitLimit) {
-                        }
-                    }
-                }
-                __syncthreads();
-                return;
-            }
-            (void)mbar_try_wait(&bar[s], (phases >> s) & 1u);  // acquire for this thread
-            phases ^= 1u << s;
+            __syncwarp();
+            return;
+        }
+        phases ^= 1u << s;
+        {
             const T *sf = smem + (size_t)s * stage_elems;
             const T *sh = sf + (size_t)Q * NX;
 #pragma unroll
@@ -550,21 +564,27 @@ lbm_rows_kernel(const StepArgs<T, R> a, const KConst<R> c) {
                 f[d] = Store<T>::lds(sf + (size_t)d * NX + xs) + c.w[cls_of(d)] * zr.dr(ez_of(d));
                 h[d] = Store<T>::lds(sh + (size_t)d * NX + xs) + c.w[cls_of(d)] * zr.dq(ez_of(d));
             }
-        } else {
-            pull_global<T, R>(f, h, a.pp, P, node, z, zr, c, false);
         }
         const Moments<R> mo = moments(f, h, zr);
         warp_plane_sum((float)mo.rho, (float)mo.charge, a.psum,
-                       ((size_t)z * NY + y) * nw + (threadIdx.x >> 5));
+                       ((size_t)z * NY + y) * nw + warp);
         finish_node<T, R, MACROS>(f, h, mo, x, y, z, node, zr, a, c, false, false);
-        // the stage is free once every thread has read it: refill it with the
-        // row two iterations ahead
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            const long long rn = r + 2LL * gridDim.x;
-            if (needs_copy(rn)) {
+        // this warp is done with the stage; the last of the nw warps refills it
+        __syncwarp();
+        unsigned last = 0u;
+        if (lane == 0) {
+            __threadfence_block();
+            last = atomicAdd(&cnt[s], 1u) == nw - 1u;
+            if (last) atomicExch(&cnt[s], 0u);
+        }
+        last = __shfl_sync(0xffffffffu, last, 0);
+        advance(y, z);  // the next row of this block
+        if (last) {
+            int y2 = y, z2 = z;
+            advance(y2, z2);
+            if (z2 < NZ) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                issue(rn, s);
+                issue(y2, z2, s);
             }
         }
     }
@@ -707,7 +727,7 @@ cudaError_t prepare_lbm_rows(int nx, int ny, int nz, int *grid) {
         (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, lbm_rows_kernel<T, R, false>, nx,
                                                            sm)) != cudaSuccess)
         return e;
-    const long long rows = (long long)ny * nz;
+    const long long rows = (long long)ny * (nz - 1);
     *grid = (int)std::min<long long>(rows, (long long)nsm * std::min(occ_a, occ_b));
     return cudaSuccess;
 }
@@ -743,7 +763,15 @@ cudaError_t launch_lbm_step(const LbmArgs &la, const StepConst &c, int local_pop
     const KConst<R> k = make_kconst<R>(c);
     const bool general = local_pops || e_arrays;
     if (!general && la.rows_grid > 0) {
-        // the shared-memory attribute was set by prepare_lbm_rows
+        // plane z = 0 on the per-node kernel, in blocks of whole warps along
+        // x so that its plane sums land in the row kernel's slots
+        // [y][x / 32]; then the planes z >= 1 on the row kernel (its
+        // shared-memory attribute was set by prepare_lbm_rows)
+        int bx = 128;
+        while (c.nx % bx != 0) bx -= 32;
+        const dim3 g0(c.nx / bx, c.ny, 1);
+        if (macros) lbm_step_kernel<T, R, false, true><<<g0, bx, 0, s>>>(a, k, 0, 0);
+        else lbm_step_kernel<T, R, false, false><<<g0, bx, 0, s>>>(a, k, 0, 0);
         const size_t sm = lbm_rows_smem(c.nx, sizeof(T));
         if (macros) lbm_rows_kernel<T, R, true><<<la.rows_grid, c.nx, sm, s>>>(a, k);
         else lbm_rows_kernel<T, R, false><<<la.rows_grid, c.nx, sm, s>>>(a, k);
