@@ -40,7 +40,10 @@ ROOT = Path(__file__).resolve().parent
 PKG = ROOT / "ehd-convection-3d_b200"
 NX, NY, NZ = 256, 256, 129  # the workload; --grid overrides it for profiling only
 NODES = NX * NY * NZ
-KERNELS_PER_STEP = 6  # lbm_step + 5 Poisson kernels (rows_fwd, cols, zsolve, cols, rows_inv)
+# kernels per step of the FP32 256-wide workload: lbm_step (plane z = 0), lbm_rows
+# (planes z >= 1), reduce_tables, and the Poisson's rows_fwd, cols, zdst, cols,
+# rows_inv
+KERNELS_PER_STEP = 8
 # Algorithmic bytes per node of one lbm_step launch (macros written, as
 # ehd_stream_collide_save does): 27 f + 27 g read and written, q written,
 # phi' read, rho/u/v/w written.  s = population bytes, p = field bytes.
@@ -48,10 +51,11 @@ def lbm_bytes_per_node(s: int, p: int) -> int:
     return 2 * 27 * 2 * s + p * (1 + 1 + 4)
 
 
-# DRAM traffic (read + write) of one lbm_step launch on the full 256x256x129 grid:
-# an ncu capture of the 256x256x33 case (profiles/lbm_step_fp32_256x256x33.md)
-# scaled by the node count.
-NCU_TRAFFIC_BYTES = 3.663e9
+# DRAM traffic (read + write) of the LBM half of one step on the full
+# 256x256x129 grid: the ncu capture of the 256x256x33 case
+# (profiles/lbm_rows_fp32_256x256x33.md), 431.4 B per node of the row kernel
+# times the 256x256x128 nodes it updates, plus the z = 0 plane's launch.
+NCU_TRAFFIC_BYTES = 3.66e9
 
 
 def reduce_max(x: float, dist=None, device="cpu") -> float:
@@ -183,7 +187,8 @@ def run_ours(args, rank, world, local_rank):
         return reduce_max(x, dist, "cuda")
 
     def device_mlups(prec, sampler_gpu=None):
-        sim = ehd.Simulation(p, prec, device=local_rank, stream=stream.cuda_stream)
+        sim = ehd.Simulation(p, prec, device=local_rank, stream=stream.cuda_stream,
+                             row_kernel=not args.node_kernel)
         cs = ClockSampler(sampler_gpu) if sampler_gpu is not None else None
         try:
             sim.set_fields(fields)
@@ -306,7 +311,9 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": round(8 + field_bytes / K),
                 "how": "ehd_set_fields from pinned host memory, K x (ehd_step(1) + "
                        "ehd_current readback), ehd_get_fields to pinned host memory; wall clock"},
-        "roofline": {"bound": "hbm", "kernel": "lbm_step_kernel<float,float>",
+        "roofline": {"bound": "hbm",
+                     "kernel": "LBM half of the step: lbm_rows_kernel<float,float> (z >= 1) + "
+                               "lbm_step_kernel (z = 0) + plane-sum reduction and tables",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "bytes_per_node": lbm_bytes_per_node(4, 4),
@@ -397,6 +404,8 @@ def main():
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--node-kernel", action="store_true",
+                    help="profiling: every LBM step on the one-thread-per-node kernel")
     ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32", "fp16", "bf16"],
                     help="storage of the headline run (profiling)")
     ap.add_argument("--grid", type=int, nargs=3, metavar=("NX", "NY", "NZ"),

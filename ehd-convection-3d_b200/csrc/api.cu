@@ -254,10 +254,9 @@ int lbm(ehd_ctx *c, bool macros) {
     // now (the same phase of the injector's two-step alternation)
     const int p = c->cur;
     const int nblk = rows ? lbm_rows_slots_per_plane(c->p.nx, c->p.ny) : c->psum_blocks;
-    e = launch_psum_reduce(c->psum, c->mean[p ^ 1], nblk, c->sc, c->stream);
-    if (e == cudaSuccess)
-        e = c->rsize == 8 ? launch_build_tables<double>(c->mean[p], c->wref[p], c->wref[p ^ 1], c->ktab[p ^ 1], c->sc, c->stream)
-                          : launch_build_tables<float>(c->mean[p], c->wref[p], c->wref[p ^ 1], c->ktab[p ^ 1], c->sc, c->stream);
+    e = c->rsize == 8
+            ? launch_reduce_tables<double>(c->psum, c->mean[p ^ 1], nblk, c->mean[p], c->wref[p], c->wref[p ^ 1], c->ktab[p ^ 1], c->sc, c->stream)
+            : launch_reduce_tables<float>(c->psum, c->mean[p ^ 1], nblk, c->mean[p], c->wref[p], c->wref[p ^ 1], c->ktab[p ^ 1], c->sc, c->stream);
     if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "reference tables: %s", cudaGetErrorString(e));
     c->cur ^= 1;
     c->pops_local = false;

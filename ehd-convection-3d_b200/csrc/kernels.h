@@ -48,11 +48,15 @@ cudaError_t launch_fields_to_compute(double *const *out_dev, void *rho, void *u,
 // step kernel's table (compute type, 10 per plane).
 cudaError_t launch_fields_plane_mean(const double *rho, const double *q, double *m,
                                      const StepConst &c, cudaStream_t s);
-cudaError_t launch_psum_reduce(const float2 *psum, double *m, int nblk, const StepConst &c,
-                               cudaStream_t s);
 template <typename R>
 cudaError_t launch_build_tables(const double *msrc, double *wdst, const double *wread,
                                 void *ktab, const StepConst &c, cudaStream_t s);
+// psum_reduce and build_tables in one launch (the tables read msrc, the
+// previous means, so the two parts are independent)
+template <typename R>
+cudaError_t launch_reduce_tables(const float2 *psum, double *m, int nblk, const double *msrc,
+                                 double *wdst, const double *wread, void *ktab,
+                                 const StepConst &c, cudaStream_t s);
 int lbm_blocks_per_plane(int nx, int ny);
 // whether the bulk-copy row kernel serves this grid and storage type
 bool lbm_rows_usable(int nx, size_t tsize);

@@ -893,29 +893,36 @@ __global__ void fields_plane_mean_kernel(const double *__restrict__ rho,
 }
 
 // Plane means from the step kernel's per-block sums (fixed order).
-__global__ void psum_reduce_kernel(const float2 *__restrict__ psum, double *__restrict__ m,
-                                   int nblk, long long nxy) {
-    __shared__ double sr[256], sq[256];
-    const int z = blockIdx.x;
+// Plane z's sums of rho and q over its nblk per-warp slots, as means, into
+// m[2z], m[2z+1]; fixed summation order.  One block of 256 threads.
+__device__ __forceinline__ void psum_reduce_block(const float2 *__restrict__ psum,
+                                                  double *__restrict__ m, int nblk, long long nxy,
+                                                  int z) {
+    __shared__ double wr[8], wq[8];
     double a = 0.0, b = 0.0;
-    for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
+    for (int i = threadIdx.x; i < nblk; i += 256) {
         const float2 v = psum[(size_t)z * nblk + i];
         a += v.x;
         b += v.y;
     }
-    sr[threadIdx.x] = a;
-    sq[threadIdx.x] = b;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) {
-            sr[threadIdx.x] += sr[threadIdx.x + o];
-            sq[threadIdx.x] += sq[threadIdx.x + o];
-        }
-        __syncthreads();
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
     }
+    if ((threadIdx.x & 31) == 0) {
+        wr[threadIdx.x >> 5] = a;
+        wq[threadIdx.x >> 5] = b;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
-        m[2 * z] = sr[0] / (double)nxy;
-        m[2 * z + 1] = sq[0] / (double)nxy;
+        double sr = 0.0, sq = 0.0;
+        for (int w = 0; w < 8; ++w) {
+            sr += wr[w];
+            sq += wq[w];
+        }
+        m[2 * z] = sr / (double)nxy;
+        m[2 * z + 1] = sq / (double)nxy;
     }
 }
 
@@ -925,8 +932,9 @@ __global__ void psum_reduce_kernel(const float2 *__restrict__ psum, double *__re
 // wdst (layout of load_zref).  The references only choose what the stored
 // deviations are relative to; any choice is exact in exact arithmetic.
 template <typename R>
-__global__ void build_tables_kernel(const double *__restrict__ msrc, double *wdst,
-                                    const double *wread, R *__restrict__ ktab, int nz) {
+__device__ __forceinline__ void build_tables_block(const double *__restrict__ msrc, double *wdst,
+                                                   const double *wread, R *__restrict__ ktab,
+                                                   int nz) {
     for (int z = threadIdx.x; z < nz; z += blockDim.x) {
         const int zs = z == nz - 1 ? nz - 2 : z;
         wdst[2 * z] = msrc[2 * zs];
@@ -950,17 +958,29 @@ __global__ void build_tables_kernel(const double *__restrict__ msrc, double *wds
     }
 }
 
+template <typename R>
+__global__ void build_tables_kernel(const double *__restrict__ msrc, double *wdst,
+                                    const double *wread, R *__restrict__ ktab, int nz) {
+    build_tables_block<R>(msrc, wdst, wread, ktab, nz);
+}
+
+// Blocks 0..nz-1: psum_reduce of plane z; block nz: build_tables (which reads
+// the previous means, not the ones reduced here).  One launch per step.
+template <typename R>
+__global__ void __launch_bounds__(256)
+reduce_tables_kernel(const float2 *__restrict__ psum, double *__restrict__ m, int nblk,
+                     long long nxy, const double *__restrict__ msrc, double *wdst,
+                     const double *wread, R *__restrict__ ktab, int nz) {
+    if ((int)blockIdx.x < nz) psum_reduce_block(psum, m, nblk, nxy, blockIdx.x);
+    else build_tables_block<R>(msrc, wdst, wread, ktab, nz);
+}
+
 cudaError_t launch_fields_plane_mean(const double *rho, const double *q, double *m,
                                      const StepConst &c, cudaStream_t s) {
     fields_plane_mean_kernel<<<c.nz, 256, 0, s>>>(rho, q, m, c.nxy);
     return cudaGetLastError();
 }
 
-cudaError_t launch_psum_reduce(const float2 *psum, double *m, int nblk, const StepConst &c,
-                               cudaStream_t s) {
-    psum_reduce_kernel<<<c.nz, 256, 0, s>>>(psum, m, nblk, c.nxy);
-    return cudaGetLastError();
-}
 
 template <typename R>
 cudaError_t launch_build_tables(const double *msrc, double *wdst, const double *wread,
@@ -968,6 +988,20 @@ cudaError_t launch_build_tables(const double *msrc, double *wdst, const double *
     build_tables_kernel<R><<<1, 256, 0, s>>>(msrc, wdst, wread, (R *)ktab, c.nz);
     return cudaGetLastError();
 }
+template <typename R>
+cudaError_t launch_reduce_tables(const float2 *psum, double *m, int nblk, const double *msrc,
+                                 double *wdst, const double *wread, void *ktab,
+                                 const StepConst &c, cudaStream_t s) {
+    reduce_tables_kernel<R><<<c.nz + 1, 256, 0, s>>>(psum, m, nblk, c.nxy, msrc, wdst, wread,
+                                                     (R *)ktab, c.nz);
+    return cudaGetLastError();
+}
+template cudaError_t launch_reduce_tables<float>(const float2 *, double *, int, const double *,
+                                                 double *, const double *, void *,
+                                                 const StepConst &, cudaStream_t);
+template cudaError_t launch_reduce_tables<double>(const float2 *, double *, int, const double *,
+                                                  double *, const double *, void *,
+                                                  const StepConst &, cudaStream_t);
 template cudaError_t launch_build_tables<float>(const double *, double *, const double *, void *,
                                                 const StepConst &, cudaStream_t);
 template cudaError_t launch_build_tables<double>(const double *, double *, const double *,
