@@ -95,6 +95,23 @@ struct KConst {
 };
 
 // ---- storage types ---------------------------------------------------------
+// Opt a kernel in to the largest dynamic shared memory the device allows.
+// The attribute belongs to the function, not to a context of this library, so
+// it is never set to one context's size: a smaller value set for one grid
+// would make another context's larger launch invalid.
+template <typename K>
+inline cudaError_t allow_max_dynamic_smem(K kern) {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kern);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 optin - (int)fa.sharedSizeBytes);
+    return e;
+}
+
 template <typename T> struct Store;
 template <> struct Store<double> {
     __device__ __forceinline__ static double ld(const double *p) { return __ldg(p); }

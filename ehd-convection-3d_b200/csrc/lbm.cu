@@ -714,10 +714,8 @@ cudaError_t prepare_lbm_rows(int nx, int ny, int nz, int *grid) {
     if (!lbm_rows_usable(nx, sizeof(T))) return cudaSuccess;
     const int sm = (int)lbm_rows_smem(nx, sizeof(T));
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(lbm_rows_kernel<T, R, true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, sm)) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(lbm_rows_kernel<T, R, false>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, sm)) != cudaSuccess)
+    if ((e = allow_max_dynamic_smem(lbm_rows_kernel<T, R, true>)) != cudaSuccess ||
+        (e = allow_max_dynamic_smem(lbm_rows_kernel<T, R, false>)) != cudaSuccess)
         return e;
     int dev = 0, nsm = 0, occ_a = 0, occ_b = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess ||

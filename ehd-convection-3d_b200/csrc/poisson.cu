@@ -696,9 +696,10 @@ poisson_zdst(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::T *
 // launcher
 // ---------------------------------------------------------------------------
 
-// Opt in to more than 48 KB of dynamic shared memory.  Skipped while the
-// stream is being captured into a graph: the attribute is set by the first,
-// uncaptured launch on the device.
+// Opt in to more than 48 KB of dynamic shared memory (to the device's
+// maximum, see allow_max_dynamic_smem).  Skipped while the stream is being
+// captured into a graph: the attribute is set by the first, uncaptured launch
+// on the device.
 template <typename K>
 static cudaError_t set_smem(K kern, size_t bytes, cudaStream_t s) {
     if (bytes <= 48 * 1024) return cudaSuccess;
@@ -706,7 +707,7 @@ static cudaError_t set_smem(K kern, size_t bytes, cudaStream_t s) {
     cudaError_t e = cudaStreamIsCapturing(s, &st);
     if (e != cudaSuccess) return e;
     if (st != cudaStreamCaptureStatusNone) return cudaSuccess;
-    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    return allow_max_dynamic_smem(kern);
 }
 
 bool poisson_fast_size(int n) { return n == 64 || n == 128 || n == 256 || n == 512; }

@@ -79,3 +79,37 @@ def test_row_kernel_graphs_and_direct_launches_agree_bitwise():
             out.append(sim.get_fields())
     for k in O.FIELDS:
         assert np.array_equal(out[0][k], out[1][k]), k
+
+
+def test_contexts_of_different_sizes_share_kernels():
+    """Kernel attributes are per function, not per context: contexts of
+    different widths created one after the other (the larger first) must all
+    still launch.  96- and 64-wide FP32 grids share the row kernel; 480- and
+    384-wide FP64 grids share the run-time-radix row FFT, each with more than
+    48 KB of shared memory."""
+    cases = [((96, 16, 9), "fp32"), ((64, 16, 9), "fp32"), ((480, 6, 5), "fp64"),
+             ((384, 6, 5), "fp64")]
+    sims, refs = [], []
+    for (nx, ny, nz), prec in cases:
+        dz = 1.0 / (nz - 1)
+        p = O.params_from_groups(nx, ny, nz, nx * dz, ny * dz, T=200, M=10, C=10, Fe=4000)
+        f = random_fields(p, 7)
+        sim = ehd.Simulation(to_ehd(p), prec)
+        sim.set_fields(f)
+        sims.append(sim)
+        o = O.Oracle(p)
+        o.set_fields(f)
+        o.step(3)
+        refs.append(o.get_fields())
+    try:
+        for k in range(3):
+            for sim in sims:
+                sim.step(1)
+        for ((shape, prec), sim, ref) in zip(cases, sims, refs):
+            out = sim.get_fields()
+            tol = 1e-10 if prec == "fp64" else 1e-5
+            for k in ("q", "phi"):
+                assert relerr(out[k], ref[k]) < tol, (shape, prec, k, relerr(out[k], ref[k]))
+    finally:
+        for sim in sims:
+            sim.close()
