@@ -109,7 +109,9 @@ struct ehd_ctx {
     void *ktab[2] = {nullptr, nullptr};
     float2 *psum = nullptr;
     int psum_blocks = 0;   // psum slots per plane of the per-node kernel
-    int rows_grid = 0;     // CTAs of the bulk-copy row kernel, 0: not used
+    int rows_grid = 0;     // CTAs of the bulk-copy row kernel, 0: not available
+    ehd_tuning tune{};     // launch shapes (ehd_set_tuning)
+    unsigned generation = 0;  // bumped by ehd_set_tuning
     int *err = nullptr;    // device flag set by a row-kernel wait that gave up
     double *out[9] = {};
     double **out_dev = nullptr;
@@ -239,8 +241,9 @@ int lbm(ehd_ctx *c, bool macros) {
     a.psum = c->psum;
     a.err = c->err;
     const int loc = c->pops_local ? 1 : 0, ea = c->e_arrays ? 1 : 0;
-    const bool rows = c->rows_grid > 0 && !loc && !ea;
+    const bool rows = c->rows_grid > 0 && c->tune.lbm_kernel == 0 && !loc && !ea;
     a.rows_grid = rows ? c->rows_grid : 0;
+    a.node_bx = c->tune.node_block_x;
     cudaError_t e = cudaErrorInvalidValue;
     switch (c->prec) {
         case EHD_PREC_FP64: e = launch_lbm_step<double, double>(a, c->sc, loc, ea, macros, c->stream); break;
@@ -254,6 +257,7 @@ int lbm(ehd_ctx *c, bool macros) {
     // now (the same phase of the injector's two-step alternation)
     const int p = c->cur;
     const int nblk = rows ? lbm_rows_slots_per_plane(c->p.nx, c->p.ny) : c->psum_blocks;
+    // (psum_blocks follows the node kernel's block shape, see ehd_set_tuning)
     e = c->rsize == 8
             ? launch_reduce_tables<double>(c->psum, c->mean[p ^ 1], nblk, c->mean[p], c->wref[p], c->wref[p ^ 1], c->ktab[p ^ 1], c->sc, c->stream)
             : launch_reduce_tables<float>(c->psum, c->mean[p ^ 1], nblk, c->mean[p], c->wref[p], c->wref[p ^ 1], c->ktab[p ^ 1], c->sc, c->stream);
@@ -371,7 +375,31 @@ int materialize(ehd_ctx *c) {
 
 }  // namespace
 
+namespace ehd {
+cudaStream_t ctx_stream(const ehd_ctx *c) { return c->stream; }
+int ctx_device(const ehd_ctx *c) { return c->device; }
+int ctx_precision(const ehd_ctx *c) { return c->prec; }
+bool ctx_steady(const ehd_ctx *c) { return c->have_state && !c->pops_local && !c->e_arrays; }
+int ctx_parity(const ehd_ctx *c) { return c->cur; }
+int ctx_launch_step(ehd_ctx *c, bool macros) {
+    const int cur0 = c->cur;
+    int r = lbm(c, macros);
+    if (r == EHD_OK) r = poisson(c);
+    c->cur = cur0;
+    return r;
+}
+unsigned ctx_generation(const ehd_ctx *c) { return c->generation; }
+double ctx_reference_current(const ehd_ctx *c) { return c->i0; }
+void ctx_commit_step(ehd_ctx *c) {
+    c->cur ^= 1;
+    c->step += 1;
+    c->t += c->p.dt;
+    c->out_valid = false;
+}
+}  // namespace ehd
+
 extern "C" {
+
 
 int ehd_abi_version(void) { return EHD_ABI_VERSION; }
 
@@ -455,8 +483,10 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
         if ((r = dalloc(c, (void **)&c->mean[i], sizeof(double) * 2 * nz))) return bail(r);
         if ((r = dalloc(c, &c->ktab[i], c->rsize * 10 * nz))) return bail(r);
     }
-    c->psum_blocks = lbm_blocks_per_plane(nx, ny);
-    if (!(cfg.flags & EHD_FLAG_NODE_KERNEL)) {
+    c->tune.lbm_kernel = (cfg.flags & EHD_FLAG_NODE_KERNEL) ? 1 : 0;
+    c->tune.node_block_x = lbm_default_block_x(nx);
+    c->psum_blocks = lbm_blocks_per_plane(nx, ny, c->tune.node_block_x);
+    {
         // the bulk-copy row kernel for steady-state steps, where it applies
         cudaError_t e = cudaSuccess;
         switch (c->prec) {
@@ -468,7 +498,9 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
         if (e != cudaSuccess) return bail(fail(EHD_ERR_CUDA, "row kernel set-up: %s", cudaGetErrorString(e)));
     }
     {
-        const int slots = std::max(c->psum_blocks, c->rows_grid > 0 ? lbm_rows_slots_per_plane(nx, ny) : 0);
+        // room for the plane sums of every launch shape ehd_set_tuning allows
+        int slots = c->rows_grid > 0 ? lbm_rows_slots_per_plane(nx, ny) : 0;
+        for (int bx = 16; bx <= 128; bx *= 2) slots = std::max(slots, lbm_blocks_per_plane(nx, ny, bx));
         if ((r = dalloc(c, (void **)&c->psum, sizeof(float2) * (size_t)slots * nz))) return bail(r);
     }
     if ((r = dalloc(c, (void **)&c->err, sizeof(int)))) return bail(r);
@@ -495,6 +527,8 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
         pa.cols_per_block = cols;
         if ((size_t)2 * rows * nx * c2 > 200 * 1024 || (size_t)2 * cols * ny * c2 > 200 * 1024)
             return bail(fail(EHD_ERR_INVALID, "nx or ny too large for the in-shared-memory FFT"));
+        c->tune.fft_rows = rows;
+        c->tune.fft_cols = cols;
     }
     pa.px = make_plan(nx);
     pa.py = make_plan(ny);
@@ -626,6 +660,36 @@ int ehd_destroy(ehd_ctx *c) {
 int ehd_device_bytes(const ehd_ctx *c, size_t *bytes) {
     if (!c || !bytes) return fail(EHD_ERR_INVALID, "NULL argument");
     *bytes = c->bytes;
+    return EHD_OK;
+}
+
+int ehd_get_tuning(const ehd_ctx *c, ehd_tuning *t) {
+    if (!c || !t) return fail(EHD_ERR_INVALID, "NULL argument");
+    *t = c->tune;
+    return EHD_OK;
+}
+
+int ehd_set_tuning(ehd_ctx *c, const ehd_tuning *t) {
+    if (!c || !t) return fail(EHD_ERR_INVALID, "NULL argument");
+    if (t->lbm_kernel != 0 && t->lbm_kernel != 1) return fail(EHD_ERR_INVALID, "lbm_kernel must be 0 or 1");
+    const int bx = t->node_block_x;
+    if (bx != 16 && bx != 32 && bx != 64 && bx != 128)
+        return fail(EHD_ERR_INVALID, "node_block_x must be 16, 32, 64 or 128 (got %d)", bx);
+    const size_t c2 = 2 * c->rsize;
+    if (t->fft_rows < 1 || t->fft_cols < 1 ||
+        (size_t)2 * t->fft_rows * c->p.nx * c2 > 200 * 1024 ||
+        (size_t)2 * t->fft_cols * c->p.ny * c2 > 200 * 1024)
+        return fail(EHD_ERR_INVALID, "fft_rows/fft_cols out of range for the shared-memory FFT");
+    for (int i : t->reserved)
+        if (i != 0) return fail(EHD_ERR_INVALID, "reserved fields must be 0");
+    DeviceGuard dg(c->device);
+    EHD_CK(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);
+    c->tune = *t;
+    c->generation += 1;
+    c->psum_blocks = lbm_blocks_per_plane(c->p.nx, c->p.ny, bx);
+    c->pa.rows_per_block = t->fft_rows;
+    c->pa.cols_per_block = t->fft_cols;
     return EHD_OK;
 }
 

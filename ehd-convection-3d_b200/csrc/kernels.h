@@ -19,6 +19,7 @@ struct LbmArgs {
     int *err;                       // device flag: a bounded wait gave up
     int rows_grid;                  // > 0: steady-state steps run the bulk-copy
                                     // row kernel on this many CTAs
+    int node_bx;                    // per-node kernel block: node_bx x (128 / node_bx)
 };
 
 template <typename T, typename R>
@@ -57,7 +58,10 @@ template <typename R>
 cudaError_t launch_reduce_tables(const float2 *psum, double *m, int nblk, const double *msrc,
                                  double *wdst, const double *wread, void *ktab,
                                  const StepConst &c, cudaStream_t s);
-int lbm_blocks_per_plane(int nx, int ny);
+// psum slots per plane of the per-node kernel with blocks of bx x (128 / bx)
+int lbm_blocks_per_plane(int nx, int ny, int bx);
+// the per-node kernel's default block width for a grid nx wide
+int lbm_default_block_x(int nx);
 // whether the bulk-copy row kernel serves this grid and storage type
 bool lbm_rows_usable(int nx, size_t tsize);
 // sets the row kernel's shared-memory attribute (before any stream capture)
@@ -138,5 +142,22 @@ namespace ehd {
 // a context's parameters and its physical time (for the text writers)
 const ::ehd_params *ctx_params(const ::ehd_ctx *c);
 double *ctx_time(::ehd_ctx *c);
+
+// For the batch (csrc/batch.cu): a context's stream, device and precision;
+// whether its next step can be captured (not the first after an upload);
+// its buffer parity; the launches of one steady step on its stream with the
+// buffer parity left unchanged (as a graph capture needs); and the
+// bookkeeping once that step has run.
+cudaStream_t ctx_stream(const ::ehd_ctx *c);
+int ctx_device(const ::ehd_ctx *c);
+int ctx_precision(const ::ehd_ctx *c);
+bool ctx_steady(const ::ehd_ctx *c);
+int ctx_parity(const ::ehd_ctx *c);
+int ctx_launch_step(::ehd_ctx *c, bool macros);
+void ctx_commit_step(::ehd_ctx *c);
+// changes whenever the context's launches change (ehd_set_tuning), so that
+// captured graphs holding them are rebuilt
+unsigned ctx_generation(const ::ehd_ctx *c);
+double ctx_reference_current(const ::ehd_ctx *c);
 
 }  // namespace ehd

@@ -461,9 +461,9 @@ __device__ __forceinline__ int ez_rt(int d) { return (int)((kEzPack >> (2 * d)) 
 // No block-wide barrier in the loop: each warp waits for its stage on the
 // stage's mbarrier, reads its 54 values into registers and counts itself out
 // of the stage (shared counter); the warp that counts last refills the stage
-// with the row two iterations ahead while the others compute.  The rows of
-// the injector plane z = 0 (own-node g and z = 1 populations) follow at the
-// end, pulled from global memory.  A wait that does not complete within
+// with the row two iterations ahead while the others compute.  The injector
+// plane z = 0 (own-node g and z = 1 populations) is left to the per-node
+// kernel, launched for that plane alone.  A wait that does not complete within
 // kWaitLimit polls sets *err, waits (bounded) for the copies that may still
 // be landing, and ends the warp.
 template <typename T, typename R, bool MACROS>
@@ -775,7 +775,8 @@ cudaError_t launch_lbm_step(const LbmArgs &la, const StepConst &c, int local_pop
         else lbm_rows_kernel<T, R, false><<<la.rows_grid, c.nx, sm, s>>>(a, k);
         return cudaGetLastError();
     }
-    dim3 block(c.nx >= 64 ? 64 : 32, c.nx >= 64 ? 2 : 4, 1);
+    const int bx = la.node_bx > 0 ? la.node_bx : lbm_default_block_x(c.nx);
+    dim3 block(bx, 128 / bx, 1);
     dim3 grid((c.nx + block.x - 1) / block.x, (c.ny + block.y - 1) / block.y, c.nz);
 #define EHD_LAUNCH(G, M) lbm_step_kernel<T, R, G, M><<<grid, block, 0, s>>>(a, k, local_pops, e_arrays)
     if (general) {
@@ -1006,8 +1007,10 @@ template cudaError_t launch_build_tables<double>(const double *, double *, const
                                                  void *, const StepConst &, cudaStream_t);
 
 // number of per-warp partial sums per plane written by the step kernel
-int lbm_blocks_per_plane(int nx, int ny) {
-    const int bx = nx >= 64 ? 64 : 32, by = nx >= 64 ? 2 : 4;
+int lbm_default_block_x(int nx) { return nx >= 64 ? 64 : 32; }
+
+int lbm_blocks_per_plane(int nx, int ny, int bx) {
+    const int by = 128 / bx;
     return ((nx + bx - 1) / bx) * ((ny + by - 1) / by) * 4;
 }
 

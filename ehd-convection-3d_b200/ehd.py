@@ -74,6 +74,15 @@ class Diag(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad_"}
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("lbm_kernel", ctypes.c_int32), ("node_block_x", ctypes.c_int32),
+                ("fft_rows", ctypes.c_int32), ("fft_cols", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 4)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 # every symbol include/ehd.h declares, with (restype, argtypes)
 _dp = ctypes.POINTER(ctypes.c_double)
 _vp = ctypes.c_void_p
@@ -106,6 +115,19 @@ SIGNATURES = {
     "ehd_write_data_end": (_i, [_vp, ctypes.c_char_p]),
     "ehd_read_data_end": (_i, [_vp, ctypes.c_char_p]),
     "ehd_write_tecplot": (_i, [_vp, ctypes.c_char_p, _i]),
+    "ehd_get_tuning": (_i, [_vp, ctypes.POINTER(Tuning)]),
+    "ehd_set_tuning": (_i, [_vp, ctypes.POINTER(Tuning)]),
+    "ehd_batch_create": (_i, [ctypes.POINTER(Params), _i, ctypes.POINTER(Config),
+                              ctypes.POINTER(_vp)]),
+    "ehd_batch_destroy": (_i, [_vp]),
+    "ehd_batch_size": (_i, [_vp]),
+    "ehd_batch_instance": (_i, [_vp, _i, ctypes.POINTER(_vp)]),
+    "ehd_batch_set_active": (_i, [_vp, _i, _i]),
+    "ehd_batch_step": (_i, [_vp, _i]),
+    "ehd_batch_run_to_saturation": (_i, [_vp, _i, ctypes.c_double, _i, ctypes.c_int64,
+                                         ctypes.POINTER(ctypes.c_int32),
+                                         ctypes.POINTER(ctypes.c_int64), _dp]),
+    "ehd_batch_autotune": (_i, [_vp, _i]),
 }
 
 _lib = None
@@ -187,10 +209,22 @@ class Simulation:
         h = _vp()
         _check(lib().ehd_create(ctypes.byref(params), ctypes.byref(cfg), ctypes.byref(h)))
         self.h = h
+        self.owned = True
+
+    @classmethod
+    def _view(cls, handle, params: Params):
+        """A context owned by someone else (a Batch instance)."""
+        sim = cls.__new__(cls)
+        sim.p = params
+        sim.shape = (params.nz, params.ny, params.nx)
+        sim.h = handle
+        sim.owned = False
+        return sim
 
     def close(self):
         if getattr(self, "h", None):
-            lib().ehd_destroy(self.h)
+            if getattr(self, "owned", True):
+                lib().ehd_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -273,7 +307,79 @@ class Simulation:
     def write_tecplot(self, path, first=True):
         _check(lib().ehd_write_tecplot(self.h, str(path).encode(), int(bool(first))))
 
+    def get_tuning(self) -> dict:
+        t = Tuning()
+        _check(lib().ehd_get_tuning(self.h, ctypes.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        t = Tuning()
+        _check(lib().ehd_get_tuning(self.h, ctypes.byref(t)))
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        _check(lib().ehd_set_tuning(self.h, ctypes.byref(t)))
+
     def device_bytes(self) -> int:
         b = ctypes.c_size_t()
         _check(lib().ehd_device_bytes(self.h, ctypes.byref(b)))
         return b.value
+
+
+class Batch:
+    """Independent instances on one GPU, stepped together (ehd_batch)."""
+
+    def __init__(self, params: list, precision: str = "fp32", device: int = 0):
+        arr = (Params * len(params))(*params)
+        cfg = Config(precision=PRECISIONS[precision], device=device)
+        h = _vp()
+        _check(lib().ehd_batch_create(arr, len(params), ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+        self.params = list(params)
+        self.instances = []
+        for i, p in enumerate(self.params):
+            c = _vp()
+            _check(lib().ehd_batch_instance(self.h, i, ctypes.byref(c)))
+            self.instances.append(Simulation._view(c, p))
+
+    def __len__(self):
+        return len(self.instances)
+
+    def __getitem__(self, i) -> Simulation:
+        return self.instances[i]
+
+    def set_active(self, i: int, active: bool):
+        _check(lib().ehd_batch_set_active(self.h, int(i), int(bool(active))))
+
+    def step(self, n: int = 1):
+        _check(lib().ehd_batch_step(self.h, int(n)))
+
+    def autotune(self, trial_steps: int = 20):
+        _check(lib().ehd_batch_autotune(self.h, int(trial_steps)))
+
+    def run_to_saturation(self, sample_every=1000, tol=1e-3, hold=3, max_steps=10**7):
+        n = len(self)
+        sat = (ctypes.c_int32 * n)()
+        steps = (ctypes.c_int64 * n)()
+        nu = (ctypes.c_double * n)()
+        _check(lib().ehd_batch_run_to_saturation(self.h, int(sample_every), float(tol),
+                                                 int(hold), int(max_steps), sat, steps, nu))
+        return [{"saturated": bool(sat[i]), "steps": steps[i], "nu_e": nu[i]} for i in range(n)]
+
+    def close(self):
+        if getattr(self, "h", None):
+            for sim in self.instances:
+                sim.h = None
+            lib().ehd_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -79,6 +79,20 @@ typedef struct ehd_config {
 
 typedef struct ehd_ctx ehd_ctx;
 
+/* Launch shapes of a context's kernels.  No reference counterpart: the
+ * reference fixes its launch shape at compile time (nThreads, LBM.h).  A
+ * shape changes only the order of the FP32 partial plane sums behind the
+ * per-plane reference states, i.e. results at round-off level. */
+typedef struct ehd_tuning {
+    int32_t lbm_kernel;      /* 0: steady steps on the row kernel where it
+                                applies, else the per-node kernel; 1: per-node */
+    int32_t node_block_x;    /* per-node kernel block: x extent 16, 32, 64 or
+                                128, y extent 128 / node_block_x              */
+    int32_t fft_rows;        /* run-time-radix x FFT: rows per block          */
+    int32_t fft_cols;        /* run-time-radix y FFT: columns per block       */
+    int32_t reserved[4];     /* must be 0                                     */
+} ehd_tuning;
+
 /* Scalar diagnostics, reduced on the device in FP64. */
 typedef struct ehd_diag {
     double current;          /* I = K dy^2 sum_xy q(NZ-1) Ez(NZ-1), LBM.cu:1647 */
@@ -203,6 +217,48 @@ int ehd_write_tecplot(ehd_ctx *ctx, const char *path, int first);
 
 /* Message of the last failed call on this thread ("" if none). */
 const char *ehd_last_error(void);
+
+/* ---- Batches of instances (parameter sweeps) ------------------------------
+ * No reference counterpart: the reference runs one instance per process.  A
+ * batch holds n independent instances (each an ehd_ctx, any grid, one GPU),
+ * steps all active ones together -- one CUDA graph launch per step, holding
+ * every instance's kernels as parallel branches -- and runs them to
+ * saturation of Nu_e, each stopping on its own. */
+typedef struct ehd_batch ehd_batch;
+
+/* n instances from params[0..n-1]; config applies to each (its stream is
+ * ignored: every instance gets a stream of its own). */
+int ehd_batch_create(const ehd_params *params, int n, const ehd_config *config,
+                     ehd_batch **out);
+int ehd_batch_destroy(ehd_batch *batch);
+int ehd_batch_size(const ehd_batch *batch);
+/* Instance i as a context (set its state, diagnostics, checkpoints ...); the
+ * batch owns it. */
+int ehd_batch_instance(ehd_batch *batch, int i, ehd_ctx **ctx);
+int ehd_batch_set_active(ehd_batch *batch, int i, int active);
+/* nsteps steps of every active instance.  Instances whose next step is the
+ * first after an upload take that step on their own streams; after it, one
+ * graph launch per step covers all active instances. */
+int ehd_batch_step(ehd_batch *batch, int nsteps);
+/* ehd_run_to_saturation for every active instance at once: each instance
+ * stops when it saturates or reaches max_steps; saturated[i], steps[i] and
+ * nu_e[i] as there (entries of inactive instances untouched).  Needs I0 set
+ * on every active instance. */
+int ehd_batch_run_to_saturation(ehd_batch *batch, int sample_every, double tol, int hold,
+                                int64_t max_steps, int32_t *saturated, int64_t *steps,
+                                double *nu_e);
+/* Autotuner: times batch steps (trial_steps each) of a scratch batch with
+ * the same parameters while it varies, one distinct grid at a time, the
+ * launch shapes of that grid's instances (row or per-node kernel, per-node
+ * block, run-time-radix FFT batches), keeps what is faster, and applies the
+ * result to every instance of that grid (ehd_get_tuning reads the choice).
+ * The instances' states are not touched. */
+int ehd_batch_autotune(ehd_batch *batch, int trial_steps);
+
+/* The context's launch shapes (defaults chosen at ehd_create) and a change
+ * of them; no reference counterpart (see ehd_tuning). */
+int ehd_get_tuning(const ehd_ctx *ctx, ehd_tuning *out);
+int ehd_set_tuning(ehd_ctx *ctx, const ehd_tuning *tuning);
 
 /* Bytes of device memory the context holds. */
 int ehd_device_bytes(const ehd_ctx *ctx, size_t *bytes);
