@@ -262,9 +262,13 @@ int ehd_batch_run_to_saturation(ehd_batch *b, int sample_every, double tol, int 
             if (!run[i]) continue;
             ehd_diag d{};
             if ((r = ehd_diagnostics(b->inst[i], &d)) != EHD_OK) return r;
-            if (d.nonfinite) return err(EHD_ERR_NUMERIC, "ehd_batch_run_to_saturation: non-finite field");
             last[i] = d.nu_e;
             if (steps) steps[i] = done;
+            if (d.nonfinite) {  // this instance stops; the others go on
+                ok[i] = -1;
+                run[i] = 0;
+                continue;
+            }
             if (!first[i] && std::fabs(d.nu_e - prev[i]) <= tol * std::fabs(d.nu_e)) {
                 if (++held[i] >= hold) {
                     ok[i] = 1;

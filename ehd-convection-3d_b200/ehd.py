@@ -363,7 +363,9 @@ class Batch:
         nu = (ctypes.c_double * n)()
         _check(lib().ehd_batch_run_to_saturation(self.h, int(sample_every), float(tol),
                                                  int(hold), int(max_steps), sat, steps, nu))
-        return [{"saturated": bool(sat[i]), "steps": steps[i], "nu_e": nu[i]} for i in range(n)]
+        # saturated: True, False (budget used up) or None (a field went non-finite)
+        st = {1: True, 0: False, -1: None}
+        return [{"saturated": st[sat[i]], "steps": steps[i], "nu_e": nu[i]} for i in range(n)]
 
     def close(self):
         if getattr(self, "h", None):

@@ -241,9 +241,10 @@ int ehd_batch_set_active(ehd_batch *batch, int i, int active);
  * graph launch per step covers all active instances. */
 int ehd_batch_step(ehd_batch *batch, int nsteps);
 /* ehd_run_to_saturation for every active instance at once: each instance
- * stops when it saturates or reaches max_steps; saturated[i], steps[i] and
- * nu_e[i] as there (entries of inactive instances untouched).  Needs I0 set
- * on every active instance. */
+ * stops when it saturates, reaches max_steps or has a non-finite field;
+ * saturated[i] is 1, 0 or -1 for these, steps[i] and nu_e[i] as in
+ * ehd_run_to_saturation (entries of inactive instances untouched).  Needs I0
+ * set on every active instance. */
 int ehd_batch_run_to_saturation(ehd_batch *batch, int sample_every, double tol, int hold,
                                 int64_t max_steps, int32_t *saturated, int64_t *steps,
                                 double *nu_e);
