@@ -56,6 +56,10 @@ CASES = {
                         **_GROUPS),
     # the small production-like case: 64 x 64 x 33, hydrostatic + seeded noise
     "config0": dict(nx=64, ny=64, nz=33, threads=64, flag=1, **_GROUPS),
+    # 64 x 64 x 33 at T=400 (M=10, C=10, Fe=4000) with the reference's own
+    # magic parameters: the developed-convection run to non-finite fields
+    "config0_t400": dict(nx=64, ny=64, nz=33, threads=64, flag=1, nu=0.0625, K=2.5e-5,
+                         charge0=10.0, diffu=6.25e-5, V=1.0 / 12.0, VC=1.0e-6),
     # timing only: 256 x 256 x 129, reference initialisation, no text output
     "bench": dict(nx=256, ny=256, nz=129, threads=128, flag=0, no_output=True, **_GROUPS),
 }
