@@ -1,0 +1,52 @@
+// gemm_bf16.cuh -- batched matrix product on the BF16 tensor cores with FP32
+// accumulation, for the Fourier neural operator (csrc/fno.cu).
+//
+// C[m][n] = alpha * sum_k A[m][k] B[k][n] (+ beta C) (+ bias[n]), optionally
+// with a second output gelu(C), over a batch of independent products.  Every
+// index of every operand goes through a two-level map i -> (i / g) s1 +
+// (i % g) s0, so one kernel serves transposed operands and the layouts of the
+// FNO's truncated transforms, whose real/imaginary index sits above the
+// transformed axis.  A and B are read as FP32 or BF16 and rounded to BF16 in
+// shared memory; products accumulate in FP32 (mma.sync m16n8k16).  With
+// ksplit > 1 the K range is split over blocks that add into C atomically
+// (beta must then be 1, no bias, no second output).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+namespace ehd {
+namespace fno {
+
+struct Map {
+    long long s0 = 1, s1 = 0;
+    int g = 1 << 30;
+};
+__host__ __device__ __forceinline__ long long at(const Map &d, long long i) {
+    return (i / d.g) * d.s1 + (i % d.g) * d.s0;
+}
+inline Map lin(long long s0) { return Map{s0, 0, 1 << 30}; }
+inline Map two(long long s0, int g, long long s1) { return Map{s0, s1, g}; }
+
+struct GemmArgs {
+    int M = 0, N = 0, K = 0, batch = 1, ksplit = 1;
+    const void *A = nullptr;
+    Map am, ak, abat;
+    int a_bf16 = 0;
+    const void *B = nullptr;
+    Map bk, bn, bbat;
+    int b_bf16 = 0;
+    float *C = nullptr;
+    Map cm, cn, cbat;
+    float alpha = 1.f, beta = 0.f;
+    const float *bias = nullptr;  // per column n
+    float *C2 = nullptr;          // gelu(C), same indexing
+    // elements in the A, B and C (and C2) buffers: gemm() rejects a product
+    // whose largest offset falls outside them
+    long long a_n = 0, b_n = 0, c_n = 0;
+};
+
+cudaError_t gemm(const GemmArgs &a, cudaStream_t s);
+
+}  // namespace fno
+}  // namespace ehd

@@ -1,0 +1,146 @@
+"""ctypes binding of include/ehd_fno.h: the Fourier neural operator warm start.
+
+Tensors cross the boundary as CUDA device pointers; torch tensors are the
+container here (channels-last FP32, [batch][z][y][x][channel]).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+import ehd
+
+_i = ctypes.c_int
+_vp = ctypes.c_void_p
+_fp = ctypes.POINTER(ctypes.c_float)
+_i64 = ctypes.c_int64
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+                ("in_channels", ctypes.c_int32), ("out_channels", ctypes.c_int32),
+                ("width", ctypes.c_int32), ("layers", ctypes.c_int32),
+                ("modes_x", ctypes.c_int32), ("modes_y", ctypes.c_int32),
+                ("modes_z", ctypes.c_int32), ("hidden", ctypes.c_int32),
+                ("max_batch", ctypes.c_int32), ("seed", ctypes.c_uint64),
+                ("device", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
+
+
+# every symbol include/ehd_fno.h declares, with (restype, argtypes)
+SIGNATURES = {
+    "ehd_fno_create": (_i, [ctypes.POINTER(Config), ctypes.POINTER(_vp)]),
+    "ehd_fno_destroy": (_i, [_vp]),
+    "ehd_fno_param_count": (_i, [_vp, ctypes.POINTER(_i64)]),
+    "ehd_fno_get_params": (_i, [_vp, _fp]),
+    "ehd_fno_set_params": (_i, [_vp, _fp]),
+    "ehd_fno_forward": (_i, [_vp, _i, _vp, _vp]),
+    "ehd_fno_backward": (_i, [_vp, _i, _vp, _vp, ctypes.POINTER(ctypes.c_double)]),
+    "ehd_fno_get_grads": (_i, [_vp, _fp]),
+    "ehd_fno_adam_step": (_i, [_vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                               ctypes.c_float]),
+    "ehd_fno_synchronize": (_i, [_vp]),
+    "ehd_bf16_gemm": (_i, [_i, _i, _i, _i, _vp, _i64, _i64, _i64, _vp, _i64, _i64, _i64, _vp,
+                           _i64, _i64, _i64, ctypes.c_float, ctypes.c_float, _vp]),
+}
+
+_bound = False
+
+
+def lib():
+    global _bound
+    L = ehd.lib()
+    if not _bound:
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _bound = True
+    return L
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(_fp)
+
+
+def gemm(A, B, C, alpha=1.0, beta=0.0):
+    """C[b] = alpha A[b] @ B[b] + beta C[b] on the BF16 tensor cores, for
+    3-D CUDA float32 tensors (any strides)."""
+    bt, M, K = A.shape
+    _, _, N = B.shape
+    ehd._check(lib().ehd_bf16_gemm(M, N, K, bt, A.data_ptr(), A.stride(1), A.stride(2),
+                                   A.stride(0), B.data_ptr(), B.stride(1), B.stride(2),
+                                   B.stride(0), C.data_ptr(), C.stride(1), C.stride(2),
+                                   C.stride(0), float(alpha), float(beta), None))
+
+
+class FNO:
+    """One Fourier neural operator (ehd_fno) on one GPU."""
+
+    def __init__(self, nx, ny, nz, in_channels, out_channels, width=32, layers=4, modes=(12, 12, 12),
+                 hidden=128, max_batch=4, seed=0, device=0):
+        self.cfg = Config(nx=nx, ny=ny, nz=nz, in_channels=in_channels,
+                          out_channels=out_channels, width=width, layers=layers,
+                          modes_x=modes[0], modes_y=modes[1], modes_z=modes[2], hidden=hidden,
+                          max_batch=max_batch, seed=seed, device=device)
+        h = _vp()
+        ehd._check(lib().ehd_fno_create(ctypes.byref(self.cfg), ctypes.byref(h)))
+        self.h = h
+        n = _i64()
+        ehd._check(lib().ehd_fno_param_count(self.h, ctypes.byref(n)))
+        self.nparam = n.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ehd_fno_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.nparam, np.float32)
+        ehd._check(lib().ehd_fno_get_params(self.h, _fptr(out)))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.nparam
+        ehd._check(lib().ehd_fno_set_params(self.h, _fptr(p)))
+
+    def grads(self) -> np.ndarray:
+        out = np.empty(self.nparam, np.float32)
+        ehd._check(lib().ehd_fno_get_grads(self.h, _fptr(out)))
+        return out
+
+    def forward(self, a):
+        """a: CUDA float32 [batch, nz, ny, nx, in_channels] -> u of out_channels."""
+        import torch
+        a = a.contiguous()
+        u = torch.empty(a.shape[:-1] + (self.cfg.out_channels,), dtype=torch.float32,
+                        device=a.device)
+        ehd._check(lib().ehd_fno_forward(self.h, a.shape[0], a.data_ptr(), u.data_ptr()))
+        self.synchronize()
+        return u
+
+    def backward(self, a, target) -> float:
+        a, target = a.contiguous(), target.contiguous()
+        loss = ctypes.c_double()
+        ehd._check(lib().ehd_fno_backward(self.h, a.shape[0], a.data_ptr(), target.data_ptr(),
+                                          ctypes.byref(loss)))
+        return loss.value
+
+    def adam_step(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8):
+        ehd._check(lib().ehd_fno_adam_step(self.h, lr, beta1, beta2, eps))
+
+    def synchronize(self):
+        ehd._check(lib().ehd_fno_synchronize(self.h))

@@ -29,6 +29,7 @@ def _load(name, path):
 
 
 ehd = _load("ehd", PKG / "ehd.py")
+fno = _load("ehd_fno_binding", PKG / "fno.py")
 import oracle as O  # noqa: E402
 
 

@@ -82,3 +82,16 @@ def test_create_without_gpu_reports_cuda_error():
     with pytest.raises(ehd.EhdError) as e:
         ehd.Simulation(p, "fp32")
     assert e.value.code in (-1, -2)
+
+
+def test_fno_header_is_exported_and_bound():
+    from conftest import fno
+    text = re.sub(r"/\*.*?\*/", "", (ROOT / "include" / "ehd_fno.h").read_text(), flags=re.S)
+    names = sorted(set(re.findall(r"\b(ehd_[a-z_0-9]+)\s*\(", text)))
+    assert len(names) >= 10
+    out = subprocess.run(["nm", "-D", "--defined-only", str(ehd.LIB_PATH)], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(re.findall(r"\bT (ehd_\w+)", out))
+    assert not [n for n in names if n not in exported]
+    assert sorted(fno.SIGNATURES) == names
+    fno.lib()  # binds every signature
