@@ -70,7 +70,7 @@ def targets(f, p):
 
 
 def trajectories(ehd, groups, horizon, chunk=64, transits=4.0, precision="fp32", device=0,
-                 extra=0):
+                 extra=0, grid=(64, 64, 33)):
     """(inputs, targets, per-instance info) for the groups; instances whose
     fields go non-finite are dropped.  With extra > 0 the runs go on `extra`
     steps past the horizon and info records Nu_e there too."""
@@ -78,7 +78,7 @@ def trajectories(ehd, groups, horizon, chunk=64, transits=4.0, precision="fp32",
     ins, outs, info = [], [], []
     for c0 in range(0, len(groups), chunk):
         gs = groups[c0:c0 + chunk]
-        ps = [params_of(ehd, g) for g in gs]
+        ps = [params_of(ehd, g, *grid) for g in gs]
         starts = sweep.hydrostatic_profiles(ehd, ps, [sweep.hydrostatic_steps(p, transits)
                                                       for p in ps], device=device)
         with ehd.Batch(ps, precision, device=device) as b:
@@ -145,8 +145,11 @@ def main(argv=None):
     ap.add_argument("--width", type=int, default=32)
     ap.add_argument("--modes", type=int, default=12)
     ap.add_argument("--layers", type=int, default=4)
+    ap.add_argument("--hidden", type=int, default=128)
+    ap.add_argument("--grid", type=int, nargs=3, default=(64, 64, 33), metavar=("NX", "NY", "NZ"))
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
+    grid = tuple(a.grid)
     import torch
 
     import ehd
@@ -158,8 +161,8 @@ def main(argv=None):
     t0 = time.perf_counter()
     gtr = sample_groups(a.train, seed=1)
     gte = sample_groups(a.test, seed=2)
-    xtr, ytr, itr = trajectories(ehd, gtr, a.horizon)
-    xte, yte, ite = trajectories(ehd, gte, a.horizon, extra=a.relax)
+    xtr, ytr, itr = trajectories(ehd, gtr, a.horizon, grid=grid)
+    xte, yte, ite = trajectories(ehd, gte, a.horizon, extra=a.relax, grid=grid)
     t_data = time.perf_counter() - t0
     log(f"trajectories: {len(itr)} train, {len(ite)} test, {t_data:.1f} s")
     mean = ytr.reshape(-1, COUT).mean(0)
@@ -170,7 +173,7 @@ def main(argv=None):
     nz, ny, nx = xtr.shape[1:4]
     net = fno.FNO(nx, ny, nz, CIN, COUT, width=a.width, layers=a.layers,
                   modes=(a.modes, a.modes, min(a.modes, nz // 2)),
-                  hidden=128, max_batch=a.batch, seed=7)
+                  hidden=a.hidden, max_batch=a.batch, seed=7)
     t1 = time.perf_counter()
     hist = train(net, Xtr, Ytr, a.epochs, a.lr, a.batch, log=log)
     t_train = time.perf_counter() - t1
@@ -187,7 +190,7 @@ def main(argv=None):
     nu_warm, nu_cold, nu_none = [], [], []
     import sweep
     m = min(len(ite), 16)
-    ps = [params_of(ehd, ite[k]) for k in range(m)]
+    ps = [params_of(ehd, ite[k], *grid) for k in range(m)]
     starts = sweep.hydrostatic_profiles(ehd, ps, [sweep.hydrostatic_steps(p, 4.0) for p in ps])
     with ehd.Batch(ps, "fp32") as bw, ehd.Batch(ps, "fp32") as bn:
         for k in range(m):
