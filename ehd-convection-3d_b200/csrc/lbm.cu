@@ -31,6 +31,7 @@
 //                 rest populations are double-buffered, so the z = 0 node
 //                 always sees the pre-collision value.
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -183,6 +184,88 @@ __device__ __forceinline__ void warp_plane_sum(float rho, float charge, float2 *
     if ((threadIdx.x & 31) == 0) psum[slot] = v;
 }
 
+// ---- packed FP32x2 collision (sm_100 FFMA2): two opposite pairs of one weight
+// class at once, the same algebra as the scalar loops of finish_node ----
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+struct PackF {
+    float2 rp_hi, nrp_lo, rm_hi, nrm_lo, half, mone;
+    float2 PK[4], QK[4], nhWR[4], nWR[4], nc1[4], nc2[4];
+    float tux, tuy, tuz, fx, fy, fz;
+};
+
+template <int D1, int D2, typename T>
+__device__ __forceinline__ void f_pair2(const float (&f)[Q], const PackF &p,
+                                        const PopPtrs<T> &pp, unsigned node) {
+    constexpr int K = cls_of(D1);
+    static_assert(cls_of(D2) == K, "pairs of one weight class");
+    const float2 fd = f2(f[D1], f[D2]), fo = f2(f[D1 + 1], f[D2 + 1]);
+    const float2 cu = f2(dot_e(D1, p.tux, p.tuy, p.tuz), dot_e(D2, p.tux, p.tuy, p.tuz));
+    const float2 eF = f2(dot_e(D1, p.fx, p.fy, p.fz), dot_e(D2, p.fx, p.fy, p.fz));
+    float2 X = __ffma2_rn(p.half, __fadd2_rn(fd, fo), p.PK[K]);
+    X = __ffma2_rn(__fmul2_rn(p.nhWR[K], cu), cu, X);
+    float2 A = __ffma2_rn(p.nrp_lo, X, p.QK[K]);
+    A = __ffma2_rn(p.rp_hi, X, A);
+    A = __ffma2_rn(p.nc1[K], __fmul2_rn(cu, eF), A);
+    const float2 D = __ffma2_rn(p.mone, fo, fd);
+    const float2 Y = __ffma2_rn(p.half, D, __fmul2_rn(p.nWR[K], cu));
+    float2 B = __ffma2_rn(p.nrm_lo, Y, __fmul2_rn(p.nc2[K], eF));
+    B = __ffma2_rn(p.rm_hi, Y, B);
+    const float2 od = __ffma2_rn(p.mone, __fadd2_rn(A, B), fd);
+    const float2 oo = __ffma2_rn(p.mone, A, __fadd2_rn(fo, B));
+    Store<T>::st(pp.fb[D1] + node, od.x);
+    Store<T>::st(pp.fb[D2] + node, od.y);
+    Store<T>::st(pp.fb[D1 + 1] + node, oo.x);
+    Store<T>::st(pp.fb[D2 + 1] + node, oo.y);
+}
+
+struct PackG {
+    float2 cp_hi, ncp_lo, cm_hi, ncm_lo, cm_lo, half, mone;
+    float2 PQ[4], nhWQ[4], nWQ[4], twoWQ[4], wup[4];
+    float tux, tuy, tuz;
+    bool over;  // antisymmetric rate over-relaxed: hi = 2 exactly
+};
+
+template <int D1, int D2, typename T>
+__device__ __forceinline__ void g_pair2(const float (&h)[Q], const PackG &p,
+                                        const PopPtrs<T> &pp, unsigned node, unsigned nodeup,
+                                        bool dup) {
+    constexpr int K = cls_of(D1);
+    static_assert(cls_of(D2) == K, "pairs of one weight class");
+    const float2 hd = f2(h[D1], h[D2]), ho = f2(h[D1 + 1], h[D2 + 1]);
+    const float2 cu = f2(dot_e(D1, p.tux, p.tuy, p.tuz), dot_e(D2, p.tux, p.tuy, p.tuz));
+    float2 X = __ffma2_rn(p.half, __fadd2_rn(hd, ho), p.PQ[K]);
+    X = __ffma2_rn(__fmul2_rn(p.nhWQ[K], cu), cu, X);
+    const float2 Dd = __ffma2_rn(p.mone, ho, hd);
+    const float2 Y = __ffma2_rn(p.half, Dd, __fmul2_rn(p.nWQ[K], cu));
+    const float2 A = __ffma2_rn(p.cp_hi, X, __fmul2_rn(p.ncp_lo, X));
+    float2 od, oo;
+    if (p.over) {
+        // with B = 2 Y - lo Y: hd - 2 Y = ho + 2 WQ cu and ho + 2 Y = hd - 2 WQ cu
+        // exactly, so the outputs never form hd - B, which cancels when the
+        // rate is close to 2
+        const float2 t = __fmul2_rn(p.twoWQ[K], cu);
+        od = __ffma2_rn(p.cm_lo, Y, __ffma2_rn(p.mone, A, __fadd2_rn(ho, t)));
+        oo = __ffma2_rn(p.ncm_lo, Y, __ffma2_rn(p.mone, A, __ffma2_rn(p.mone, t, hd)));
+    } else {
+        const float2 B = __ffma2_rn(p.cm_hi, Y, __fmul2_rn(p.ncm_lo, Y));
+        od = __ffma2_rn(p.mone, __fadd2_rn(A, B), hd);
+        oo = __ffma2_rn(p.mone, A, __fadd2_rn(ho, B));
+    }
+    Store<T>::st(pp.hb[D1] + node, od.x);
+    Store<T>::st(pp.hb[D2] + node, od.y);
+    Store<T>::st(pp.hb[D1 + 1] + node, oo.x);
+    Store<T>::st(pp.hb[D2 + 1] + node, oo.y);
+    if (dup) {
+        const float2 ud = __fadd2_rn(od, p.wup[K]), uo = __fadd2_rn(oo, p.wup[K]);
+        Store<T>::st(pp.hb[D1] + nodeup, ud.x);
+        Store<T>::st(pp.hb[D2] + nodeup, ud.y);
+        Store<T>::st(pp.hb[D1 + 1] + nodeup, uo.x);
+        Store<T>::st(pp.hb[D2 + 1] + nodeup, uo.y);
+    }
+}
+
 // Everything after the moments: E, the injector override, the macroscopic
 // outputs, the TRT collisions of f and g and the wall rules on store.
 //
@@ -301,6 +384,47 @@ __device__ __forceinline__ void finish_node(R (&f)[Q], R (&h)[Q], const Moments<
             QK[k] = c.c3[k] * uF;
         }
         Store<T>::st(a.pp.fb[0] + node, f[0] - relax(rp_hi, rp_lo, f[0] + PK[0]) - QK[0]);
+        if constexpr (sizeof(R) == 4) {
+            PackF pk;
+            pk.rp_hi = f2(rp_hi);
+            pk.nrp_lo = f2(-rp_lo);
+            pk.rm_hi = f2(rm_hi);
+            pk.nrm_lo = f2(-rm_lo);
+            pk.half = f2(0.5f);
+            pk.mone = f2(-1.f);
+#pragma unroll
+            for (int k = 1; k < 4; ++k) {
+                pk.PK[k] = f2(PK[k]);
+                pk.QK[k] = f2(QK[k]);
+                pk.nhWR[k] = f2(-0.5f * WR[k]);
+                pk.nWR[k] = f2(-WR[k]);
+                pk.nc1[k] = f2(-c.c1[k]);
+                pk.nc2[k] = f2(-c.c2[k]);
+            }
+            pk.tux = tux;
+            pk.tuy = tuy;
+            pk.tuz = tuz;
+            pk.fx = fx;
+            pk.fy = fy;
+            pk.fz = fz;
+            f_pair2<1, 3>(f, pk, a.pp, node);
+            f_pair2<7, 9>(f, pk, a.pp, node);
+            f_pair2<11, 13>(f, pk, a.pp, node);
+            f_pair2<15, 17>(f, pk, a.pp, node);
+            f_pair2<19, 21>(f, pk, a.pp, node);
+            f_pair2<23, 25>(f, pk, a.pp, node);
+            {  // the fifth pair of class 1 alone
+                constexpr int d = 5, o = 6, k = 1;
+                const R cu = dot_e(d, tux, tuy, tuz);
+                const R eF = dot_e(d, fx, fy, fz);
+                const R X = (R)0.5 * (f[d] + f[o]) + PK[k] - (R)0.5 * WR[k] * cu * cu;
+                const R A = relax(rp_hi, rp_lo, X) + QK[k] - c.c1[k] * cu * eF;
+                const R Y = (R)0.5 * (f[d] - f[o]) - WR[k] * cu;
+                const R B = relax(rm_hi, rm_lo, Y) - c.c2[k] * eF;
+                Store<T>::st(a.pp.fb[d] + node, f[d] - A - B);
+                Store<T>::st(a.pp.fb[o] + node, f[o] - A + B);
+            }
+        } else {
 #pragma unroll
         for (int d = 1; d < Q; d += 2) {
             const int o = d + 1, k = cls_of(d);
@@ -312,6 +436,7 @@ __device__ __forceinline__ void finish_node(R (&f)[Q], R (&h)[Q], const Moments<
             const R B = relax(rm_hi, rm_lo, Y) - c.c2[k] * eF;
             Store<T>::st(a.pp.fb[d] + node, f[d] - A - B);
             Store<T>::st(a.pp.fb[o] + node, f[o] - A + B);
+        }
         }
     }
 
@@ -337,21 +462,81 @@ __device__ __forceinline__ void finish_node(R (&f)[Q], R (&h)[Q], const Moments<
             Store<T>::st(a.pp.hb[0] + node, z == 0 ? -out + (R)2 * (c.q0 - zr.qref) * c.w[0] : out);
             if (dup) Store<T>::st(a.pp.hb[0] + nodeup, out + c.w[0] * up);
         }
-#pragma unroll
-        for (int d = 1; d < Q; d += 2) {
-            const int o = d + 1, k = cls_of(d);
+        auto g_one = [&](auto dc) {
+            constexpr int d = decltype(dc)::value, o = d + 1, k = cls_of(d);
             const R cu = dot_e(d, tux, tuy, tuz);
             const R X = (R)0.5 * (h[d] + h[o]) + PQ[k] - (R)0.5 * WQ[k] * cu * cu;
             const R Y = (R)0.5 * (h[d] - h[o]) - WQ[k] * cu;
             const R A = relax(cp_hi, cp_lo, X);
-            const R B = relax(cm_hi, cm_lo, Y);
-            const R outd = h[d] - A - B;
-            const R outo = h[o] - A + B;
+            R outd, outo;
+            if (cm_hi == (R)2) {  // cancellation-free form, see g_pair2
+                const R t = (R)2 * WQ[k] * cu;
+                outd = (h[o] + t) - A + cm_lo * Y;
+                outo = (h[d] - t) - A - cm_lo * Y;
+            } else {
+                const R B = relax(cm_hi, cm_lo, Y);
+                outd = h[d] - A - B;
+                outo = h[o] - A + B;
+            }
             Store<T>::st(a.pp.hb[d] + node, outd);
             Store<T>::st(a.pp.hb[o] + node, outo);
             if (dup) {
                 Store<T>::st(a.pp.hb[d] + nodeup, outd + c.w[k] * up);
                 Store<T>::st(a.pp.hb[o] + nodeup, outo + c.w[k] * up);
+            }
+        };
+        if constexpr (sizeof(R) == 4) {
+            PackG pg;
+            pg.cp_hi = f2(cp_hi);
+            pg.ncp_lo = f2(-cp_lo);
+            pg.cm_hi = f2(cm_hi);
+            pg.ncm_lo = f2(-cm_lo);
+            pg.cm_lo = f2(cm_lo);
+            pg.over = cm_hi == 2.f;
+            pg.half = f2(0.5f);
+            pg.mone = f2(-1.f);
+#pragma unroll
+            for (int k = 1; k < 4; ++k) {
+                pg.PQ[k] = f2(PQ[k]);
+                pg.nhWQ[k] = f2(-0.5f * WQ[k]);
+                pg.nWQ[k] = f2(-WQ[k]);
+                pg.twoWQ[k] = f2(2.f * WQ[k]);
+                pg.wup[k] = f2(c.w[k] * up);
+            }
+            pg.tux = tux;
+            pg.tuy = tuy;
+            pg.tuz = tuz;
+            g_pair2<1, 3>(h, pg, a.pp, node, nodeup, dup);
+            g_pair2<7, 9>(h, pg, a.pp, node, nodeup, dup);
+            g_pair2<11, 13>(h, pg, a.pp, node, nodeup, dup);
+            g_pair2<15, 17>(h, pg, a.pp, node, nodeup, dup);
+            g_pair2<19, 21>(h, pg, a.pp, node, nodeup, dup);
+            g_pair2<23, 25>(h, pg, a.pp, node, nodeup, dup);
+            g_one(std::integral_constant<int, 5>{});
+        } else {
+#pragma unroll
+            for (int d = 1; d < Q; d += 2) {
+                const int o = d + 1, k = cls_of(d);
+                const R cu = dot_e(d, tux, tuy, tuz);
+                const R X = (R)0.5 * (h[d] + h[o]) + PQ[k] - (R)0.5 * WQ[k] * cu * cu;
+                const R Y = (R)0.5 * (h[d] - h[o]) - WQ[k] * cu;
+                const R A = relax(cp_hi, cp_lo, X);
+                R outd, outo;
+                if (cm_hi == (R)2) {  // cancellation-free form, see g_pair2
+                    const R t = (R)2 * WQ[k] * cu;
+                    outd = (h[o] + t) - A + cm_lo * Y;
+                    outo = (h[d] - t) - A - cm_lo * Y;
+                } else {
+                    const R B = relax(cm_hi, cm_lo, Y);
+                    outd = h[d] - A - B;
+                    outo = h[o] - A + B;
+                }
+                Store<T>::st(a.pp.hb[d] + node, outd);
+                Store<T>::st(a.pp.hb[o] + node, outo);
+                if (dup) {
+                    Store<T>::st(a.pp.hb[d] + nodeup, outd + c.w[k] * up);
+                    Store<T>::st(a.pp.hb[o] + nodeup, outo + c.w[k] * up);
+                }
             }
         }
     }
