@@ -469,7 +469,7 @@ __device__ __forceinline__ void finish_node(R (&f)[Q], R (&h)[Q], const Moments<
             const R Y = (R)0.5 * (h[d] - h[o]) - WQ[k] * cu;
             const R A = relax(cp_hi, cp_lo, X);
             R outd, outo;
-            if (cm_hi == (R)2) {  // cancellation-free form, see g_pair2
+            if (sizeof(R) == 4 && cm_hi == (R)2) {  // cancellation-free form, see g_pair2
                 const R t = (R)2 * WQ[k] * cu;
                 outd = (h[o] + t) - A + cm_lo * Y;
                 outo = (h[d] - t) - A - cm_lo * Y;
@@ -522,7 +522,7 @@ __device__ __forceinline__ void finish_node(R (&f)[Q], R (&h)[Q], const Moments<
                 const R Y = (R)0.5 * (h[d] - h[o]) - WQ[k] * cu;
                 const R A = relax(cp_hi, cp_lo, X);
                 R outd, outo;
-                if (cm_hi == (R)2) {  // cancellation-free form, see g_pair2
+                if (sizeof(R) == 4 && cm_hi == (R)2) {  // cancellation-free form, see g_pair2
                     const R t = (R)2 * WQ[k] * cu;
                     outd = (h[o] + t) - A + cm_lo * Y;
                     outo = (h[d] - t) - A - cm_lo * Y;
