@@ -20,11 +20,6 @@ namespace {
 
 constexpr int BM = 64, BN = 64, BK = 32, PK = BK + 8;
 
-__device__ __forceinline__ __nv_bfloat16 load_bf16(const void *p, long long off, int is_bf16) {
-    return is_bf16 ? reinterpret_cast<const __nv_bfloat16 *>(p)[off]
-                   : __float2bfloat16_rn(reinterpret_cast<const float *>(p)[off]);
-}
-
 __device__ __forceinline__ void mma16816(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
                                          uint32_t a3, uint32_t b0, uint32_t b1) {
     asm volatile(
@@ -38,6 +33,12 @@ __device__ __forceinline__ float gelu(float v) {
     return 0.5f * v * (1.f + erff(v * 0.70710678118654752f));
 }
 
+// Each thread stages one k column (kk = lane) of 16 rows (warp + 4 r) of both
+// tiles, so the row offsets of A and B are computed once per block and only
+// one k offset per operand per K step; the epilogue likewise computes the
+// offsets of its 4 rows and 8 columns once.  Off is int where every offset of
+// the product fits in 31 bits, else long long.
+template <typename Off>
 __global__ void __launch_bounds__(128) gemm_kernel(const GemmArgs a) {
     __shared__ __align__(16) __nv_bfloat16 As[BM][PK];
     __shared__ __align__(16) __nv_bfloat16 Bs[BN][PK];
@@ -46,10 +47,26 @@ __global__ void __launch_bounds__(128) gemm_kernel(const GemmArgs a) {
     const int gq = lane >> 2, tq = lane & 3;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const int bidx = blockIdx.z / a.ksplit, split = blockIdx.z % a.ksplit;
-    const long long aoff = at(a.abat, bidx), boff = at(a.bbat, bidx), coff = at(a.cbat, bidx);
+    const Off aoff = at_off<Off>(a.abat, bidx), boff = at_off<Off>(a.bbat, bidx);
     const int kper = ((a.K + a.ksplit - 1) / a.ksplit + BK - 1) / BK * BK;
     const int kbeg = split * kper;
     const int kend = min(a.K, kbeg + kper);
+
+    Off aro[16], bco[16];
+    unsigned amask = 0, bmask = 0;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+        const int m = m0 + warp + 4 * r, n = n0 + warp + 4 * r;
+        aro[r] = aoff + (m < a.M ? at_off<Off>(a.am, m) : (Off)0);
+        bco[r] = boff + (n < a.N ? at_off<Off>(a.bn, n) : (Off)0);
+        amask |= (m < a.M ? 1u : 0u) << r;
+        bmask |= (n < a.N ? 1u : 0u) << r;
+    }
+    const float *Af = reinterpret_cast<const float *>(a.A);
+    const float *Bf = reinterpret_cast<const float *>(a.B);
+    const __nv_bfloat16 *Ah = reinterpret_cast<const __nv_bfloat16 *>(a.A);
+    const __nv_bfloat16 *Bh = reinterpret_cast<const __nv_bfloat16 *>(a.B);
+    const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
 
     float acc[2][4][4];
 #pragma unroll
@@ -60,23 +77,30 @@ __global__ void __launch_bounds__(128) gemm_kernel(const GemmArgs a) {
             for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
 
     for (int k0 = kbeg; k0 < kend; k0 += BK) {
-#pragma unroll 4
-        for (int r = 0; r < (BM * BK) / 128; ++r) {
-            const int i = tid + 128 * r;
-            const int mm = i / BK, kk = i % BK;
-            const int m = m0 + mm, k = k0 + kk;
-            As[mm][kk] = (m < a.M && k < kend)
-                             ? load_bf16(a.A, aoff + at(a.am, m) + at(a.ak, k), a.a_bf16)
-                             : __float2bfloat16_rn(0.f);
+        const int k = k0 + lane;
+        const bool kin = k < kend;
+        const Off ako = kin ? at_off<Off>(a.ak, k) : (Off)0;
+        const Off bko = kin ? at_off<Off>(a.bk, k) : (Off)0;
+        const unsigned am = kin ? amask : 0u, bm = kin ? bmask : 0u;
+        if (a.a_bf16) {
+#pragma unroll
+            for (int r = 0; r < 16; ++r)
+                As[warp + 4 * r][lane] = (am >> r & 1u) ? Ah[aro[r] + ako] : zero;
+        } else {
+#pragma unroll
+            for (int r = 0; r < 16; ++r)
+                As[warp + 4 * r][lane] =
+                    (am >> r & 1u) ? __float2bfloat16_rn(Af[aro[r] + ako]) : zero;
         }
-#pragma unroll 4
-        for (int r = 0; r < (BN * BK) / 128; ++r) {
-            const int i = tid + 128 * r;
-            const int nn = i / BK, kk = i % BK;
-            const int n = n0 + nn, k = k0 + kk;
-            Bs[nn][kk] = (n < a.N && k < kend)
-                             ? load_bf16(a.B, boff + at(a.bk, k) + at(a.bn, n), a.b_bf16)
-                             : __float2bfloat16_rn(0.f);
+        if (a.b_bf16) {
+#pragma unroll
+            for (int r = 0; r < 16; ++r)
+                Bs[warp + 4 * r][lane] = (bm >> r & 1u) ? Bh[bco[r] + bko] : zero;
+        } else {
+#pragma unroll
+            for (int r = 0; r < 16; ++r)
+                Bs[warp + 4 * r][lane] =
+                    (bm >> r & 1u) ? __float2bfloat16_rn(Bf[bco[r] + bko]) : zero;
         }
         __syncthreads();
 #pragma unroll
@@ -106,23 +130,38 @@ __global__ void __launch_bounds__(128) gemm_kernel(const GemmArgs a) {
         __syncthreads();
     }
 
+    // epilogue: rows m0 + wm 32 + i 16 + gq + h 8, columns n0 + wn 32 + j 8 + 2 tq + c
+    const Off coff = at_off<Off>(a.cbat, bidx);
+    Off cmo[4], cno[8];
+    unsigned cmask = 0;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const int m = m0 + wm * 32 + (t >> 1) * 16 + gq + (t & 1) * 8;
+        cmo[t] = coff + (m < a.M ? at_off<Off>(a.cm, m) : (Off)0);
+        cmask |= (m < a.M ? 1u : 0u) << t;
+    }
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const int n = n0 + wn * 32 + (t >> 1) * 8 + tq * 2 + (t & 1);
+        cno[t] = n < a.N ? at_off<Off>(a.cn, n) : (Off)0;
+        cmask |= (n < a.N ? 1u : 0u) << (4 + t);
+    }
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j)
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-                const int m = m0 + wm * 32 + i * 16 + gq + (e >> 1) * 8;
-                const int n = n0 + wn * 32 + j * 8 + tq * 2 + (e & 1);
-                if (m >= a.M || n >= a.N) continue;
-                const long long off = coff + at(a.cm, m) + at(a.cn, n);
+                const int tm = i * 2 + (e >> 1), tn = j * 2 + (e & 1);
+                if (!((cmask >> tm) & (cmask >> (4 + tn)) & 1u)) continue;
+                const Off off = cmo[tm] + cno[tn];
                 float v = a.alpha * acc[i][j][e];
                 if (a.ksplit > 1) {
                     atomicAdd(a.C + off, v);
                     continue;
                 }
                 if (a.beta != 0.f) v += a.beta * a.C[off];
-                if (a.bias) v += a.bias[n];
+                if (a.bias) v += a.bias[n0 + wn * 32 + j * 8 + tq * 2 + (e & 1)];
                 a.C[off] = v;
                 if (a.C2) a.C2[off] = gelu(v);
             }
@@ -135,6 +174,7 @@ namespace {
 // largest offset of the map over i = 0 .. n-1 (strides >= 0)
 long long max_at(const Map &d, long long n) {
     if (n <= 0) return 0;
+    if (d.g == (1 << 30)) return (n - 1) * d.s0;  // one level, as at()
     const long long q = (n - 1) / d.g, r = (n - 1) % d.g;
     long long m = q * d.s1 + r * d.s0;
     if (q >= 1) m = std::max(m, (q - 1) * d.s1 + (long long)(d.g - 1) * d.s0);
@@ -160,7 +200,12 @@ cudaError_t gemm(const GemmArgs &a, cudaStream_t s) {
     const long long gy = (a.M + BM - 1) / BM, gz = (long long)a.batch * a.ksplit;
     if (gy > 65535 || gz > 65535) return cudaErrorInvalidValue;
     dim3 grid((a.N + BN - 1) / BN, (unsigned)gy, (unsigned)gz);
-    gemm_kernel<<<grid, 128, 0, s>>>(a);
+    // every offset below a_n, b_n or c_n: 32-bit offsets when all three fit
+    const long long lim = 1ll << 31;
+    if (a.a_n < lim && a.b_n < lim && a.c_n < lim)
+        gemm_kernel<int><<<grid, 128, 0, s>>>(a);
+    else
+        gemm_kernel<long long><<<grid, 128, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -23,7 +23,16 @@ struct Map {
     int g = 1 << 30;
 };
 __host__ __device__ __forceinline__ long long at(const Map &d, long long i) {
+    if (d.g == (1 << 30)) return i * d.s0;  // one level: no division
     return (i / d.g) * d.s1 + (i % d.g) * d.s0;
+}
+// the same for a non-negative int index, in the offset type Off (int where
+// every offset of the product fits, else long long); 32-bit division
+template <typename Off>
+__host__ __device__ __forceinline__ Off at_off(const Map &d, int i) {
+    if (d.g == (1 << 30)) return (Off)i * (Off)d.s0;
+    const unsigned q = (unsigned)i / (unsigned)d.g, r = (unsigned)i - q * (unsigned)d.g;
+    return (Off)q * (Off)d.s1 + (Off)r * (Off)d.s0;
 }
 inline Map lin(long long s0) { return Map{s0, 0, 1 << 30}; }
 inline Map two(long long s0, int g, long long s1) { return Map{s0, s1, g}; }
