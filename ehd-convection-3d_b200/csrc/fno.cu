@@ -296,7 +296,7 @@ GemmArgs weight_grad(size_t rows, int K, int N, const float *Xs, const float *D,
     g.cm = lin(N);
     g.cn = lin(1);
     g.beta = 1.f;
-    g.ksplit = (int)std::min<size_t>(2048, std::max<size_t>(1, rows / 2048));
+    g.ksplit = (int)std::min<size_t>(2048, std::max<size_t>(1, rows / 1024));
     g.a_n = (long long)rows * K;
     g.b_n = (long long)rows * N;
     g.c_n = (long long)K * N;
@@ -347,12 +347,13 @@ struct Dims {
 // the eight products of one spectral convolution (forward), and their
 // adjoints; `tr` selects the transposed DFT matrix
 GemmArgs x_fwd(const Dims &d, const __nv_bfloat16 *Fx, const float *v, float *xh, bool adj_of_inv) {
-    // xh[q][(ri,kx)][c] = Fx[(ri,kx)][x] v[q][x][c]; adj_of_inv: Gx^T instead of Fx
+    // xh[q][(ri,kx)][(y,c)] = Fx[(ri,kx)][x] v[q][(y,x,c)] over q = (b, z), the
+    // columns n = (y, c); adj_of_inv: Gx^T instead of Fx
     GemmArgs g;
     g.M = (int)(2 * d.mx);
     g.K = (int)d.X;
-    g.N = (int)d.W;
-    g.batch = (int)(d.B * d.Z * d.Y);
+    g.N = (int)(d.Y * d.W);
+    g.batch = (int)(d.B * d.Z);
     g.A = Fx;
     g.a_bf16 = 1;
     if (adj_of_inv) {  // Gx is [X][2mx]
@@ -365,12 +366,12 @@ GemmArgs x_fwd(const Dims &d, const __nv_bfloat16 *Fx, const float *v, float *xh
     g.abat = lin(0);
     g.B = v;
     g.bk = lin(d.W);
-    g.bn = lin(1);
-    g.bbat = lin(d.X * d.W);
+    g.bn = two(1, (int)d.W, d.X * d.W);
+    g.bbat = lin(d.Y * d.X * d.W);
     g.C = xh;
     g.cm = two(d.W, (int)d.mx, d.Y * d.mx * d.W);
-    g.cn = lin(1);
-    g.cbat = two(d.mx * d.W, (int)d.Y, 2 * d.Y * d.mx * d.W);
+    g.cn = two(1, (int)d.W, d.mx * d.W);
+    g.cbat = lin(2 * d.Y * d.mx * d.W);
     g.a_n = 2 * d.mx * d.X;
     g.b_n = d.nv();
     g.c_n = d.nxh();
@@ -379,12 +380,13 @@ GemmArgs x_fwd(const Dims &d, const __nv_bfloat16 *Fx, const float *v, float *xh
 
 GemmArgs x_inv(const Dims &d, const __nv_bfloat16 *Gx, const float *xh, float *v, float beta,
                bool adj_of_fwd) {
-    // v[q][x][c] (+)= Gx[x][(ri,kx)] xh[q][(ri,kx)][c]; adj_of_fwd: Fx^T
+    // v[q][(y,x,c)] (+)= Gx[x][(ri,kx)] xh[q][(ri,kx)][(y,c)] over q = (b, z), the
+    // columns n = (y, c); adj_of_fwd: Fx^T
     GemmArgs g;
     g.M = (int)d.X;
     g.K = (int)(2 * d.mx);
-    g.N = (int)d.W;
-    g.batch = (int)(d.B * d.Z * d.Y);
+    g.N = (int)(d.Y * d.W);
+    g.batch = (int)(d.B * d.Z);
     g.A = Gx;
     g.a_bf16 = 1;
     if (adj_of_fwd) {  // Fx is [2mx][X]
@@ -397,12 +399,12 @@ GemmArgs x_inv(const Dims &d, const __nv_bfloat16 *Gx, const float *xh, float *v
     g.abat = lin(0);
     g.B = xh;
     g.bk = two(d.W, (int)d.mx, d.Y * d.mx * d.W);
-    g.bn = lin(1);
-    g.bbat = two(d.mx * d.W, (int)d.Y, 2 * d.Y * d.mx * d.W);
+    g.bn = two(1, (int)d.W, d.mx * d.W);
+    g.bbat = lin(2 * d.Y * d.mx * d.W);
     g.C = v;
     g.cm = lin(d.W);
-    g.cn = lin(1);
-    g.cbat = lin(d.X * d.W);
+    g.cn = two(1, (int)d.W, d.X * d.W);
+    g.cbat = lin(d.Y * d.X * d.W);
     g.beta = beta;
     g.a_n = 2 * d.mx * d.X;
     g.b_n = d.nxh();

@@ -33,11 +33,83 @@ __device__ __forceinline__ float gelu(float v) {
     return 0.5f * v * (1.f + erff(v * 0.70710678118654752f));
 }
 
-// Each thread stages one k column (kk = lane) of 16 rows (warp + 4 r) of both
-// tiles, so the row offsets of A and B are computed once per block and only
-// one k offset per operand per K step; the epilogue likewise computes the
-// offsets of its 4 rows and 8 columns once.  Off is int where every offset of
-// the product fits in 31 bits, else long long.
+// Raw bits of one operand element: the FP32 value, or the BF16 value in the
+// low half.
+__device__ __forceinline__ uint32_t ld_raw(const void *p, long long off, int is_bf16) {
+    return is_bf16 ? (uint32_t)__ldg(reinterpret_cast<const unsigned short *>(p) + off)
+                   : __float_as_uint(__ldg(reinterpret_cast<const float *>(p) + off));
+}
+__device__ __forceinline__ __nv_bfloat16 to_bf16(uint32_t raw, int is_bf16) {
+    return is_bf16 ? __ushort_as_bfloat16((unsigned short)raw)
+                   : __float2bfloat16_rn(__uint_as_float(raw));
+}
+
+// One operand's share of a 64-row x 32-k tile.  Lanes run along whichever
+// index has unit stride in memory, so a warp reads 32 consecutive elements:
+//  - along k (rows_fast = 0): k = k0 + lane, rows warp + 4 r (r < 16); the
+//    16 row offsets ro[r] are fixed for the block, one k offset per K step;
+//  - along rows (rows_fast = 1): row tid % 64 (offset ro[0]), k = k0 + tid / 64
+//    + 2 r; 16 k offsets per K step.
+// Elements outside the product (row >= rows or k >= kend) read as zero.
+template <typename Off>
+__device__ __forceinline__ void load_tile(uint32_t (&raw)[16], const void *P, int is_bf16,
+                                          int rows_fast, const Off (&ro)[16], unsigned mask,
+                                          const Map &km, int k0, int kend, int tid) {
+    if (!rows_fast) {
+        const int k = k0 + (tid & 31);
+        const bool kin = k < kend;
+        const Off ko = kin ? at_off<Off>(km, k) : (Off)0;
+        const unsigned m = kin ? mask : 0u;
+#pragma unroll
+        for (int r = 0; r < 16; ++r) raw[r] = (m >> r & 1u) ? ld_raw(P, ro[r] + ko, is_bf16) : 0u;
+    } else {
+        const int kb = k0 + (tid >> 6);
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            const int k = kb + 2 * r;
+            raw[r] = ((mask & 1u) && k < kend) ? ld_raw(P, ro[0] + at_off<Off>(km, k), is_bf16)
+                                               : 0u;
+        }
+    }
+}
+
+__device__ __forceinline__ void store_tile(__nv_bfloat16 (*S)[PK], const uint32_t (&raw)[16],
+                                           int is_bf16, int rows_fast, int tid) {
+    if (!rows_fast) {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) S[(tid >> 5) + 4 * r][tid & 31] = to_bf16(raw[r], is_bf16);
+    } else {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) S[tid & 63][(tid >> 6) + 2 * r] = to_bf16(raw[r], is_bf16);
+    }
+}
+
+// row offsets of one operand's tile rows for this thread (see load_tile)
+template <typename Off>
+__device__ __forceinline__ void row_offsets(Off (&ro)[16], unsigned &mask, const Map &rm,
+                                            Off base, int r0, int rows, int rows_fast, int tid) {
+    mask = 0;
+    if (!rows_fast) {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            const int i = r0 + (tid >> 5) + 4 * r;
+            ro[r] = base + (i < rows ? at_off<Off>(rm, i) : (Off)0);
+            mask |= (i < rows ? 1u : 0u) << r;
+        }
+    } else {
+        const int i = r0 + (tid & 63);
+#pragma unroll
+        for (int r = 0; r < 16; ++r) ro[r] = base;
+        if (i < rows) {
+            ro[0] = base + at_off<Off>(rm, i);
+            mask = 1u;
+        }
+    }
+}
+
+// The next K step's operands are loaded into registers while the tensor
+// cores work on the current one.  Off is int where every offset of the
+// product fits in 31 bits, else long long.
 template <typename Off>
 __global__ void __launch_bounds__(128) gemm_kernel(const GemmArgs a) {
     __shared__ __align__(16) __nv_bfloat16 As[BM][PK];
@@ -47,26 +119,14 @@ __global__ void __launch_bounds__(128) gemm_kernel(const GemmArgs a) {
     const int gq = lane >> 2, tq = lane & 3;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const int bidx = blockIdx.z / a.ksplit, split = blockIdx.z % a.ksplit;
-    const Off aoff = at_off<Off>(a.abat, bidx), boff = at_off<Off>(a.bbat, bidx);
     const int kper = ((a.K + a.ksplit - 1) / a.ksplit + BK - 1) / BK * BK;
     const int kbeg = split * kper;
     const int kend = min(a.K, kbeg + kper);
 
-    Off aro[16], bco[16];
-    unsigned amask = 0, bmask = 0;
-#pragma unroll
-    for (int r = 0; r < 16; ++r) {
-        const int m = m0 + warp + 4 * r, n = n0 + warp + 4 * r;
-        aro[r] = aoff + (m < a.M ? at_off<Off>(a.am, m) : (Off)0);
-        bco[r] = boff + (n < a.N ? at_off<Off>(a.bn, n) : (Off)0);
-        amask |= (m < a.M ? 1u : 0u) << r;
-        bmask |= (n < a.N ? 1u : 0u) << r;
-    }
-    const float *Af = reinterpret_cast<const float *>(a.A);
-    const float *Bf = reinterpret_cast<const float *>(a.B);
-    const __nv_bfloat16 *Ah = reinterpret_cast<const __nv_bfloat16 *>(a.A);
-    const __nv_bfloat16 *Bh = reinterpret_cast<const __nv_bfloat16 *>(a.B);
-    const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
+    Off aro[16], bro[16];
+    unsigned amask, bmask;
+    row_offsets<Off>(aro, amask, a.am, at_off<Off>(a.abat, bidx), m0, a.M, a.a_rows_fast, tid);
+    row_offsets<Off>(bro, bmask, a.bn, at_off<Off>(a.bbat, bidx), n0, a.N, a.b_rows_fast, tid);
 
     float acc[2][4][4];
 #pragma unroll
@@ -76,33 +136,19 @@ __global__ void __launch_bounds__(128) gemm_kernel(const GemmArgs a) {
 #pragma unroll
             for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
 
+    uint32_t ra[16], rb[16];
+    if (kbeg < kend) {
+        load_tile<Off>(ra, a.A, a.a_bf16, a.a_rows_fast, aro, amask, a.ak, kbeg, kend, tid);
+        load_tile<Off>(rb, a.B, a.b_bf16, a.b_rows_fast, bro, bmask, a.bk, kbeg, kend, tid);
+    }
     for (int k0 = kbeg; k0 < kend; k0 += BK) {
-        const int k = k0 + lane;
-        const bool kin = k < kend;
-        const Off ako = kin ? at_off<Off>(a.ak, k) : (Off)0;
-        const Off bko = kin ? at_off<Off>(a.bk, k) : (Off)0;
-        const unsigned am = kin ? amask : 0u, bm = kin ? bmask : 0u;
-        if (a.a_bf16) {
-#pragma unroll
-            for (int r = 0; r < 16; ++r)
-                As[warp + 4 * r][lane] = (am >> r & 1u) ? Ah[aro[r] + ako] : zero;
-        } else {
-#pragma unroll
-            for (int r = 0; r < 16; ++r)
-                As[warp + 4 * r][lane] =
-                    (am >> r & 1u) ? __float2bfloat16_rn(Af[aro[r] + ako]) : zero;
-        }
-        if (a.b_bf16) {
-#pragma unroll
-            for (int r = 0; r < 16; ++r)
-                Bs[warp + 4 * r][lane] = (bm >> r & 1u) ? Bh[bco[r] + bko] : zero;
-        } else {
-#pragma unroll
-            for (int r = 0; r < 16; ++r)
-                Bs[warp + 4 * r][lane] =
-                    (bm >> r & 1u) ? __float2bfloat16_rn(Bf[bco[r] + bko]) : zero;
-        }
+        store_tile(As, ra, a.a_bf16, a.a_rows_fast, tid);
+        store_tile(Bs, rb, a.b_bf16, a.b_rows_fast, tid);
         __syncthreads();
+        if (k0 + BK < kend) {
+            load_tile<Off>(ra, a.A, a.a_bf16, a.a_rows_fast, aro, amask, a.ak, k0 + BK, kend, tid);
+            load_tile<Off>(rb, a.B, a.b_bf16, a.b_rows_fast, bro, bmask, a.bk, k0 + BK, kend, tid);
+        }
 #pragma unroll
         for (int kk = 0; kk < BK; kk += 16) {
             uint32_t af[2][4], bf[4][2];
@@ -200,12 +246,17 @@ cudaError_t gemm(const GemmArgs &a, cudaStream_t s) {
     const long long gy = (a.M + BM - 1) / BM, gz = (long long)a.batch * a.ksplit;
     if (gy > 65535 || gz > 65535) return cudaErrorInvalidValue;
     dim3 grid((a.N + BN - 1) / BN, (unsigned)gy, (unsigned)gz);
+    // lanes along the operand's unit-stride index: k where it has one, else
+    // the row index (m of A, n of B)
+    GemmArgs g = a;
+    g.a_rows_fast = (a.ak.s0 != 1 && a.am.s0 == 1) ? 1 : 0;
+    g.b_rows_fast = (a.bk.s0 != 1 && a.bn.s0 == 1) ? 1 : 0;
     // every offset below a_n, b_n or c_n: 32-bit offsets when all three fit
     const long long lim = 1ll << 31;
     if (a.a_n < lim && a.b_n < lim && a.c_n < lim)
-        gemm_kernel<int><<<grid, 128, 0, s>>>(a);
+        gemm_kernel<int><<<grid, 128, 0, s>>>(g);
     else
-        gemm_kernel<long long><<<grid, 128, 0, s>>>(a);
+        gemm_kernel<long long><<<grid, 128, 0, s>>>(g);
     return cudaGetLastError();
 }
 

@@ -53,6 +53,9 @@ struct GemmArgs {
     // elements in the A, B and C (and C2) buffers: gemm() rejects a product
     // whose largest offset falls outside them
     long long a_n = 0, b_n = 0, c_n = 0;
+    // set by gemm(): which index of A (m) and B (n) the lanes of a warp run
+    // along when staging a tile (the one with unit stride)
+    int a_rows_fast = 0, b_rows_fast = 0;
 };
 
 cudaError_t gemm(const GemmArgs &a, cudaStream_t s);
