@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <utility>
 
 #include "gemm_bf16.cuh"
 
@@ -35,12 +36,14 @@ __device__ __forceinline__ float gelu(float v) {
 
 // Raw bits of one operand element: the FP32 value, or the BF16 value in the
 // low half.
-__device__ __forceinline__ uint32_t ld_raw(const void *p, long long off, int is_bf16) {
-    return is_bf16 ? (uint32_t)__ldg(reinterpret_cast<const unsigned short *>(p) + off)
+template <int BF>
+__device__ __forceinline__ uint32_t ld_raw(const void *p, long long off) {
+    return BF ? (uint32_t)__ldg(reinterpret_cast<const unsigned short *>(p) + off)
                    : __float_as_uint(__ldg(reinterpret_cast<const float *>(p) + off));
 }
-__device__ __forceinline__ __nv_bfloat16 to_bf16(uint32_t raw, int is_bf16) {
-    return is_bf16 ? __ushort_as_bfloat16((unsigned short)raw)
+template <int BF>
+__device__ __forceinline__ __nv_bfloat16 to_bf16(uint32_t raw) {
+    return BF ? __ushort_as_bfloat16((unsigned short)raw)
                    : __float2bfloat16_rn(__uint_as_float(raw));
 }
 
@@ -50,46 +53,47 @@ __device__ __forceinline__ __nv_bfloat16 to_bf16(uint32_t raw, int is_bf16) {
 //    16 row offsets ro[r] are fixed for the block, one k offset per K step;
 //  - along rows (rows_fast = 1): row tid % 64 (offset ro[0]), k = k0 + tid / 64
 //    + 2 r; 16 k offsets per K step.
-// Elements outside the product (row >= rows or k >= kend) read as zero.
-template <typename Off>
-__device__ __forceinline__ void load_tile(uint32_t (&raw)[16], const void *P, int is_bf16,
-                                          int rows_fast, const Off (&ro)[16], unsigned mask,
-                                          const Map &km, int k0, int kend, int tid) {
-    if (!rows_fast) {
+// Elements outside the product (row >= rows or k >= kend) read as zero.  BF:
+// the operand is BF16 (else FP32); RF: rows_fast.
+template <typename Off, int BF, int RF>
+__device__ __forceinline__ void load_tile(uint32_t (&raw)[16], const void *P,
+                                          const Off (&ro)[16], unsigned mask, const Map &km,
+                                          int k0, int kend, int tid) {
+    if (!RF) {
         const int k = k0 + (tid & 31);
         const bool kin = k < kend;
         const Off ko = kin ? at_off<Off>(km, k) : (Off)0;
         const unsigned m = kin ? mask : 0u;
 #pragma unroll
-        for (int r = 0; r < 16; ++r) raw[r] = (m >> r & 1u) ? ld_raw(P, ro[r] + ko, is_bf16) : 0u;
+        for (int r = 0; r < 16; ++r) raw[r] = (m >> r & 1u) ? ld_raw<BF>(P, ro[r] + ko) : 0u;
     } else {
         const int kb = k0 + (tid >> 6);
 #pragma unroll
         for (int r = 0; r < 16; ++r) {
             const int k = kb + 2 * r;
-            raw[r] = ((mask & 1u) && k < kend) ? ld_raw(P, ro[0] + at_off<Off>(km, k), is_bf16)
-                                               : 0u;
+            raw[r] = ((mask & 1u) && k < kend) ? ld_raw<BF>(P, ro[0] + at_off<Off>(km, k)) : 0u;
         }
     }
 }
 
+template <int BF, int RF>
 __device__ __forceinline__ void store_tile(__nv_bfloat16 (*S)[PK], const uint32_t (&raw)[16],
-                                           int is_bf16, int rows_fast, int tid) {
-    if (!rows_fast) {
+                                           int tid) {
+    if (!RF) {
 #pragma unroll
-        for (int r = 0; r < 16; ++r) S[(tid >> 5) + 4 * r][tid & 31] = to_bf16(raw[r], is_bf16);
+        for (int r = 0; r < 16; ++r) S[(tid >> 5) + 4 * r][tid & 31] = to_bf16<BF>(raw[r]);
     } else {
 #pragma unroll
-        for (int r = 0; r < 16; ++r) S[tid & 63][(tid >> 6) + 2 * r] = to_bf16(raw[r], is_bf16);
+        for (int r = 0; r < 16; ++r) S[tid & 63][(tid >> 6) + 2 * r] = to_bf16<BF>(raw[r]);
     }
 }
 
 // row offsets of one operand's tile rows for this thread (see load_tile)
-template <typename Off>
+template <typename Off, int RF>
 __device__ __forceinline__ void row_offsets(Off (&ro)[16], unsigned &mask, const Map &rm,
-                                            Off base, int r0, int rows, int rows_fast, int tid) {
+                                            Off base, int r0, int rows, int tid) {
     mask = 0;
-    if (!rows_fast) {
+    if (!RF) {
 #pragma unroll
         for (int r = 0; r < 16; ++r) {
             const int i = r0 + (tid >> 5) + 4 * r;
@@ -109,9 +113,12 @@ __device__ __forceinline__ void row_offsets(Off (&ro)[16], unsigned &mask, const
 
 // The next K step's operands are loaded into registers while the tensor
 // cores work on the current one.  Off is int where every offset of the
-// product fits in 31 bits, else long long.
-template <typename Off>
-__global__ void __launch_bounds__(128) gemm_kernel(const GemmArgs a) {
+// product fits in 31 bits, else long long.  The operand types (ABF, BBF) and
+// staging directions (AR, BR) are compile-time, so each instance is
+// straight-line code: with them as run-time switches the kernel stalled on
+// instruction fetch.
+template <typename Off, int ABF, int AR, int BBF, int BR>
+__global__ void __launch_bounds__(128, 4) gemm_kernel(const GemmArgs a) {
     __shared__ __align__(16) __nv_bfloat16 As[BM][PK];
     __shared__ __align__(16) __nv_bfloat16 Bs[BN][PK];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -125,8 +132,8 @@ __global__ void __launch_bounds__(128) gemm_kernel(const GemmArgs a) {
 
     Off aro[16], bro[16];
     unsigned amask, bmask;
-    row_offsets<Off>(aro, amask, a.am, at_off<Off>(a.abat, bidx), m0, a.M, a.a_rows_fast, tid);
-    row_offsets<Off>(bro, bmask, a.bn, at_off<Off>(a.bbat, bidx), n0, a.N, a.b_rows_fast, tid);
+    row_offsets<Off, AR>(aro, amask, a.am, at_off<Off>(a.abat, bidx), m0, a.M, tid);
+    row_offsets<Off, BR>(bro, bmask, a.bn, at_off<Off>(a.bbat, bidx), n0, a.N, tid);
 
     float acc[2][4][4];
 #pragma unroll
@@ -138,16 +145,16 @@ __global__ void __launch_bounds__(128) gemm_kernel(const GemmArgs a) {
 
     uint32_t ra[16], rb[16];
     if (kbeg < kend) {
-        load_tile<Off>(ra, a.A, a.a_bf16, a.a_rows_fast, aro, amask, a.ak, kbeg, kend, tid);
-        load_tile<Off>(rb, a.B, a.b_bf16, a.b_rows_fast, bro, bmask, a.bk, kbeg, kend, tid);
+        load_tile<Off, ABF, AR>(ra, a.A, aro, amask, a.ak, kbeg, kend, tid);
+        load_tile<Off, BBF, BR>(rb, a.B, bro, bmask, a.bk, kbeg, kend, tid);
     }
     for (int k0 = kbeg; k0 < kend; k0 += BK) {
-        store_tile(As, ra, a.a_bf16, a.a_rows_fast, tid);
-        store_tile(Bs, rb, a.b_bf16, a.b_rows_fast, tid);
+        store_tile<ABF, AR>(As, ra, tid);
+        store_tile<BBF, BR>(Bs, rb, tid);
         __syncthreads();
         if (k0 + BK < kend) {
-            load_tile<Off>(ra, a.A, a.a_bf16, a.a_rows_fast, aro, amask, a.ak, k0 + BK, kend, tid);
-            load_tile<Off>(rb, a.B, a.b_bf16, a.b_rows_fast, bro, bmask, a.bk, k0 + BK, kend, tid);
+            load_tile<Off, ABF, AR>(ra, a.A, aro, amask, a.ak, k0 + BK, kend, tid);
+            load_tile<Off, BBF, BR>(rb, a.B, bro, bmask, a.bk, k0 + BK, kend, tid);
         }
 #pragma unroll
         for (int kk = 0; kk < BK; kk += 16) {
@@ -229,6 +236,22 @@ long long max_at(const Map &d, long long n) {
 
 bool nonneg(const Map &d) { return d.s0 >= 0 && d.s1 >= 0 && d.g >= 1; }
 
+using Kern = void (*)(const GemmArgs);
+
+template <typename Off, int C>
+constexpr Kern kern() {
+    return gemm_kernel<Off, (C >> 3) & 1, (C >> 2) & 1, (C >> 1) & 1, C & 1>;
+}
+
+// instance by code: bit 4 32-bit offsets, 3 A is BF16, 2 A staged along m,
+// 1 B is BF16, 0 B staged along n
+template <int... C>
+const Kern *table(std::integer_sequence<int, C...>) {
+    static const Kern t[] = {kern<long long, C>()..., kern<int, C>()...};
+    return t;
+}
+const Kern *kernel_table() { return table(std::make_integer_sequence<int, 16>{}); }
+
 }  // namespace
 
 cudaError_t gemm(const GemmArgs &a, cudaStream_t s) {
@@ -252,11 +275,10 @@ cudaError_t gemm(const GemmArgs &a, cudaStream_t s) {
     g.a_rows_fast = (a.ak.s0 != 1 && a.am.s0 == 1) ? 1 : 0;
     g.b_rows_fast = (a.bk.s0 != 1 && a.bn.s0 == 1) ? 1 : 0;
     // every offset below a_n, b_n or c_n: 32-bit offsets when all three fit
-    const long long lim = 1ll << 31;
-    if (a.a_n < lim && a.b_n < lim && a.c_n < lim)
-        gemm_kernel<int><<<grid, 128, 0, s>>>(g);
-    else
-        gemm_kernel<long long><<<grid, 128, 0, s>>>(g);
+    const bool narrow = a.a_n < (1ll << 31) && a.b_n < (1ll << 31) && a.c_n < (1ll << 31);
+    const int code = (narrow ? 16 : 0) | (a.a_bf16 ? 8 : 0) | (g.a_rows_fast ? 4 : 0) |
+                     (a.b_bf16 ? 2 : 0) | (g.b_rows_fast ? 1 : 0);
+    kernel_table()[code]<<<grid, 128, 0, s>>>(g);
     return cudaGetLastError();
 }
 
