@@ -46,19 +46,20 @@ __global__ void cast_bf16_kernel(const float *__restrict__ src, __nv_bfloat16 *_
         dst[i] = __float2bfloat16_rn(src[i]);
 }
 
-// real form [[Re, -Im], [Im, Re]] of R per mode, W x W blocks -> 2W x 2W
+// real form [[Re, -Im], [Im, Re]] of R per mode, W x W blocks -> 2W x 2W: one
+// thread per (mode, o, c) reads Re and Im once and writes the four entries
+// (modes W^2 < 2^32: 32-bit index arithmetic)
 __global__ void build_block_kernel(const float *__restrict__ re, const float *__restrict__ im,
                                    __nv_bfloat16 *__restrict__ blk, int modes, int W) {
-    const size_t n = (size_t)modes * 4 * W * W;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-         i += (size_t)gridDim.x * blockDim.x) {
-        const int col = (int)(i % (2 * W));
-        const int row = (int)((i / (2 * W)) % (2 * W));
-        const size_t md = i / (4 * (size_t)W * W);
-        const int ro = row / W, o = row % W, rc = col / W, c = col % W;
-        const size_t k = (md * W + o) * W + c;
-        float v = ro == rc ? re[k] : (ro == 0 ? -im[k] : im[k]);
-        blk[i] = __float2bfloat16_rn(v);
+    const unsigned n = (unsigned)modes * W * W, w = (unsigned)W, w2 = 2u * W;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned c = i % w, t = i / w, o = t % w, md = t / w;
+        const __nv_bfloat16 r = __float2bfloat16_rn(re[i]), m = __float2bfloat16_rn(im[i]);
+        __nv_bfloat16 *b = blk + (size_t)md * 4 * w * w;
+        b[o * w2 + c] = r;
+        b[o * w2 + w + c] = __hneg(m);
+        b[(w + o) * w2 + c] = m;
+        b[(w + o) * w2 + w + c] = r;
     }
 }
 
@@ -244,12 +245,23 @@ cudaError_t make_dft(ehd_fno *f) {
     return cudaSuccess;
 }
 
-// BF16 copies of the parameters and the layers' block matrices
+// BF16 copies of the parameters and the layers' block matrices.  The products
+// read the spectral weights only through the block matrices, so only the
+// parameters between the layers' (Re R, Im R) ranges are cast.
 cudaError_t refresh(ehd_fno *f) {
-    cast_bf16_kernel<<<grid_for(f->nparam), 256, 0, f->stream>>>(f->param, f->pbf, f->nparam);
-    for (int l = 0; l < f->L; ++l)
-        build_block_kernel<<<grid_for((size_t)f->modes * 4 * f->W * f->W), 256, 0, f->stream>>>(
-            f->param + f->lo[l].Rre, f->param + f->lo[l].Rim, f->blk[l], f->modes, f->W);
+    const size_t spec = (size_t)f->modes * f->W * f->W;
+    size_t from = 0;
+    for (int l = 0; l <= f->L; ++l) {
+        const size_t to = l < f->L ? f->lo[l].Rre : f->nparam;
+        if (to > from)
+            cast_bf16_kernel<<<grid_for(to - from), 256, 0, f->stream>>>(f->param + from,
+                                                                         f->pbf + from, to - from);
+        if (l < f->L) {
+            build_block_kernel<<<grid_for(spec), 256, 0, f->stream>>>(
+                f->param + f->lo[l].Rre, f->param + f->lo[l].Rim, f->blk[l], f->modes, f->W);
+            from = f->lo[l].Rim + spec;
+        }
+    }
     return cudaGetLastError();
 }
 

@@ -144,3 +144,62 @@ class FNO:
 
     def synchronize(self):
         ehd._check(lib().ehd_fno_synchronize(self.h))
+
+
+def main(argv=None):
+    """Times the network's forward pass and training step (backward + Adam)
+    on random inputs of the given grid and batch: wall time over `steps`
+    calls between two synchronisations of the network's stream.
+
+        python ehd-convection-3d_b200/fno.py --grid 64 64 33 --batch 4
+    """
+    import argparse
+    import json
+    import time
+
+    import torch
+    ap = argparse.ArgumentParser(description="time the FNO forward pass and training step")
+    ap.add_argument("--grid", type=int, nargs=3, default=(64, 64, 33), metavar=("NX", "NY", "NZ"))
+    ap.add_argument("--in-channels", type=int, default=9)
+    ap.add_argument("--out-channels", type=int, default=5)
+    ap.add_argument("--width", type=int, default=32)
+    ap.add_argument("--layers", type=int, default=4)
+    ap.add_argument("--modes", type=int, default=12)
+    ap.add_argument("--hidden", type=int, default=128)
+    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    a = ap.parse_args(argv)
+    nx, ny, nz = a.grid
+    net = FNO(nx, ny, nz, a.in_channels, a.out_channels, width=a.width, layers=a.layers,
+              modes=(a.modes, a.modes, min(a.modes, nz // 2)), hidden=a.hidden,
+              max_batch=a.batch, seed=7)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn(a.batch, nz, ny, nx, a.in_channels, device="cuda", generator=g)
+    t = torch.randn(a.batch, nz, ny, nx, a.out_channels, device="cuda", generator=g)
+    for _ in range(a.warmup):
+        net.forward(x)
+        net.backward(x, t)
+        net.adam_step(1e-4)
+    net.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        net.forward(x)
+    net.synchronize()
+    t1 = time.perf_counter()
+    for _ in range(a.steps):
+        net.backward(x, t)
+        net.adam_step(1e-4)
+    net.synchronize()
+    t2 = time.perf_counter()
+    out = {"grid": [nx, ny, nz], "batch": a.batch, "width": a.width, "layers": a.layers,
+           "modes": a.modes, "parameters": net.nparam,
+           "forward_ms": 1e3 * (t1 - t0) / max(1, a.steps),
+           "train_step_ms": 1e3 * (t2 - t1) / max(1, a.steps)}
+    print(json.dumps(out), flush=True)
+    net.close()
+    return out
+
+
+if __name__ == "__main__":
+    main()
