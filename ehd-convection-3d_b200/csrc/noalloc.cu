@@ -198,14 +198,13 @@ extern "C" int ehd_poisson_noalloc(const ehd_params *p, const double *q, double 
     a.dz = p->dz;
 
     const size_t nxy = (size_t)nx * ny;
-    cudaError_t e;
     // every region the solve reads before writing is set here: the tables,
     // the zero reference charge, and phi' = 0 on both electrodes
     twiddle_kernel<<<(nx + 255) / 256, 256, 0, s>>>(twx, nx);
     twiddle_kernel<<<(ny + 255) / 256, 256, 0, s>>>(twy, ny);
     pivot_kernel<<<(unsigned)((modes + 127) / 128), 128, 0, s>>>(cpt, nx, ny, nz, p->lx, p->ly,
                                                                   p->dz);
-    if ((e = cudaGetLastError()) != cudaSuccess)
+    if (cudaGetLastError() != cudaSuccess)
         return set_error(EHD_ERR_CUDA, "ehd_poisson_noalloc: table kernels failed to launch");
     if (cudaMemsetAsync(qmean, 0, sizeof(double) * 2 * nz, s) != cudaSuccess ||
         cudaMemsetAsync(phi, 0, sizeof(double) * nxy, s) != cudaSuccess ||
