@@ -869,15 +869,19 @@ int ehd_hydrostatic_profile(const ehd_params *params, const ehd_config *config, 
     std::vector<double> f(9 * (size_t)nz);
     double *fp[9];
     for (int k = 0; k < 9; ++k) fp[k] = f.data() + (size_t)k * nz;
-    ehd_diag d{};
+    // I0: the mean of the column's currents after nsteps and nsteps + 1 steps
+    // (the injection boundary makes the current alternate with a period of
+    // two steps; the profile is the state after nsteps)
+    ehd_diag d{}, d1{};
     if ((r = ehd_initialize(col)) == EHD_OK && (r = ehd_step(col, nsteps)) == EHD_OK &&
         (r = ehd_get_fields(col, fp[0], fp[1], fp[2], fp[3], fp[4], fp[5], fp[6], fp[7],
-                            fp[8])) == EHD_OK)
-        r = ehd_diagnostics(col, &d);
+                            fp[8])) == EHD_OK &&
+        (r = ehd_diagnostics(col, &d)) == EHD_OK && (r = ehd_step(col, 1)) == EHD_OK)
+        r = ehd_diagnostics(col, &d1);
     ehd_destroy(col);
     if (r != EHD_OK) return r;
     std::memcpy(profile, f.data(), sizeof(double) * 9 * nz);
-    if (i0) *i0 = d.current * (double)params->nx * (double)params->ny;
+    if (i0) *i0 = 0.5 * (d.current + d1.current) * (double)params->nx * (double)params->ny;
     return EHD_OK;
 }
 
@@ -886,19 +890,26 @@ int ehd_run_to_saturation(ehd_ctx *c, int sample_every, double tol, int hold, in
     if (!c || sample_every < 1 || hold < 1 || !(tol > 0) || max_steps < 0)
         return fail(EHD_ERR_INVALID, "bad arguments");
     if (c->i0 == 0.0) return fail(EHD_ERR_STATE, "reference current I0 not set");
-    double prev = 0.0;
+    double prev = 0.0, nu = 0.0;
     int held = 0, ok = 0;
     int64_t done = 0;
-    ehd_diag d{};
     bool first = true;
     while (done < max_steps) {
+        // a sample is the mean of the currents after the last two steps of
+        // its interval: the injection boundary makes the current alternate
+        // with a period of two steps
         const int n = (int)std::min<int64_t>(sample_every, max_steps - done);
-        int r = ehd_step(c, n);
-        if (r == EHD_OK) r = ehd_diagnostics(c, &d);
+        ehd_diag da{}, db{};
+        int r = n >= 2 ? ehd_step(c, n - 1) : EHD_OK;
+        if (r == EHD_OK && n >= 2) r = ehd_diagnostics(c, &da);
+        if (r == EHD_OK) r = ehd_step(c, 1);
+        if (r == EHD_OK) r = ehd_diagnostics(c, &db);
         if (r != EHD_OK) return r;
         done += n;
-        if (d.nonfinite) return fail(EHD_ERR_NUMERIC, "non-finite field after %lld steps", (long long)done);
-        if (!first && std::fabs(d.nu_e - prev) <= tol * std::fabs(d.nu_e)) {
+        if (da.nonfinite || db.nonfinite)
+            return fail(EHD_ERR_NUMERIC, "non-finite field after %lld steps", (long long)done);
+        nu = n >= 2 ? 0.5 * (da.current + db.current) / c->i0 : db.nu_e;
+        if (!first && std::fabs(nu - prev) <= tol * std::fabs(nu)) {
             if (++held >= hold) {
                 ok = 1;
                 break;
@@ -906,10 +917,10 @@ int ehd_run_to_saturation(ehd_ctx *c, int sample_every, double tol, int hold, in
         } else {
             held = 0;
         }
-        prev = d.nu_e;
+        prev = nu;
         first = false;
     }
-    if (nu_e) *nu_e = d.nu_e;
+    if (nu_e) *nu_e = nu;
     if (steps) *steps = done;
     if (saturated) *saturated = ok;
     return EHD_OK;

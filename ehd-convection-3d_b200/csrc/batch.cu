@@ -248,28 +248,43 @@ int ehd_batch_run_to_saturation(ehd_batch *b, int sample_every, double tol, int 
         if (b->active[i] && ctx_reference_current(b->inst[i]) == 0.0)
             return err(EHD_ERR_STATE, "ehd_batch_run_to_saturation: reference current I0 not set");
     std::vector<char> run = b->active;
-    std::vector<double> prev(n, 0.0), last(n, 0.0);
-    std::vector<int> held(n, 0), ok(n, 0);
+    std::vector<double> prev(n, 0.0), last(n, 0.0), ia(n, 0.0);
+    std::vector<int> held(n, 0), ok(n, 0), bad(n, 0);
     std::vector<char> first(n, 1);
     int64_t done = 0;
     while (done < max_steps) {
         if (std::none_of(run.begin(), run.end(), [](char a) { return a != 0; })) break;
+        // as ehd_run_to_saturation: a sample is the mean of the currents after
+        // the last two steps of its interval
         const int k = (int)std::min<int64_t>(sample_every, max_steps - done);
-        int r = batch_step(b, run, k);
-        if (r != EHD_OK) return r;
+        int r = EHD_OK;
+        if (k >= 2) {
+            if ((r = batch_step(b, run, k - 1)) != EHD_OK) return r;
+            for (size_t i = 0; i < n; ++i) {
+                if (!run[i]) continue;
+                ehd_diag d{};
+                if ((r = ehd_diagnostics(b->inst[i], &d)) != EHD_OK) return r;
+                ia[i] = d.current;
+                bad[i] = d.nonfinite;
+            }
+        }
+        if ((r = batch_step(b, run, 1)) != EHD_OK) return r;
         done += k;
         for (size_t i = 0; i < n; ++i) {
             if (!run[i]) continue;
             ehd_diag d{};
             if ((r = ehd_diagnostics(b->inst[i], &d)) != EHD_OK) return r;
-            last[i] = d.nu_e;
             if (steps) steps[i] = done;
-            if (d.nonfinite) {  // this instance stops; the others go on
+            if (d.nonfinite || (k >= 2 && bad[i])) {  // this instance stops; the others go on
+                last[i] = d.nu_e;
                 ok[i] = -1;
                 run[i] = 0;
                 continue;
             }
-            if (!first[i] && std::fabs(d.nu_e - prev[i]) <= tol * std::fabs(d.nu_e)) {
+            const double nu =
+                k >= 2 ? 0.5 * (ia[i] + d.current) / ctx_reference_current(b->inst[i]) : d.nu_e;
+            last[i] = nu;
+            if (!first[i] && std::fabs(nu - prev[i]) <= tol * std::fabs(nu)) {
                 if (++held[i] >= hold) {
                     ok[i] = 1;
                     run[i] = 0;
@@ -277,7 +292,7 @@ int ehd_batch_run_to_saturation(ehd_batch *b, int sample_every, double tol, int 
             } else {
                 held[i] = 0;
             }
-            prev[i] = d.nu_e;
+            prev[i] = nu;
             first[i] = 0;
         }
     }

@@ -196,6 +196,25 @@ def groups_of(p: Params):
     return dict(zip(("T", "M", "C", "Fe"), [o.value for o in out]))
 
 
+def _sampled(sims, n: int, step) -> list:
+    if n < 1:
+        raise ValueError("n must be >= 1")
+    first = None
+    if n >= 2:
+        step(n - 1)
+        first = [s.diagnostics()["current"] for s in sims]
+    step(1)
+    out = []
+    for k, s in enumerate(sims):
+        d = s.diagnostics()
+        mean = d["current"] if first is None else 0.5 * (first[k] + d["current"])
+        if d["current"] != 0.0:  # nu_e = current / I0
+            d["nu_e"] *= mean / d["current"]
+        d["current_mean"] = mean
+        out.append(d)
+    return out
+
+
 class Simulation:
     """One simulation instance (ehd_ctx) on one GPU."""
 
@@ -255,6 +274,13 @@ class Simulation:
 
     def step(self, n: int = 1):
         _check(lib().ehd_step(self.h, int(n)))
+
+    def step_sampled(self, n: int) -> dict:
+        """Steps n >= 1 steps; the diagnostics after the last one, with nu_e
+        the mean of the currents after the last two steps over I0, as
+        ehd_run_to_saturation samples it (the injector makes the current
+        alternate with a period of two steps)."""
+        return _sampled([self], n, self.step)[0]
 
     def stream_collide_save(self):
         _check(lib().ehd_stream_collide_save(self.h))
@@ -352,6 +378,10 @@ class Batch:
 
     def step(self, n: int = 1):
         _check(lib().ehd_batch_step(self.h, int(n)))
+
+    def step_sampled(self, n: int) -> list:
+        """Simulation.step_sampled for every instance: one list entry each."""
+        return _sampled(self.instances, n, self.step)
 
     def autotune(self, trial_steps: int = 20):
         _check(lib().ehd_batch_autotune(self.h, int(trial_steps)))

@@ -44,19 +44,23 @@ SIGNATURES = {
                            _i64, _i64, _i64, ctypes.c_float, ctypes.c_float, _vp]),
 }
 
-_bound = False
+_lib = None
 
 
 def lib():
-    global _bound
-    L = ehd.lib()
-    if not _bound:
+    """libehd.so through a handle of this module's own, so that the argument
+    types bound here (this module's Config) do not clash with another copy of
+    this module loaded under a different name."""
+    global _lib
+    if _lib is None:
+        ehd.lib()  # raises if the library was not built
+        L = ctypes.CDLL(str(ehd.LIB_PATH))
         for name, (res, args) in SIGNATURES.items():
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args
-        _bound = True
-    return L
+        _lib = L
+    return _lib
 
 
 def _fptr(a: np.ndarray):

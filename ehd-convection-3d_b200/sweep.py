@@ -95,10 +95,14 @@ def hydrostatic_profiles(ehd, params: list, nsteps: list, device=0):
             for sim in b:
                 sim.initialize()
             b.step(n)
-            for i, sim in zip(idx, b):
+            profs, cur = [], []
+            for sim in b:
                 f = sim.get_fields()
-                prof = {k: np.asarray(v).reshape(-1).copy() for k, v in f.items()}
-                i0 = sim.diagnostics()["current"] * params[i].nx * params[i].ny
+                profs.append({k: np.asarray(v).reshape(-1).copy() for k, v in f.items()})
+                cur.append(sim.diagnostics()["current"])
+            b.step(1)  # I0: mean of the currents after n and n + 1 steps
+            for i, sim, prof, c0 in zip(idx, b, profs, cur):
+                i0 = 0.5 * (c0 + sim.diagnostics()["current"]) * params[i].nx * params[i].ny
                 out[i] = (prof, i0)
     return out
 

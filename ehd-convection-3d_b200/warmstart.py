@@ -87,10 +87,9 @@ def trajectories(ehd, groups, horizon, chunk=64, transits=4.0, precision="fp32",
                 sim.set_state_seeded(prof, seed=g["seed"], amp=1e-3)
                 sim.set_reference_current(i0)
                 firsts.append(sim.get_fields())
-            b.step(horizon)
             keep = []
-            for sim, g, p, f0, (prof, i0) in zip(b, gs, ps, firsts, starts):
-                d = sim.diagnostics()
+            for sim, g, p, f0, (prof, i0), d in zip(b, gs, ps, firsts, starts,
+                                                    b.step_sampled(horizon)):
                 if d["nonfinite"]:
                     keep.append(False)
                     continue
@@ -100,11 +99,10 @@ def trajectories(ehd, groups, horizon, chunk=64, transits=4.0, precision="fp32",
                 outs.append(targets(f1, p))
                 info.append(dict(g, nu_e=d["nu_e"], kinetic_energy=d["kinetic_energy"], i0=i0))
             if extra > 0:
-                b.step(extra)
                 k = len(info) - sum(keep)
-                for sim, kp in zip(b, keep):
+                for d, kp in zip(b.step_sampled(extra), keep):
                     if kp:
-                        info[k]["nu_e_extra"] = sim.diagnostics()["nu_e"]
+                        info[k]["nu_e_extra"] = d["nu_e"]
                         k += 1
     return np.stack(ins), np.stack(outs), info
 
@@ -210,11 +208,11 @@ def main(argv=None):
             bw[k].set_reference_current(i0)
             bn[k].set_state_seeded(prof, seed=ite[k]["seed"], amp=1e-3)
             bn[k].set_reference_current(i0)
-        bw.step(a.relax)
-        bn.step(a.relax)
+        dw = bw.step_sampled(a.relax)
+        dn = bn.step_sampled(a.relax)
         for k in range(m):
-            nu_warm.append(bw[k].diagnostics()["nu_e"])
-            nu_none.append(bn[k].diagnostics()["nu_e"])
+            nu_warm.append(dw[k]["nu_e"])
+            nu_none.append(dn[k]["nu_e"])
             nu_cold.append(ite[k]["nu_e_extra"])
     res = {
         "train": len(itr), "test": len(ite), "horizon": a.horizon, "epochs": a.epochs,

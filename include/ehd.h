@@ -176,8 +176,10 @@ int ehd_diagnostics(ehd_ctx *ctx, ehd_diag *out);
  * reference's initialization (LBM.cu:69-96) for nsteps steps (even; the
  * injector alternates with period 2).  profile receives 9*NZ doubles, field
  * k at profile[k*NZ + z] in the order rho, u, v, w, q, phi, ex, ey, ez;
- * *i0 the current of that state on the full NX x NY plane (the Nu_e
- * normaliser).  Not in the reference, which starts from q = 0. */
+ * *i0 the mean of the column's currents after nsteps and nsteps + 1 steps
+ * on the full NX x NY plane (the Nu_e normaliser; the current alternates
+ * between two values, 1.5 % apart at 64 x 64 x 33).  Not in the reference,
+ * which starts from q = 0. */
 int ehd_hydrostatic_profile(const ehd_params *params, const ehd_config *config, int nsteps,
                             double *profile, double *i0);
 
@@ -192,7 +194,10 @@ int ehd_set_state_seeded(ehd_ctx *ctx, const double *profile, uint64_t seed, dou
 /* Steps until the electric Nusselt number Nu_e = I / I0 (I0 from
  * ehd_set_reference_current) changes by less than tol relative between
  * consecutive samples every sample_every steps, hold times in a row, or until
- * max_steps.  *saturated tells which; *nu_e is the last sample. */
+ * max_steps.  A sample is the mean of the currents after the last two steps
+ * of its interval (the injector makes the current alternate with a period of
+ * two steps), over I0.  *saturated tells which; *nu_e is the last sample.
+ * ehd_diagnostics' nu_e is the single-step ratio. */
 int ehd_run_to_saturation(ehd_ctx *ctx, int sample_every, double tol, int hold,
                           int64_t max_steps, double *nu_e, int64_t *steps, int *saturated);
 

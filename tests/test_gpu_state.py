@@ -16,17 +16,28 @@ def config0():
     return M, M.case_params("config0"), golden("config0")
 
 
+def _plane_current(p, prof):
+    shape = (p.nz, p.ny, p.nx)
+    return O.current_of(p, np.broadcast_to(prof["q"][:, None, None], shape),
+                        np.broadcast_to(prof["ez"][:, None, None], shape))
+
+
 def test_hydrostatic_profile_matches_oracle():
     """The u = 0 steady state of the step on a 1 x 1 x NZ column, run on the
     GPU in FP64, against the oracle's column run over the same steps
-    (stored in the config-0 fixture)."""
+    (stored in the config-0 fixture).  I0 is the mean of the currents after
+    n and n + 1 steps: the injector makes the column's current alternate
+    between two values with a period of two steps."""
     M, p, g = config0()
-    prof, i0 = ehd.hydrostatic_profile(to_ehd(p), M.hydrostatic_steps(p))
+    n = M.hydrostatic_steps(p)
+    prof, i0 = ehd.hydrostatic_profile(to_ehd(p), n)
     for k in ("rho", "q", "phi", "ez"):
         assert relerr(prof[k], g[f"prof_{k}"]) < 1e-8, k
-    ref_i0 = O.current_of(p, np.broadcast_to(g["prof_q"][:, None, None], (p.nz, p.ny, p.nx)),
-                          np.broadcast_to(g["prof_ez"][:, None, None], (p.nz, p.ny, p.nx)))
-    assert i0 == pytest.approx(ref_i0, rel=1e-8)
+    i_n = _plane_current(p, {"q": g["prof_q"], "ez": g["prof_ez"]})
+    prof1, _ = O.hydrostatic_profile(p, tol=-1.0, check_every=n + 1, max_steps=n + 1)
+    i_n1 = _plane_current(p, prof1)
+    assert abs(i_n1 / i_n - 1.0) > 1e-3  # the two phases differ
+    assert i0 == pytest.approx(0.5 * (i_n + i_n1), rel=1e-8)
 
 
 @pytest.mark.parametrize("seed", [0, 7])
@@ -130,14 +141,18 @@ def test_run_to_saturation_mechanics():
         # a loose tolerance holds from the second sample on: 1 + 3 samples
         r = sim.run_to_saturation(sample_every=20, tol=10.0, hold=3, max_steps=2000)
         assert r["saturated"] and r["steps"] == 80
-        # Nu_e = I / I0 of the state after those 80 steps, as the oracle has
-        # it (the electrode current still swings through negative values
-        # this early after the start from the column profile)
+        # Nu_e of the last sample: the mean of the currents after 79 and 80
+        # steps over I0, as the oracle has them (the electrode current still
+        # swings through negative values this early after the start from
+        # the column profile)
         o = O.Oracle(p)
         o.set_fields(O.state_from_profile(p, prof, amp=0.0))
-        o.step(80)
-        ref = o.get_fields()
-        assert r["nu_e"] == pytest.approx(O.current_of(p, ref["q"], ref["ez"]) / i0, rel=1e-3)
+        o.step(79)
+        a = o.get_fields()
+        o.step(1)
+        b = o.get_fields()
+        ref = 0.5 * (O.current_of(p, a["q"], a["ez"]) + O.current_of(p, b["q"], b["ez"])) / i0
+        assert r["nu_e"] == pytest.approx(ref, rel=1e-3)
         # an impossible tolerance runs out the budget
         r = sim.run_to_saturation(sample_every=20, tol=1e-300, hold=3, max_steps=60)
         assert not r["saturated"] and r["steps"] == 60
