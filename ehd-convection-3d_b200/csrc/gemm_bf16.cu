@@ -220,6 +220,282 @@ __global__ void __launch_bounds__(128, 4) gemm_kernel(const GemmArgs a) {
             }
 }
 
+// ---- row-streaming products ---------------------------------------------
+//
+// For products whose A is FP32 with unit stride along k (rows lda elements
+// apart), K a multiple of 16 up to 128 and N up to 128 -- the pointwise layers
+// and their input gradients.  B (K x N) is staged once per block in shared
+// memory as BF16 [n][k]; each warp then streams 16-row tiles of A from global
+// memory straight into its mma.sync A fragments (two FP32 per 64-bit load,
+// converted to a BF16 pair), and writes its C fragments directly, two FP32
+// per 64-bit store where C's rows allow.  Warps take tiles independently
+// (no block barrier after the B stage); with KT <= 2 the next tile's loads
+// are in flight during the current tile's products and epilogue.
+constexpr int RW_WARPS = 8;
+
+__device__ __forceinline__ float2 ldg2(const float *p) {
+    return __ldg(reinterpret_cast<const float2 *>(p));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float2 v) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
+    return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+template <int KT>
+__device__ __forceinline__ void rw_load(float2 (&v)[KT][4], const float *A, int lda, int M,
+                                        int tile, int gq, int tq) {
+    const int r0 = tile * 16 + gq, r1 = r0 + 8;
+    const bool ok0 = r0 < M, ok1 = r1 < M;
+    const float *p0 = A + (size_t)(ok0 ? r0 : 0) * lda + 2 * tq;
+    const float *p1 = A + (size_t)(ok1 ? r1 : 0) * lda + 2 * tq;
+    const float2 z = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int s = 0; s < KT; ++s) {
+        v[s][0] = ok0 ? ldg2(p0 + 16 * s) : z;
+        v[s][1] = ok1 ? ldg2(p1 + 16 * s) : z;
+        v[s][2] = ok0 ? ldg2(p0 + 16 * s + 8) : z;
+        v[s][3] = ok1 ? ldg2(p1 + 16 * s + 8) : z;
+    }
+}
+
+template <int KT, int NT>
+__global__ void __launch_bounds__(256) rowwise_kernel(const GemmArgs a, int lda, int ldc,
+                                                      int pair_store) {
+    constexpr int PKB = 16 * KT + 8;  // padded row of B (BF16 elements)
+    constexpr bool PF = KT <= 2;      // prefetch the next tile
+    extern __shared__ __align__(16) unsigned char rw_smem[];
+    __nv_bfloat16 *Bs = reinterpret_cast<__nv_bfloat16 *>(rw_smem);  // [8 NT][PKB]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int gq = lane >> 2, tq = lane & 3;
+    const int bidx = blockIdx.y;
+    {
+        const long long boff = at(a.bbat, bidx);
+        for (int i = tid; i < 8 * NT * 16 * KT; i += blockDim.x) {
+            const int n = i / (16 * KT), k = i - n * (16 * KT);
+            float v = 0.f;
+            if (n < a.N && k < a.K) {
+                const long long o = boff + at(a.bk, k) + at(a.bn, n);
+                v = a.b_bf16 ? __bfloat162float(reinterpret_cast<const __nv_bfloat16 *>(a.B)[o])
+                             : reinterpret_cast<const float *>(a.B)[o];
+            }
+            Bs[n * PKB + k] = __float2bfloat16_rn(v);
+        }
+    }
+    __syncthreads();
+    const float *A = reinterpret_cast<const float *>(a.A) + at(a.abat, bidx);
+    float *C = a.C + at(a.cbat, bidx);
+    float *C2 = a.C2 ? a.C2 + at(a.cbat, bidx) : nullptr;
+    const int tiles = (a.M + 15) / 16;
+    const int tstride = gridDim.x * RW_WARPS;
+    int t = blockIdx.x * RW_WARPS + warp;
+    float2 cur[KT][4];
+    if (PF && t < tiles) rw_load<KT>(cur, A, lda, a.M, t, gq, tq);
+    for (; t < tiles; t += tstride) {
+        if (!PF) rw_load<KT>(cur, A, lda, a.M, t, gq, tq);
+        uint32_t af[KT][4];
+#pragma unroll
+        for (int s = 0; s < KT; ++s)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) af[s][e] = pack_bf16(cur[s][e]);
+        if (PF && t + tstride < tiles) rw_load<KT>(cur, A, lda, a.M, t + tstride, gq, tq);
+        float acc[NT][4];
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[j][e] = 0.f;
+            const __nv_bfloat16 *bp = Bs + (8 * j + gq) * PKB + 2 * tq;
+#pragma unroll
+            for (int s = 0; s < KT; ++s) {
+                const uint32_t b0 = *reinterpret_cast<const uint32_t *>(bp + 16 * s);
+                const uint32_t b1 = *reinterpret_cast<const uint32_t *>(bp + 16 * s + 8);
+                mma16816(acc[j], af[s][0], af[s][1], af[s][2], af[s][3], b0, b1);
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int m = t * 16 + gq + 8 * h;
+            if (m >= a.M) continue;
+            float *crow = C + (size_t)m * ldc;
+            float *c2row = C2 ? C2 + (size_t)m * ldc : nullptr;
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+                const int n = 8 * j + 2 * tq;
+                if (n >= a.N) continue;
+                float v0 = a.alpha * acc[j][2 * h], v1 = a.alpha * acc[j][2 * h + 1];
+                if (pair_store && n + 1 < a.N) {
+                    if (a.beta != 0.f) {
+                        const float2 o = *reinterpret_cast<const float2 *>(crow + n);
+                        v0 += a.beta * o.x;
+                        v1 += a.beta * o.y;
+                    }
+                    if (a.bias) {
+                        v0 += __ldg(a.bias + n);
+                        v1 += __ldg(a.bias + n + 1);
+                    }
+                    *reinterpret_cast<float2 *>(crow + n) = make_float2(v0, v1);
+                    if (c2row) *reinterpret_cast<float2 *>(c2row + n) = make_float2(gelu(v0), gelu(v1));
+                } else {
+                    if (a.beta != 0.f) v0 += a.beta * crow[n];
+                    if (a.bias) v0 += __ldg(a.bias + n);
+                    crow[n] = v0;
+                    if (c2row) c2row[n] = gelu(v0);
+                    if (n + 1 < a.N) {
+                        if (a.beta != 0.f) v1 += a.beta * crow[n + 1];
+                        if (a.bias) v1 += __ldg(a.bias + n + 1);
+                        crow[n + 1] = v1;
+                        if (c2row) c2row[n + 1] = gelu(v1);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ---- products by a small left matrix --------------------------------------
+//
+// For C[b][m][n] = alpha sum_k A[m][k] B[b][k][n] with one A for the whole
+// batch, M, K <= 128, and B FP32 with unit stride along n -- the truncated
+// DFTs of the FNO, whose B is the activation tensor and A the DFT matrix.  A
+// is staged once per block in shared memory as BF16 [m][k]; each warp then
+// takes units of 8 NT consecutive columns of one batch entry and loads its
+// mma.sync B fragments straight from global memory (lanes along n: every
+// load instruction reads four fully used 32-byte sectors), the next K step's
+// fragments in flight during the current step's products, and writes its C
+// fragments directly (64-bit stores where C's layout allows).
+template <int NT>
+__device__ __forceinline__ void lm_load(float (&rb)[NT][4], const float *B, const int (&bno)[NT],
+                                        unsigned nmask, const Map &bk, int K, int s, int tq) {
+    const int k0 = 16 * s + 2 * tq;
+    int ko[4];
+    bool kin[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const int k = k0 + (e & 1) + (e >> 1) * 8;
+        kin[e] = k < K;
+        ko[e] = kin[e] ? at_off<int>(bk, k) : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            rb[j][e] = (kin[e] && (nmask >> j & 1u)) ? __ldg(B + bno[j] + ko[e]) : 0.f;
+}
+
+template <int MT, int NT>
+__global__ void __launch_bounds__(256) leftmul_kernel(const GemmArgs a, int pair_store) {
+    constexpr int NC = 8 * NT;
+    extern __shared__ __align__(16) unsigned char lm_smem[];
+    const int kt = (a.K + 15) / 16, KP = 16 * kt + 8;
+    __nv_bfloat16 *As = reinterpret_cast<__nv_bfloat16 *>(lm_smem);  // [16 MT][KP]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int gq = lane >> 2, tq = lane & 3;
+    for (int i = tid; i < 16 * MT * 16 * kt; i += blockDim.x) {
+        const int m = i / (16 * kt), k = i - m * (16 * kt);
+        float v = 0.f;
+        if (m < a.M && k < a.K) {
+            const long long o = at(a.am, m) + at(a.ak, k);
+            v = a.a_bf16 ? __bfloat162float(reinterpret_cast<const __nv_bfloat16 *>(a.A)[o])
+                         : reinterpret_cast<const float *>(a.A)[o];
+        }
+        As[m * KP + k] = __float2bfloat16_rn(v);
+    }
+    __syncthreads();
+    const float *B = reinterpret_cast<const float *>(a.B);
+    const int chunks = (a.N + NC - 1) / NC;
+    const long long units = (long long)a.batch * chunks;
+    for (long long u = (long long)blockIdx.x * 8 + warp; u < units; u += (long long)gridDim.x * 8) {
+        const int bidx = (int)(u / chunks), n0 = (int)(u - (long long)bidx * chunks) * NC;
+        const int boff = at_off<int>(a.bbat, bidx);
+        int bno[NT];
+        unsigned nmask = 0;
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+            const int n = n0 + 8 * j + gq;
+            bno[j] = boff + (n < a.N ? at_off<int>(a.bn, n) : 0);
+            nmask |= (n < a.N ? 1u : 0u) << j;
+        }
+        float acc[MT][NT][4];
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NT; ++j)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+        float rb[NT][4];
+        lm_load<NT>(rb, B, bno, nmask, a.bk, a.K, 0, tq);
+        for (int s = 0; s < kt; ++s) {
+            uint32_t bf[NT][2];
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+                bf[j][0] = pack_bf16(make_float2(rb[j][0], rb[j][1]));
+                bf[j][1] = pack_bf16(make_float2(rb[j][2], rb[j][3]));
+            }
+            if (s + 1 < kt) lm_load<NT>(rb, B, bno, nmask, a.bk, a.K, s + 1, tq);
+#pragma unroll
+            for (int i = 0; i < MT; ++i) {
+                const __nv_bfloat16 *ap = As + (16 * i + gq) * KP + 16 * s + 2 * tq;
+                const uint32_t a0 = *reinterpret_cast<const uint32_t *>(ap);
+                const uint32_t a1 = *reinterpret_cast<const uint32_t *>(ap + 8 * KP);
+                const uint32_t a2 = *reinterpret_cast<const uint32_t *>(ap + 8);
+                const uint32_t a3 = *reinterpret_cast<const uint32_t *>(ap + 8 * KP + 8);
+#pragma unroll
+                for (int j = 0; j < NT; ++j) mma16816(acc[i][j], a0, a1, a2, a3, bf[j][0], bf[j][1]);
+            }
+        }
+        // epilogue: rows 16 i + gq + 8 h, columns n0 + 8 j + 2 tq (+1)
+        const int coff = at_off<int>(a.cbat, bidx);
+        int cno[NT];
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+            const int n = n0 + 8 * j + 2 * tq;
+            cno[j] = n < a.N ? at_off<int>(a.cn, n) : 0;
+        }
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int m = 16 * i + gq + 8 * h;
+                if (m >= a.M) continue;
+                const int mo = coff + at_off<int>(a.cm, m);
+#pragma unroll
+                for (int j = 0; j < NT; ++j) {
+                    const int n = n0 + 8 * j + 2 * tq;
+                    if (n >= a.N) continue;
+                    float v0 = a.alpha * acc[i][j][2 * h], v1 = a.alpha * acc[i][j][2 * h + 1];
+                    float *c = a.C + mo + cno[j];
+                    if (pair_store && n + 1 < a.N) {
+                        if (a.beta != 0.f) {
+                            const float2 o = *reinterpret_cast<const float2 *>(c);
+                            v0 += a.beta * o.x;
+                            v1 += a.beta * o.y;
+                        }
+                        if (a.bias) {
+                            v0 += __ldg(a.bias + n);
+                            v1 += __ldg(a.bias + n + 1);
+                        }
+                        *reinterpret_cast<float2 *>(c) = make_float2(v0, v1);
+                        if (a.C2)
+                            *reinterpret_cast<float2 *>(a.C2 + mo + cno[j]) =
+                                make_float2(gelu(v0), gelu(v1));
+                    } else {
+                        if (a.beta != 0.f) v0 += a.beta * *c;
+                        if (a.bias) v0 += __ldg(a.bias + n);
+                        *c = v0;
+                        if (a.C2) a.C2[mo + cno[j]] = gelu(v0);
+                        if (n + 1 < a.N) {
+                            const int o1 = mo + at_off<int>(a.cn, n + 1);
+                            if (a.beta != 0.f) v1 += a.beta * a.C[o1];
+                            if (a.bias) v1 += __ldg(a.bias + n + 1);
+                            a.C[o1] = v1;
+                            if (a.C2) a.C2[o1] = gelu(v1);
+                        }
+                    }
+                }
+            }
+    }
+}
+
 }  // namespace
 
 namespace {
@@ -254,6 +530,135 @@ const Kern *kernel_table() { return table(std::make_integer_sequence<int, 16>{})
 
 }  // namespace
 
+namespace {
+
+using RowKern = void (*)(const GemmArgs, int, int, int);
+
+template <int KT>
+RowKern row_kernel(int nt) {
+    switch (nt) {
+        case 1: return rowwise_kernel<KT, 1>;
+        case 2: return rowwise_kernel<KT, 2>;
+        case 4: return rowwise_kernel<KT, 4>;
+        case 8: return rowwise_kernel<KT, 8>;
+        default: return rowwise_kernel<KT, 16>;
+    }
+}
+
+bool aligned8(const void *p) { return ((uintptr_t)p & 7u) == 0; }
+bool one_level(const Map &m) { return m.g == (1 << 30); }
+
+// The row-streaming kernel when the product has its shape: A FP32 with unit
+// stride along k, lda and the batch offsets even, 16 | K <= 128, N <= 128,
+// unit stride along n in C, no split K.  Returns false to leave the product
+// to the tiled kernel.
+bool try_rowwise(const GemmArgs &a, cudaStream_t s, cudaError_t *err) {
+    if (a.a_bf16 || a.ksplit != 1 || a.K % 16 != 0 || a.K > 128 || a.N > 128) return false;
+    if (!one_level(a.am) || !one_level(a.ak) || !one_level(a.abat) || !one_level(a.cm) ||
+        !one_level(a.cn) || !one_level(a.cbat))
+        return false;
+    // (the batch maps matter only with more than one product)
+    const bool odd_abat = a.batch > 1 && (a.abat.s0 & 1);
+    if (a.ak.s0 != 1 || a.cn.s0 != 1 || a.am.s0 < a.K || (a.am.s0 & 1) || odd_abat ||
+        !aligned8(a.A) || a.am.s0 > (1ll << 30) || a.cm.s0 > (1ll << 30))
+        return false;
+    const int kt = a.K / 16;
+    const int nt = a.N <= 8 ? 1 : a.N <= 16 ? 2 : a.N <= 32 ? 4 : a.N <= 64 ? 8 : 16;
+    RowKern k = nullptr;
+    switch (kt) {
+        case 1: k = row_kernel<1>(nt); break;
+        case 2: k = row_kernel<2>(nt); break;
+        case 4: k = row_kernel<4>(nt); break;
+        case 8: k = row_kernel<8>(nt); break;
+        default: return false;  // K = 48, 80, 96, 112: the tiled kernel
+    }
+    const int pair = (a.cm.s0 % 2 == 0 && (a.batch == 1 || a.cbat.s0 % 2 == 0) && aligned8(a.C) &&
+                      (!a.C2 || aligned8(a.C2)))
+                         ? 1
+                         : 0;
+    const size_t smem = (size_t)8 * nt * (16 * kt + 8) * sizeof(__nv_bfloat16);
+    int dev = 0, nsm = 0, occ = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 256, smem)) != cudaSuccess) {
+        *err = e;
+        return true;
+    }
+    const long long tiles = (a.M + 15) / 16;
+    const long long want = (tiles + RW_WARPS - 1) / RW_WARPS;
+    const long long per_batch = std::max(1ll, (long long)nsm * std::max(occ, 1) / a.batch);
+    dim3 grid((unsigned)std::min(want, per_batch), (unsigned)a.batch, 1);
+    k<<<grid, 256, smem, s>>>(a, (int)a.am.s0, (int)a.cm.s0, pair);
+    *err = cudaGetLastError();
+    return true;
+}
+
+using LeftKern = void (*)(const GemmArgs, int);
+
+template <int NT>
+LeftKern left_kernel_nt(int mt) {
+    switch (mt) {
+        case 1: return leftmul_kernel<1, NT>;
+        case 2: return leftmul_kernel<2, NT>;
+        case 3: return leftmul_kernel<3, NT>;
+        case 4: return leftmul_kernel<4, NT>;
+        case 5: return leftmul_kernel<5, NT < 4 ? NT : 2>;
+        case 6: return leftmul_kernel<6, NT < 4 ? NT : 2>;
+        case 7: return leftmul_kernel<7, NT < 4 ? NT : 2>;
+        default: return leftmul_kernel<8, NT < 4 ? NT : 2>;
+    }
+}
+
+// 8 NT columns per warp unit: the widest unit (at most 64 accumulators a
+// thread, MT NT <= 16) that still gives 4096 units, so that every warp of
+// a full GPU has several to interleave
+int left_nt(int mt, long long batch, int N) {
+    for (int nt = 4; nt > 1; nt /= 2)
+        if (mt * nt <= 16 && batch * ((N + 8 * nt - 1) / (8 * nt)) >= 4096) return nt;
+    return 1;
+}
+
+LeftKern left_kernel(int mt, int nt) {
+    return nt == 4 ? left_kernel_nt<4>(mt) : nt == 2 ? left_kernel_nt<2>(mt) : left_kernel_nt<1>(mt);
+}
+
+bool even_map(const Map &m) { return (m.s0 % 2 == 0) && (one_level(m) || m.s1 % 2 == 0); }
+
+// The small-left-matrix kernel when the product has its shape: one A for the
+// whole batch, M, K <= 128, B FP32 with unit stride along n (in runs of at
+// least a warp unit's columns), no split K, every offset below 2^31.
+bool try_leftmul(const GemmArgs &a, cudaStream_t s, cudaError_t *err) {
+    if (a.b_bf16 || a.ksplit != 1 || a.M > 128 || a.K > 128) return false;
+    if (a.batch > 1 && !(one_level(a.abat) && a.abat.s0 == 0)) return false;
+    if (a.a_n >= (1ll << 31) || a.b_n >= (1ll << 31) || a.c_n >= (1ll << 31)) return false;
+    const int mt = (a.M + 15) / 16, kt = (a.K + 15) / 16;
+    const int nt = left_nt(mt, a.batch, a.N);
+    if (a.bn.s0 != 1 || (!one_level(a.bn) && a.bn.g % (8 * nt) != 0)) return false;
+    // 64-bit stores of column pairs: unit stride along n in runs of even
+    // length, even strides elsewhere, 8-byte aligned outputs
+    const bool pair = a.cn.s0 == 1 && (one_level(a.cn) || (a.cn.g % 2 == 0 && a.cn.s1 % 2 == 0)) &&
+                      even_map(a.cm) && (a.batch == 1 || even_map(a.cbat)) && aligned8(a.C) &&
+                      (!a.C2 || aligned8(a.C2));
+    LeftKern k = left_kernel(mt, nt);
+    const size_t smem = (size_t)16 * mt * (16 * kt + 8) * sizeof(__nv_bfloat16);
+    int dev = 0, nsm = 0, occ = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 256, smem)) != cudaSuccess) {
+        *err = e;
+        return true;
+    }
+    const long long units = (long long)a.batch * ((a.N + 8 * nt - 1) / (8 * nt));
+    const long long blocks = std::min((units + 7) / 8, (long long)nsm * std::max(occ, 1));
+    k<<<(unsigned)blocks, 256, smem, s>>>(a, pair ? 1 : 0);
+    *err = cudaGetLastError();
+    return true;
+}
+
+}  // namespace
+
 cudaError_t gemm(const GemmArgs &a, cudaStream_t s) {
     if (a.M <= 0 || a.N <= 0 || a.K <= 0 || a.batch <= 0) return cudaSuccess;
     // every access in bounds: largest offset of each operand below its size
@@ -268,6 +673,8 @@ cudaError_t gemm(const GemmArgs &a, cudaStream_t s) {
         return cudaErrorInvalidValue;
     const long long gy = (a.M + BM - 1) / BM, gz = (long long)a.batch * a.ksplit;
     if (gy > 65535 || gz > 65535) return cudaErrorInvalidValue;
+    cudaError_t rerr = cudaSuccess;
+    if (try_rowwise(a, s, &rerr) || try_leftmul(a, s, &rerr)) return rerr;
     dim3 grid((a.N + BN - 1) / BN, (unsigned)gy, (unsigned)gz);
     // lanes along the operand's unit-stride index: k where it has one, else
     // the row index (m of A, n of B)

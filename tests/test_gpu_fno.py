@@ -22,11 +22,27 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
+# Kernel by case: the row-streaming one (A with unit stride along k, K in 16,
+# 32, 64, 128, N <= 128) for the first four and (24, 32, 64), (1000, 32, 64),
+# (16, 8, 16): partial 16-row tiles, odd C rows (single-element stores),
+# batches; the small-left-matrix one (one A, M, K <= 128, B with unit stride
+# along n) for the last four: M = 9..128, K = 5..128 (partial K steps), odd N;
+# the tiled one for the rest (K = 112 and 200, transposed batched A, K = 1000)
 @pytest.mark.parametrize("M,N,K,batch,ta,tb", [(64, 64, 32, 1, False, False),
+                                               (37, 5, 128, 2, False, False),
+                                               (300, 128, 32, 1, False, False),
+                                               (45, 17, 16, 3, False, False),
                                                (37, 91, 200, 3, False, False),
                                                (130, 70, 48, 2, True, False),
+                                               (1, 5, 1000, 1, True, True),
                                                (24, 32, 64, 5, False, True),
-                                               (1, 5, 1000, 1, True, True)])
+                                               (1000, 32, 64, 1, False, True),
+                                               (16, 8, 16, 1, False, False),
+                                               (17, 9, 112, 1, False, False),
+                                               (100, 300, 40, 1, True, False),
+                                               (24, 1000, 64, 1, True, False),
+                                               (128, 77, 128, 1, True, False),
+                                               (9, 33, 5, 1, True, False)])
 def test_gemm_matches_float64_products_of_bf16_operands(M, N, K, batch, ta, tb):
     import torch
     g = torch.Generator().manual_seed(M * N + K)
@@ -42,25 +58,31 @@ def test_gemm_matches_float64_products_of_bf16_operands(M, N, K, batch, ta, tb):
     assert err < 1e-5, err
 
 
-def make(seed=3, max_batch=2):
-    return fno.FNO(SMALL["nx"], SMALL["ny"], SMALL["nz"], SMALL["in_channels"],
-                   SMALL["out_channels"], width=SMALL["width"], layers=SMALL["layers"],
-                   modes=(SMALL["modes_x"], SMALL["modes_y"], SMALL["modes_z"]),
-                   hidden=SMALL["hidden"], max_batch=max_batch, seed=seed)
+# width 16, hidden 32: the pointwise layers, the projection and their input
+# gradients run on the row-streaming kernel (bias, GELU second output)
+WIDE = dict(SMALL, width=16, hidden=32)
 
 
-def data(seed, batch=2):
+def make(seed=3, max_batch=2, cfg=SMALL):
+    return fno.FNO(cfg["nx"], cfg["ny"], cfg["nz"], cfg["in_channels"],
+                   cfg["out_channels"], width=cfg["width"], layers=cfg["layers"],
+                   modes=(cfg["modes_x"], cfg["modes_y"], cfg["modes_z"]),
+                   hidden=cfg["hidden"], max_batch=max_batch, seed=seed)
+
+
+def data(seed, batch=2, cfg=SMALL):
     rng = np.random.default_rng(seed)
-    sh = (batch, SMALL["nz"], SMALL["ny"], SMALL["nx"])
-    a = rng.standard_normal(sh + (SMALL["in_channels"],)).astype(np.float32)
+    sh = (batch, cfg["nz"], cfg["ny"], cfg["nx"])
+    a = rng.standard_normal(sh + (cfg["in_channels"],)).astype(np.float32)
     t = rng.standard_normal(sh + (SMALL["out_channels"],)).astype(np.float32)
     return a, t
 
 
-def test_forward_and_gradients_match_the_oracle():
+@pytest.mark.parametrize("cfg", [SMALL, WIDE], ids=["width8", "width16"])
+def test_forward_and_gradients_match_the_oracle(cfg):
     import torch
-    a, t = data(1)
-    with make() as net:
+    a, t = data(1, cfg=cfg)
+    with make(cfg=cfg) as net:
         p = net.params()
         # larger spectral weights than the initialisation, so that the
         # spectral path carries a share of the output comparable to the rest
@@ -70,7 +92,7 @@ def test_forward_and_gradients_match_the_oracle():
         u = net.forward(torch.tensor(a).cuda()).cpu().numpy()
         loss = net.backward(torch.tensor(a).cuda(), torch.tensor(t).cuda())
         g = net.grads()
-    lref, gref, uref = F.loss_and_grads(p, a, t, SMALL)
+    lref, gref, uref = F.loss_and_grads(p, a, t, cfg)
     assert rel(u, uref) < 2e-2, rel(u, uref)
     assert loss == pytest.approx(lref, rel=2e-2)
     assert rel(g, gref) < 5e-2, rel(g, gref)
