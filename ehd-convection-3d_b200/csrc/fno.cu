@@ -1,6 +1,8 @@
 // fno.cu -- the Fourier neural operator of include/ehd_fno.h: parameters,
-// forward pass, backward pass and Adam, every contraction on the BF16 tensor
-// cores through the batched product of gemm_bf16.cu.
+// forward pass, backward pass and Adam.  The pointwise layers, the truncated
+// DFTs and their adjoints run on the BF16 tensor cores through the products
+// of gemm_bf16.cu; the per-mode mixing (a batch of matrix-vector products,
+// one per kept mode) runs in FP32 on the complex weights.
 //
 // Layouts.  Activations are channels-last, v[b][z][y][x][c] (W channels).
 // The spectral convolution of a layer runs as three truncated DFTs, each a
@@ -10,8 +12,8 @@
 //   Yh[b][ri][z][ky][kx][c]    after the transform along y (2 my modes)
 //   Zh[b][ri][kz][ky][kx][c]   after the transform along z (2 mz modes)
 // ri is 0 for the real, 1 for the imaginary part.  The mode mixing multiplies,
-// per mode, the 2W x 2W real form [[Re R, -Im R], [Im R, Re R]] of R with the
-// (Re, Im) column of every sample.  The inverse transforms mirror the forward
+// per mode, the complex W x W matrix R with every sample's complex channel
+// vector (conj(R)^T in the adjoint).  The inverse transforms mirror the forward
 // ones, ending with the real inverse along x (factor 2 on kx > 0) and the
 // 1 / (NX NY NZ) normalisation.  The backward pass applies the transposed
 // matrices in the reverse order.
@@ -46,35 +48,111 @@ __global__ void cast_bf16_kernel(const float *__restrict__ src, __nv_bfloat16 *_
         dst[i] = __float2bfloat16_rn(src[i]);
 }
 
-// real form [[Re, -Im], [Im, Re]] of R per mode, W x W blocks -> 2W x 2W: one
-// thread per (mode, o, c) reads Re and Im once and writes the four entries
-// (modes W^2 < 2^32: 32-bit index arithmetic)
-__global__ void build_block_kernel(const float *__restrict__ re, const float *__restrict__ im,
-                                   __nv_bfloat16 *__restrict__ blk, int modes, int W) {
-    const unsigned n = (unsigned)modes * W * W, w = (unsigned)W, w2 = 2u * W;
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const unsigned c = i % w, t = i / w, o = t % w, md = t / w;
-        const __nv_bfloat16 r = __float2bfloat16_rn(re[i]), m = __float2bfloat16_rn(im[i]);
-        __nv_bfloat16 *b = blk + (size_t)md * 4 * w * w;
-        b[o * w2 + c] = r;
-        b[o * w2 + w + c] = __hneg(m);
-        b[(w + o) * w2 + c] = m;
-        b[(w + o) * w2 + w + c] = r;
+// Mode mixing.  Per kept mode md, the complex W x W weight R[md] (FP32 Re and
+// Im, [out][in]) acts on every sample's complex channel vector, with the
+// real and imaginary parts at Zh[b][ri][md][c]:
+//   out[b][md][o] = sum_i R[md][o][i] in[b][md][i]            (adj = 0)
+//   out[b][md][i] = sum_o conj(R[md][o][i]) in[b][md][o]      (adj = 1)
+// A mode is W^2 weights against a batch of samples: a weight-streaming
+// batch of matrix-vector products, so it runs on the FP32 pipes, not the
+// tensor cores.  One warp per mode: R staged in shared memory with rows
+// padded to W + 1 (transposed for adj, so that lane = output channel reads
+// a row without bank conflicts), inputs of up to 4 samples staged beside it.
+__host__ __device__ inline size_t mix_warp_floats(int W) {
+    return (size_t)2 * W * (W + 1) + (size_t)8 * W;
+}
+
+__global__ void mix_kernel(const float *__restrict__ re, const float *__restrict__ im,
+                           const float *__restrict__ in, float *__restrict__ out, int modes, int W,
+                           int B, int adj) {
+    extern __shared__ float mix_smem[];
+    const int nw = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int WP = W + 1;
+    float *Rr = mix_smem + (size_t)warp * mix_warp_floats(W);
+    float *Ri = Rr + (size_t)W * WP;
+    float *X = Ri + (size_t)W * WP;  // [4 samples][re, im][W]
+    const size_t plane = (size_t)modes * W, WW = (size_t)W * W;
+    for (int md = blockIdx.x * nw + warp; md < modes; md += gridDim.x * nw) {
+        const float *pr = re + (size_t)md * WW, *pi = im + (size_t)md * WW;
+        __syncwarp();
+        for (int t = lane; t < W * W; t += 32) {
+            const int o = t / W, i = t - o * W;
+            const int r = adj ? i : o, c = adj ? o : i;
+            Rr[r * WP + c] = __ldg(pr + t);
+            Ri[r * WP + c] = adj ? -__ldg(pi + t) : __ldg(pi + t);
+        }
+        for (int b0 = 0; b0 < B; b0 += 4) {
+            const int nb = min(4, B - b0);
+            __syncwarp();
+            for (int t = lane; t < nb * 2 * W; t += 32) {
+                const int bb = t / (2 * W), rem = t - bb * 2 * W, ri = rem / W, c = rem - ri * W;
+                X[t] = __ldg(in + (size_t)(b0 + bb) * 2 * plane + ri * plane + (size_t)md * W + c);
+            }
+            __syncwarp();
+            for (int o = lane; o < W; o += 32) {
+                float ar[4] = {0.f, 0.f, 0.f, 0.f}, ai[4] = {0.f, 0.f, 0.f, 0.f};
+                const float *rr = Rr + o * WP, *rm = Ri + o * WP;
+                for (int i = 0; i < W; ++i) {
+                    const float r = rr[i], m = rm[i];
+#pragma unroll
+                    for (int bb = 0; bb < 4; ++bb) {
+                        const float xr = X[bb * 2 * W + i], xi = X[bb * 2 * W + W + i];
+                        ar[bb] = fmaf(r, xr, fmaf(-m, xi, ar[bb]));
+                        ai[bb] = fmaf(r, xi, fmaf(m, xr, ai[bb]));
+                    }
+                }
+#pragma unroll
+                for (int bb = 0; bb < 4; ++bb) {
+                    if (bb >= nb) break;
+                    float *po = out + (size_t)(b0 + bb) * 2 * plane + (size_t)md * W + o;
+                    po[0] = ar[bb];
+                    po[plane] = ai[bb];
+                }
+            }
+        }
     }
 }
 
-// gradient of R from the gradient of its real form
-__global__ void fold_block_kernel(const float *__restrict__ g, float *__restrict__ gre,
-                                  float *__restrict__ gim, int modes, int W) {
-    const size_t n = (size_t)modes * W * W;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-         i += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(i % W), o = (int)((i / W) % W);
-        const size_t md = i / ((size_t)W * W);
-        const float *b = g + md * 4 * W * W;
-        const int w2 = 2 * W;
-        gre[i] += b[o * w2 + c] + b[(W + o) * w2 + W + c];
-        gim[i] += b[(W + o) * w2 + c] - b[o * w2 + W + c];
+// Gradient of R from the mixing's output gradient dout and its input x
+// (both Zh layout), added to gRe, gIm ([mode][out][in]):
+//   gRe[o][i] += sum_b dout_re[o] x_re[i] + dout_im[o] x_im[i]
+//   gIm[o][i] += sum_b dout_im[o] x_re[i] - dout_re[o] x_im[i]
+// One warp per mode, both vectors of up to 4 samples staged in shared
+// memory, lanes along i (coalesced read-modify-write of the gradient rows).
+__global__ void mix_wgrad_kernel(const float *__restrict__ dout, const float *__restrict__ x,
+                                 float *__restrict__ gre, float *__restrict__ gim, int modes,
+                                 int W, int B) {
+    extern __shared__ float mix_smem[];
+    const int nw = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float *D = mix_smem + (size_t)warp * 16 * W;  // [4][re, im][W]
+    float *X = D + 8 * W;
+    const size_t plane = (size_t)modes * W, WW = (size_t)W * W;
+    for (int md = blockIdx.x * nw + warp; md < modes; md += gridDim.x * nw) {
+        float *gr = gre + (size_t)md * WW, *gm = gim + (size_t)md * WW;
+        for (int b0 = 0; b0 < B; b0 += 4) {
+            const int nb = min(4, B - b0);
+            __syncwarp();
+            for (int t = lane; t < 8 * W; t += 32) {
+                const int bb = t / (2 * W), rem = t - bb * 2 * W, ri = rem / W, c = rem - ri * W;
+                const size_t o = (size_t)(b0 + bb) * 2 * plane + ri * plane + (size_t)md * W + c;
+                D[t] = bb < nb ? __ldg(dout + o) : 0.f;
+                X[t] = bb < nb ? __ldg(x + o) : 0.f;
+            }
+            __syncwarp();
+            for (int t = lane; t < W * W; t += 32) {
+                const int o = t / W, i = t - o * W;
+                float sr = 0.f, sm = 0.f;
+#pragma unroll
+                for (int bb = 0; bb < 4; ++bb) {
+                    const float dr = D[bb * 2 * W + o], di = D[bb * 2 * W + W + o];
+                    const float xr = X[bb * 2 * W + i], xi = X[bb * 2 * W + W + i];
+                    sr = fmaf(dr, xr, fmaf(di, xi, sr));
+                    sm = fmaf(di, xr, fmaf(-dr, xi, sm));
+                }
+                gr[t] += sr;
+                gm[t] += sm;
+            }
+        }
     }
 }
 
@@ -136,8 +214,6 @@ struct ehd_fno {
     std::vector<void *> allocs;
     float *param = nullptr, *grad = nullptr, *adam_m = nullptr, *adam_v = nullptr;
     __nv_bfloat16 *pbf = nullptr;                 // BF16 copy of every parameter
-    std::vector<__nv_bfloat16 *> blk;             // per layer: [modes][2W][2W]
-    float *dblk = nullptr;                        // gradient of one layer's blocks
     __nv_bfloat16 *Fx = nullptr, *Fy = nullptr, *Fz = nullptr, *Gx = nullptr, *Gy = nullptr,
                   *Gz = nullptr;
     float *one = nullptr;
@@ -245,9 +321,8 @@ cudaError_t make_dft(ehd_fno *f) {
     return cudaSuccess;
 }
 
-// BF16 copies of the parameters and the layers' block matrices.  The products
-// read the spectral weights only through the block matrices, so only the
-// parameters between the layers' (Re R, Im R) ranges are cast.
+// BF16 copies of the parameters the products read: every parameter but the
+// spectral weights, which the mode mixing reads in FP32.
 cudaError_t refresh(ehd_fno *f) {
     const size_t spec = (size_t)f->modes * f->W * f->W;
     size_t from = 0;
@@ -256,11 +331,7 @@ cudaError_t refresh(ehd_fno *f) {
         if (to > from)
             cast_bf16_kernel<<<grid_for(to - from), 256, 0, f->stream>>>(f->param + from,
                                                                          f->pbf + from, to - from);
-        if (l < f->L) {
-            build_block_kernel<<<grid_for(spec), 256, 0, f->stream>>>(
-                f->param + f->lo[l].Rre, f->param + f->lo[l].Rim, f->blk[l], f->modes, f->W);
-            from = f->lo[l].Rim + spec;
-        }
+        if (l < f->L) from = f->lo[l].Rim + spec;
     }
     return cudaGetLastError();
 }
@@ -548,60 +619,27 @@ GemmArgs z_inv(const Dims &d, const __nv_bfloat16 *G, const float *zh, float *yh
     return g;
 }
 
-// per mode: out[(ro,o)][b] = blk[(ro,o)][(ri,i)] in[(ri,i)][b]; tr: blk^T
-GemmArgs mix(const Dims &d, const __nv_bfloat16 *blk, const float *in, float *out, bool tr) {
-    GemmArgs g;
-    g.M = (int)(2 * d.W);
-    g.K = (int)(2 * d.W);
-    g.N = (int)d.B;
-    g.batch = (int)d.Mo;
-    g.A = blk;
-    g.a_bf16 = 1;
-    if (tr) {
-        g.am = lin(1);
-        g.ak = lin(2 * d.W);
-    } else {
-        g.am = lin(2 * d.W);
-        g.ak = lin(1);
-    }
-    g.abat = lin(4 * d.W * d.W);
-    g.B = in;
-    g.bk = two(1, (int)d.W, d.Mo * d.W);
-    g.bn = lin(2 * d.Mo * d.W);
-    g.bbat = lin(d.W);
-    g.C = out;
-    g.cm = two(1, (int)d.W, d.Mo * d.W);
-    g.cn = lin(2 * d.Mo * d.W);
-    g.cbat = lin(d.W);
-    g.a_n = d.Mo * 4 * d.W * d.W;
-    g.b_n = d.nzh();
-    g.c_n = d.nzh();
-    return g;
+// launches of the mixing kernels: warps per block by the shared memory a
+// warp needs (at most 48 KB a block)
+int mix_warps(int W, size_t per_warp_floats) {
+    const size_t per = per_warp_floats * sizeof(float);
+    return (int)std::max<size_t>(1, std::min<size_t>(8, (48u << 10) / per));
 }
 
-// per mode: dblk[(ro,o)][(ri,i)] = sum_b dout[(ro,o)][b] in[(ri,i)][b]
-GemmArgs mix_wgrad(const Dims &d, const float *dout, const float *in, float *dblk) {
-    GemmArgs g;
-    g.M = (int)(2 * d.W);
-    g.N = (int)(2 * d.W);
-    g.K = (int)d.B;
-    g.batch = (int)d.Mo;
-    g.A = dout;
-    g.am = two(1, (int)d.W, d.Mo * d.W);
-    g.ak = lin(2 * d.Mo * d.W);
-    g.abat = lin(d.W);
-    g.B = in;
-    g.bk = lin(2 * d.Mo * d.W);
-    g.bn = two(1, (int)d.W, d.Mo * d.W);
-    g.bbat = lin(d.W);
-    g.C = dblk;
-    g.cm = lin(2 * d.W);
-    g.cn = lin(1);
-    g.cbat = lin(4 * d.W * d.W);
-    g.a_n = d.nzh();
-    g.b_n = d.nzh();
-    g.c_n = d.Mo * 4 * d.W * d.W;
-    return g;
+cudaError_t mix(const ehd_fno *f, int l, const float *in, float *out, int B, bool adj) {
+    const int nw = mix_warps(f->W, mix_warp_floats(f->W));
+    const unsigned blocks = (unsigned)std::min<size_t>((f->modes + nw - 1) / nw, 148 * 16);
+    mix_kernel<<<blocks, 32 * nw, nw * mix_warp_floats(f->W) * sizeof(float), f->stream>>>(
+        f->param + f->lo[l].Rre, f->param + f->lo[l].Rim, in, out, f->modes, f->W, B, adj ? 1 : 0);
+    return cudaGetLastError();
+}
+
+cudaError_t mix_wgrad(const ehd_fno *f, int l, const float *dout, const float *x, float *g, int B) {
+    const int nw = mix_warps(f->W, (size_t)16 * f->W);
+    const unsigned blocks = (unsigned)std::min<size_t>((f->modes + nw - 1) / nw, 148 * 16);
+    mix_wgrad_kernel<<<blocks, 32 * nw, (size_t)nw * 16 * f->W * sizeof(float), f->stream>>>(
+        dout, x, g + f->lo[l].Rre, g + f->lo[l].Rim, f->modes, f->W, B);
+    return cudaGetLastError();
 }
 
 Dims dims(const ehd_fno *f, int B) {
@@ -628,7 +666,7 @@ int forward(ehd_fno *f, int B, const float *a) {
         FNO_CK(gemm(x_fwd(d, f->Fx, f->v[l], f->xh, false), s));
         FNO_CK(gemm(y_fwd(d, f->Fy, f->xh, f->yh, false), s));
         FNO_CK(gemm(z_fwd(d, f->Fz, f->yh, f->zh[l], false), s));
-        FNO_CK(gemm(mix(d, f->blk[l], f->zh[l], f->mh, false), s));
+        FNO_CK(mix(f, l, f->zh[l], f->mh, B, false));
         FNO_CK(gemm(z_inv(d, f->Gz, f->mh, f->yh, false), s));
         FNO_CK(gemm(y_inv(d, f->Gy, f->yh, f->xh, false), s));
         GemmArgs g = x_inv(d, f->Gx, f->xh, zl, 1.f, false);
@@ -745,7 +783,6 @@ int ehd_fno_create(const ehd_fno_config *cfg, ehd_fno **out) {
     if ((e = alloc(f, &f->param, n)) != cudaSuccess || (e = alloc(f, &f->grad, n)) != cudaSuccess ||
         (e = alloc(f, &f->adam_m, n)) != cudaSuccess || (e = alloc(f, &f->adam_v, n)) != cudaSuccess ||
         (e = alloc(f, &f->pbf, n)) != cudaSuccess ||
-        (e = alloc(f, &f->dblk, (size_t)f->modes * 4 * WW)) != cudaSuccess ||
         (e = alloc(f, &f->one, 1)) != cudaSuccess || (e = alloc(f, &f->lsum, 1)) != cudaSuccess ||
         (e = alloc(f, &f->xh, nxh)) != cudaSuccess || (e = alloc(f, &f->yh, nyh)) != cudaSuccess ||
         (e = alloc(f, &f->mh, nzh)) != cudaSuccess || (e = alloc(f, &f->hpre, rows * H)) != cudaSuccess ||
@@ -758,11 +795,9 @@ int ehd_fno_create(const ehd_fno_config *cfg, ehd_fno **out) {
     f->v.assign(f->L + 1, nullptr);
     f->z.assign(f->L, nullptr);
     f->zh.assign(f->L, nullptr);
-    f->blk.assign(f->L, nullptr);
     for (int l = 0; l < f->L; ++l) {
         if ((e = alloc(f, &f->z[l], rows * W)) != cudaSuccess ||
-            (e = alloc(f, &f->zh[l], nzh)) != cudaSuccess ||
-            (e = alloc(f, &f->blk[l], (size_t)f->modes * 4 * WW)) != cudaSuccess)
+            (e = alloc(f, &f->zh[l], nzh)) != cudaSuccess)
             return bail(cuda_fail("ehd_fno_create allocation", e));
     }
     for (int l = 0; l < f->L; ++l)  // v[L] is z[L-1] (no activation after the last layer)
@@ -873,11 +908,8 @@ int ehd_fno_backward(ehd_fno *f, int B, const float *a, const float *target, dou
         FNO_CK(gemm(x_fwd(d, f->Gx, dz, f->xh, true), s));
         FNO_CK(gemm(y_fwd(d, f->Gy, f->xh, f->yh, true), s));
         FNO_CK(gemm(z_fwd(d, f->Gz, f->yh, f->mh, true), s));
-        FNO_CK(gemm(mix_wgrad(d, f->mh, f->zh[l], f->dblk), s));
-        fold_block_kernel<<<grid_for((size_t)f->modes * f->W * f->W), 256, 0, s>>>(
-            f->dblk, g + o.Rre, g + o.Rim, f->modes, f->W);
-        FNO_CK(cudaGetLastError());
-        FNO_CK(gemm(mix(d, f->blk[l], f->mh, f->zh[l], true), s));  // zh[l] is free now
+        FNO_CK(mix_wgrad(f, l, f->mh, f->zh[l], g, B));
+        FNO_CK(mix(f, l, f->mh, f->zh[l], B, true));  // zh[l] is free now
         FNO_CK(gemm(z_inv(d, f->Fz, f->zh[l], f->yh, true), s));
         FNO_CK(gemm(y_inv(d, f->Fy, f->yh, f->xh, true), s));
         FNO_CK(gemm(x_inv(d, f->Fx, f->xh, f->dv2, 1.f, true), s));

@@ -12,10 +12,11 @@
  * kx = 0..mx-1 of a real transform along x and the mx_y, mx_z lowest
  * positive and negative modes along y and z; R_l is a complex
  * width x width matrix per kept mode.  Transforms are truncated DFTs carried
- * out as matrix products, so every contraction -- lift, pointwise layers,
- * transforms, mode mixing, projection and all of their adjoints -- runs on
- * the BF16 tensor cores with FP32 accumulation.  Weights are kept in FP32
- * (the optimizer's copy) and read by the kernels as BF16.
+ * out as matrix products, so the lift, pointwise layers, transforms,
+ * projection and all of their adjoints run on the BF16 tensor cores with
+ * FP32 accumulation, the weights read as BF16 copies of the FP32 ones (the
+ * optimizer's).  The mode mixing -- per kept mode a matrix-vector product
+ * for each sample, weight-bound -- runs in FP32 on the FP32 weights.
  *
  * Fields are channels-last FP32 device arrays [batch][z][y][x][channel]. */
 #ifndef EHD_FNO_H
