@@ -216,7 +216,6 @@ struct ehd_fno {
     __nv_bfloat16 *pbf = nullptr;                 // BF16 copy of every parameter
     __nv_bfloat16 *Fx = nullptr, *Fy = nullptr, *Fz = nullptr, *Gx = nullptr, *Gy = nullptr,
                   *Gz = nullptr;
-    float *one = nullptr;
     double *lsum = nullptr;
     // activations for max_batch samples
     std::vector<float *> v, z, zh;                // v[0..L], z[0..L-1], zh[0..L-1]
@@ -360,38 +359,6 @@ GemmArgs pointwise(size_t rows, int K, int N, const float *A, const __nv_bfloat1
     g.a_n = (long long)rows * K;
     g.b_n = (long long)K * N;
     g.c_n = (long long)rows * N;
-    return g;
-}
-
-// gradient of a pointwise layer's weight: G[K][N] += X^T[K][rows] D[rows][N]
-GemmArgs weight_grad(size_t rows, int K, int N, const float *Xs, const float *D, float *G) {
-    GemmArgs g;
-    g.M = K;
-    g.N = N;
-    g.K = (int)rows;
-    g.A = Xs;
-    g.am = lin(1);
-    g.ak = lin(K);
-    g.B = D;
-    g.bk = lin(N);
-    g.bn = lin(1);
-    g.C = G;
-    g.cm = lin(N);
-    g.cn = lin(1);
-    g.beta = 1.f;
-    g.ksplit = (int)std::min<size_t>(2048, std::max<size_t>(1, rows / 1024));
-    g.a_n = (long long)rows * K;
-    g.b_n = (long long)rows * N;
-    g.c_n = (long long)K * N;
-    return g;
-}
-
-// bias gradient: G[N] += sum over rows of D[rows][N]
-GemmArgs bias_grad(size_t rows, int N, const float *one, const float *D, float *G) {
-    GemmArgs g = weight_grad(rows, 1, N, one, D, G);
-    g.am = lin(0);
-    g.ak = lin(0);
-    g.a_n = 1;
     return g;
 }
 
@@ -783,7 +750,7 @@ int ehd_fno_create(const ehd_fno_config *cfg, ehd_fno **out) {
     if ((e = alloc(f, &f->param, n)) != cudaSuccess || (e = alloc(f, &f->grad, n)) != cudaSuccess ||
         (e = alloc(f, &f->adam_m, n)) != cudaSuccess || (e = alloc(f, &f->adam_v, n)) != cudaSuccess ||
         (e = alloc(f, &f->pbf, n)) != cudaSuccess ||
-        (e = alloc(f, &f->one, 1)) != cudaSuccess || (e = alloc(f, &f->lsum, 1)) != cudaSuccess ||
+        (e = alloc(f, &f->lsum, 1)) != cudaSuccess ||
         (e = alloc(f, &f->xh, nxh)) != cudaSuccess || (e = alloc(f, &f->yh, nyh)) != cudaSuccess ||
         (e = alloc(f, &f->mh, nzh)) != cudaSuccess || (e = alloc(f, &f->hpre, rows * H)) != cudaSuccess ||
         (e = alloc(f, &f->h, rows * H)) != cudaSuccess ||
@@ -804,9 +771,7 @@ int ehd_fno_create(const ehd_fno_config *cfg, ehd_fno **out) {
         if ((e = alloc(f, &f->v[l], rows * W)) != cudaSuccess)
             return bail(cuda_fail("ehd_fno_create allocation", e));
     f->v[f->L] = f->z[f->L - 1];
-    const float one = 1.f;
     if ((e = cudaMemcpy(f->param, h.data(), n * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemcpy(f->one, &one, sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = make_dft(f)) != cudaSuccess || (e = refresh(f)) != cudaSuccess ||
         (e = cudaStreamSynchronize(f->stream)) != cudaSuccess)
         return bail(cuda_fail("ehd_fno_create set-up", e));
@@ -884,14 +849,14 @@ int ehd_fno_backward(ehd_fno *f, int B, const float *a, const float *target, dou
     mse_kernel<<<grid_for(nout), 256, 0, s>>>(f->u, target, f->du, nout, f->lsum);
     FNO_CK(cudaGetLastError());
     // projection
-    FNO_CK(gemm(weight_grad(rows, f->H, f->cout, f->h, f->du, g + f->oQ2), s));
-    FNO_CK(gemm(bias_grad(rows, f->cout, f->one, f->du, g + f->oq2), s));
+    FNO_CK(weight_bias_grad((long long)rows, f->H, f->cout, f->h, f->H, f->du, f->cout,
+                            g + f->oQ2, f->cout, g + f->oq2, s));
     FNO_CK(gemm(input_grad(rows, f->H, f->cout, f->du, pb + f->oQ2, f->dh, 0.f), s));
     gelu_back_kernel<<<grid_for(rows * f->H), 256, 0, s>>>(f->dh, f->hpre, rows * f->H);
     FNO_CK(cudaGetLastError());
     const float *vL = f->z[f->L - 1];
-    FNO_CK(gemm(weight_grad(rows, f->W, f->H, vL, f->dh, g + f->oQ1), s));
-    FNO_CK(gemm(bias_grad(rows, f->H, f->one, f->dh, g + f->oq1), s));
+    FNO_CK(weight_bias_grad((long long)rows, f->W, f->H, vL, f->W, f->dh, f->H, g + f->oQ1, f->H,
+                            g + f->oq1, s));
     FNO_CK(gemm(input_grad(rows, f->W, f->H, f->dh, pb + f->oQ1, f->dv, 0.f), s));
     // Fourier layers: f->dv holds the gradient of v[l+1]
     for (int l = f->L - 1; l >= 0; --l) {
@@ -901,8 +866,8 @@ int ehd_fno_backward(ehd_fno *f, int B, const float *a, const float *target, dou
             FNO_CK(cudaGetLastError());
         }
         const Off &o = f->lo[l];
-        FNO_CK(gemm(weight_grad(rows, f->W, f->W, f->v[l], dz, g + o.W), s));
-        FNO_CK(gemm(bias_grad(rows, f->W, f->one, dz, g + o.b), s));
+        FNO_CK(weight_bias_grad((long long)rows, f->W, f->W, f->v[l], f->W, dz, f->W, g + o.W,
+                                f->W, g + o.b, s));
         FNO_CK(gemm(input_grad(rows, f->W, f->W, dz, pb + o.W, f->dv2, 0.f), s));
         // adjoint of the spectral convolution
         FNO_CK(gemm(x_fwd(d, f->Gx, dz, f->xh, true), s));
@@ -916,8 +881,8 @@ int ehd_fno_backward(ehd_fno *f, int B, const float *a, const float *target, dou
         std::swap(f->dv, f->dv2);
     }
     // lift
-    FNO_CK(gemm(weight_grad(rows, f->cin, f->W, a, f->dv, g + f->oP), s));
-    FNO_CK(gemm(bias_grad(rows, f->W, f->one, f->dv, g + f->op), s));
+    FNO_CK(weight_bias_grad((long long)rows, f->cin, f->W, a, f->cin, f->dv, f->W, g + f->oP, f->W,
+                            g + f->op, s));
     if (loss) {
         double sum = 0.0;
         FNO_CK(cudaMemcpyAsync(&sum, f->lsum, sizeof(double), cudaMemcpyDeviceToHost, s));

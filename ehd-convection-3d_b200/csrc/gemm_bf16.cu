@@ -496,6 +496,117 @@ __global__ void __launch_bounds__(256) leftmul_kernel(const GemmArgs a, int pair
     }
 }
 
+// ---- parameter gradients of pointwise layers ------------------------------
+//
+// G[m][n] += sum_r X[r][m] D[r][n] and gb[n] += sum_r D[r][n] over all rows r
+// (X rows ldx apart, D rows ldd apart, M <= 16 MT, N <= 8 NT): the weight and
+// bias gradients of a pointwise layer in one pass over X and D.  Each warp
+// takes 16-row chunks; its mma.sync fragments come straight from global
+// memory (lanes along the channel: every load reads four fully used 32-byte
+// sectors), the bias sums are taken in FP32 from the same D values before
+// they are rounded to BF16; the block reduces its warps' partial sums in
+// shared memory and adds them to G and gb atomically.
+template <int MT, int NT>
+__global__ void __launch_bounds__(256) wgrad_kernel(const float *__restrict__ X, int ldx, int M,
+                                                    const float *__restrict__ D, int ldd, int N,
+                                                    long long rows, float *__restrict__ G,
+                                                    int ldg, float *__restrict__ gb) {
+    constexpr int NV = MT * NT * 128;         // partial sums of G per warp
+    __shared__ float red[4][NV + NT * 8];     // warps w and w + 4 share a row
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int gq = lane >> 2, tq = lane & 3;
+    float acc[MT][NT][4], bs[NT];
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+#pragma unroll
+    for (int j = 0; j < NT; ++j) bs[j] = 0.f;
+    const long long chunks = (rows + 15) / 16;
+    for (long long c = (long long)blockIdx.x * 8 + warp; c < chunks; c += (long long)gridDim.x * 8) {
+        const long long r0 = c * 16 + 2 * tq;
+        // rows r0, r0 + 1, r0 + 8, r0 + 9 of this lane
+        long long rr[4];
+        bool rin[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            rr[e] = r0 + (e & 1) + (e >> 1) * 8;
+            rin[e] = rr[e] < rows;
+        }
+        uint32_t bf[NT][2];
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+            const int n = 8 * j + gq;
+            float v[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                v[e] = (rin[e] && n < N) ? __ldg(D + rr[e] * ldd + n) : 0.f;
+            bs[j] += (v[0] + v[1]) + (v[2] + v[3]);
+            bf[j][0] = pack_bf16(make_float2(v[0], v[1]));
+            bf[j][1] = pack_bf16(make_float2(v[2], v[3]));
+        }
+#pragma unroll
+        for (int i = 0; i < MT; ++i) {
+            const int m0 = 16 * i + gq, m1 = m0 + 8;
+            float x[8];  // (m0, m1) x rows e
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                x[e] = (rin[e] && m0 < M) ? __ldg(X + rr[e] * ldx + m0) : 0.f;
+                x[4 + e] = (rin[e] && m1 < M) ? __ldg(X + rr[e] * ldx + m1) : 0.f;
+            }
+            const uint32_t a0 = pack_bf16(make_float2(x[0], x[1]));
+            const uint32_t a1 = pack_bf16(make_float2(x[4], x[5]));
+            const uint32_t a2 = pack_bf16(make_float2(x[2], x[3]));
+            const uint32_t a3 = pack_bf16(make_float2(x[6], x[7]));
+#pragma unroll
+            for (int j = 0; j < NT; ++j) mma16816(acc[i][j], a0, a1, a2, a3, bf[j][0], bf[j][1]);
+        }
+    }
+    // bias sums of column 8 j + gq: the four lanes of a row group
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+        bs[j] += __shfl_xor_sync(0xffffffffu, bs[j], 1);
+        bs[j] += __shfl_xor_sync(0xffffffffu, bs[j], 2);
+    }
+    // warps 4..7 store their partial sums, warps 0..3 add theirs to them
+    float *my = red[warp & 3];
+    for (int half = 1; half >= 0; --half) {
+        if ((warp >> 2) == half) {
+#pragma unroll
+            for (int i = 0; i < MT; ++i)
+#pragma unroll
+                for (int j = 0; j < NT; ++j)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        float &r = my[((i * NT + j) * 4 + e) * 32 + lane];
+                        r = half ? acc[i][j][e] : r + acc[i][j][e];
+                    }
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+                float &r = my[NV + 8 * j + gq];
+                if (tq == 0) r = half ? bs[j] : r + bs[j];
+            }
+        }
+        __syncthreads();
+    }
+    for (int t = tid; t < NV + NT * 8; t += blockDim.x) {
+        float sum = 0.f;
+#pragma unroll
+        for (int w = 0; w < 4; ++w) sum += red[w][t];
+        if (t < NV) {
+            const int ln = t & 31, f = t >> 5;
+            const int e = f & 3, j = (f >> 2) % NT, i = (f >> 2) / NT;
+            const int m = 16 * i + (ln >> 2) + (e >> 1) * 8, n = 8 * j + (ln & 3) * 2 + (e & 1);
+            if (m < M && n < N) atomicAdd(G + (size_t)m * ldg + n, sum);
+        } else if (gb) {
+            const int n = t - NV;
+            if (n < N) atomicAdd(gb + n, sum);
+        }
+    }
+}
+
 }  // namespace
 
 namespace {
@@ -657,7 +768,51 @@ bool try_leftmul(const GemmArgs &a, cudaStream_t s, cudaError_t *err) {
     return true;
 }
 
+using WgradKern = void (*)(const float *, int, int, const float *, int, int, long long, float *,
+                           int, float *);
+
+template <int MT>
+WgradKern wgrad_kernel_nt(int nt) {
+    switch (nt) {
+        case 1: return wgrad_kernel<MT, 1>;
+        case 2: return wgrad_kernel<MT, (16 / MT >= 2 ? 2 : 1)>;
+        case 4: return wgrad_kernel<MT, (16 / MT >= 4 ? 4 : 1)>;
+        case 8: return wgrad_kernel<MT, (16 / MT >= 8 ? 8 : 1)>;
+        default: return wgrad_kernel<MT, (16 / MT >= 8 ? 8 : 1)>;
+    }
+}
+
 }  // namespace
+
+cudaError_t weight_bias_grad(long long rows, int M, int N, const float *X, int ldx, const float *D,
+                             int ldd, float *G, int ldg, float *gb, cudaStream_t s) {
+    if (rows <= 0 || M <= 0 || N <= 0) return cudaSuccess;
+    if (M > 128 || ldx < M || ldd < N || ldg < N) return cudaErrorInvalidValue;
+    const int mt = M <= 16 ? 1 : M <= 32 ? 2 : M <= 64 ? 4 : 8;
+    const int ntmax = std::min(8, 16 / mt);  // at most 64 accumulators a thread
+    int dev = 0, nsm = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return e;
+    // columns in passes of at most 8 ntmax
+    for (int n0 = 0; n0 < N; n0 += 8 * ntmax) {
+        const int nn = std::min(N - n0, 8 * ntmax);
+        int nt = 1;
+        while (8 * nt < nn) nt *= 2;
+        WgradKern k = mt == 1 ? wgrad_kernel_nt<1>(nt) : mt == 2 ? wgrad_kernel_nt<2>(nt)
+                    : mt == 4 ? wgrad_kernel_nt<4>(nt) : wgrad_kernel_nt<8>(nt);
+        int occ = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 256, 0)) != cudaSuccess)
+            return e;
+        const long long chunks = (rows + 15) / 16;
+        const long long blocks = std::min((chunks + 7) / 8, (long long)nsm * std::max(occ, 1));
+        k<<<(unsigned)blocks, 256, 0, s>>>(X, ldx, M, D + n0, ldd, nn, rows, G + n0, ldg,
+                                          gb ? gb + n0 : nullptr);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
 
 cudaError_t gemm(const GemmArgs &a, cudaStream_t s) {
     if (a.M <= 0 || a.N <= 0 || a.K <= 0 || a.batch <= 0) return cudaSuccess;

@@ -60,5 +60,12 @@ struct GemmArgs {
 
 cudaError_t gemm(const GemmArgs &a, cudaStream_t s);
 
+// G[m][n] += sum_r X[r][m] D[r][n] (BF16 products, FP32 sums) and, unless gb
+// is null, gb[n] += sum_r D[r][n] (FP32), over r < rows: the weight and bias
+// gradients of a pointwise layer in one pass.  M <= 128; X rows ldx apart,
+// D rows ldd apart, G rows ldg apart.
+cudaError_t weight_bias_grad(long long rows, int M, int N, const float *X, int ldx, const float *D,
+                             int ldd, float *G, int ldg, float *gb, cudaStream_t s);
+
 }  // namespace fno
 }  // namespace ehd
