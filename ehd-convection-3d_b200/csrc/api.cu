@@ -853,6 +853,166 @@ int ehd_set_state_seeded(ehd_ctx *c, const double *profile, uint64_t seed, doubl
     return after_upload(c);
 }
 
+int ehd_hydrostatic_column(const ehd_params *params, const ehd_config *config, int nsteps,
+                           ehd_ctx **column, double *i0) {
+    if (!params || !column) return fail(EHD_ERR_INVALID, "NULL argument");
+    if (nsteps < 0) return fail(EHD_ERR_INVALID, "nsteps < 0");
+    *column = nullptr;
+    ehd_params q = *params;
+    q.nx = 1;
+    q.ny = 1;
+    q.lx = params->dx;
+    q.ly = params->dy;
+    ehd_ctx *col = nullptr;
+    int r = ehd_create(&q, config, &col);
+    if (r != EHD_OK) return r;
+    // I0: the mean of the currents after nsteps and nsteps + 1 steps; the
+    // column is left after nsteps + 1
+    ehd_diag d{}, d1{};
+    if ((r = ehd_initialize(col)) == EHD_OK && (r = ehd_step(col, nsteps)) == EHD_OK &&
+        (r = ehd_diagnostics(col, &d)) == EHD_OK && (r = ehd_step(col, 1)) == EHD_OK)
+        r = ehd_diagnostics(col, &d1);
+    if (r != EHD_OK) {
+        ehd_destroy(col);
+        return r;
+    }
+    if (i0) *i0 = 0.5 * (d.current + d1.current) * (double)params->nx * (double)params->ny;
+    *column = col;
+    return EHD_OK;
+}
+
+namespace {
+// every parameter of a column context equal to the context's, but for the
+// plane's extent (nx, ny, lx, ly)
+bool column_matches(const ehd_params &a, const ehd_params &b) {
+    const double x[] = {a.lz, a.dx, a.dy, a.dz, a.dt, a.cfl, a.rho0, a.charge0, a.voltage,
+                        a.eps, a.diffu, a.nu, a.K, a.uw, a.exf, a.lambda_f, a.lambda_g};
+    const double y[] = {b.lz, b.dx, b.dy, b.dz, b.dt, b.cfl, b.rho0, b.charge0, b.voltage,
+                        b.eps, b.diffu, b.nu, b.K, b.uw, b.exf, b.lambda_f, b.lambda_g};
+    if (a.nz != b.nz) return false;
+    for (size_t i = 0; i < sizeof(x) / sizeof(x[0]); ++i)
+        if (x[i] != y[i]) return false;
+    return true;
+}
+
+double read_real(const std::vector<unsigned char> &b, size_t i, size_t size) {
+    if (size == 8) {
+        double v;
+        std::memcpy(&v, b.data() + 8 * i, 8);
+        return v;
+    }
+    float v;
+    std::memcpy(&v, b.data() + 4 * i, 4);
+    return v;
+}
+
+void write_real(std::vector<unsigned char> &b, size_t i, size_t size, double v) {
+    if (size == 8) {
+        std::memcpy(b.data() + 8 * i, &v, 8);
+    } else {
+        const float f = (float)v;
+        std::memcpy(b.data() + 4 * i, &f, 4);
+    }
+}
+}  // namespace
+
+int ehd_set_state_from_column(ehd_ctx *c, ehd_ctx *col, uint64_t seed, double amp) {
+    if (!c || !col) return fail(EHD_ERR_INVALID, "NULL argument");
+    if (!std::isfinite(amp)) return fail(EHD_ERR_INVALID, "amp not finite");
+    if (col->p.nx != 1 || col->p.ny != 1)
+        return fail(EHD_ERR_INVALID, "column: nx and ny must be 1");
+    if (!column_matches(c->p, col->p))
+        return fail(EHD_ERR_INVALID, "column: parameters differ from the context's");
+    if (!col->have_state || col->pops_local || col->e_arrays)
+        return fail(EHD_ERR_STATE, "column: needs a state stepped at least once since its upload");
+    if (col->tsize < 4) return fail(EHD_ERR_INVALID, "column: FP64 or FP32 populations needed");
+    const int nz = c->p.nz;
+    const size_t nzs = (size_t)nz;
+    // the column's fields, population values and tables, on the host
+    std::vector<double> prof(9 * nzs);
+    int r = ehd_get_fields(col, prof.data(), prof.data() + nzs, prof.data() + 2 * nzs,
+                           prof.data() + 3 * nzs, prof.data() + 4 * nzs, prof.data() + 5 * nzs,
+                           prof.data() + 6 * nzs, prof.data() + 7 * nzs, prof.data() + 8 * nzs);
+    if (r != EHD_OK) return r;
+    std::vector<unsigned char> fb(Q * nzs * col->tsize), hb(Q * nzs * col->tsize);
+    std::vector<unsigned char> kt[2] = {std::vector<unsigned char>(10 * nzs * col->rsize),
+                                        std::vector<unsigned char>(10 * nzs * col->rsize)};
+    std::vector<double> wref[2] = {std::vector<double>(2 * nzs), std::vector<double>(2 * nzs)};
+    std::vector<double> mean[2] = {std::vector<double>(2 * nzs), std::vector<double>(2 * nzs)};
+    std::vector<double> phi00(nzs), ez00(nzs);
+    {
+        DeviceGuard dg(col->device);
+        EHD_CK(cudaMemcpy(fb.data(), col->f[col->cur], fb.size(), cudaMemcpyDeviceToHost));
+        EHD_CK(cudaMemcpy(hb.data(), col->h[col->cur], hb.size(), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < 2; ++k) {
+            EHD_CK(cudaMemcpy(kt[k].data(), col->ktab[k], kt[k].size(), cudaMemcpyDeviceToHost));
+            EHD_CK(cudaMemcpy(wref[k].data(), col->wref[k], 16 * nzs, cudaMemcpyDeviceToHost));
+            EHD_CK(cudaMemcpy(mean[k].data(), col->mean[k], 16 * nzs, cudaMemcpyDeviceToHost));
+        }
+        EHD_CK(cudaMemcpy(phi00.data(), col->phi00, 8 * nzs, cudaMemcpyDeviceToHost));
+        EHD_CK(cudaMemcpy(ez00.data(), col->ez00, 8 * nzs, cudaMemcpyDeviceToHost));
+    }
+    // population values: stored deviation + w_d times the plane's reference
+    const std::vector<double> &wc = wref[col->cur];
+    std::vector<double> colv(2 * Q * nzs);
+    for (int d = 0; d < Q; ++d)
+        for (size_t z = 0; z < nzs; ++z) {
+            colv[d * nzs + z] = read_real(fb, d * nzs + z, col->tsize) + w_of(d) * wc[2 * z];
+            colv[(Q + d) * nzs + z] = read_real(hb, d * nzs + z, col->tsize) + w_of(d) * wc[2 * z + 1];
+        }
+    // the step kernel's tables in this context's compute type
+    for (int k = 0; k < 2; ++k) {
+        std::vector<unsigned char> conv(10 * nzs * c->rsize);
+        for (size_t j = 0; j < 10 * nzs; ++j) write_real(conv, j, c->rsize, read_real(kt[k], j, col->rsize));
+        kt[k].swap(conv);
+    }
+    DeviceGuard dg(c->device);
+    EHD_CK(cudaStreamSynchronize(c->stream));
+    double *colv_dev = nullptr;
+    EHD_CK(cudaMalloc((void **)&colv_dev, sizeof(double) * colv.size()));
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+        if ((e = cudaMemcpy(c->wref[k], wref[k].data(), 16 * nzs, cudaMemcpyHostToDevice)) == cudaSuccess &&
+            (e = cudaMemcpy(c->mean[k], mean[k].data(), 16 * nzs, cudaMemcpyHostToDevice)) == cudaSuccess)
+            e = cudaMemcpy(c->ktab[k], kt[k].data(), kt[k].size(), cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpy(colv_dev, colv.data(), sizeof(double) * colv.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(c->phi00, phi00.data(), 8 * nzs, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(c->ez00, ez00.data(), 8 * nzs, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(c->prof_dev, prof.data(), sizeof(double) * prof.size(), cudaMemcpyHostToDevice);
+    c->cur = col->cur;
+    if (e == cudaSuccess) e = launch_seeded_state(c->out_dev, c->prof_dev, (unsigned long long)seed, amp, c->sc, c->stream);
+    if (e == cudaSuccess) {
+        void *f = c->f[c->cur], *h = c->h[c->cur];
+        const double *ref = c->wref[c->cur];
+        switch (c->prec) {
+            case EHD_PREC_FP64: e = launch_column_state<double, double>(f, h, c->out_dev, c->prof_dev, colv_dev, ref, c->phip, c->phi00, c->sc, c->stream); break;
+            case EHD_PREC_FP32: e = launch_column_state<float, float>(f, h, c->out_dev, c->prof_dev, colv_dev, ref, c->phip, c->phi00, c->sc, c->stream); break;
+            case EHD_PREC_FP16: e = launch_column_state<__half, float>(f, h, c->out_dev, c->prof_dev, colv_dev, ref, c->phip, c->phi00, c->sc, c->stream); break;
+            default: e = launch_column_state<__nv_bfloat16, float>(f, h, c->out_dev, c->prof_dev, colv_dev, ref, c->phip, c->phi00, c->sc, c->stream); break;
+        }
+    }
+    if (e == cudaSuccess)
+        e = c->prec == EHD_PREC_FP64
+                ? launch_fields_to_compute<double>(c->out_dev, c->rho, c->u, c->v, c->w, c->q, c->sc.n, c->stream)
+                : launch_fields_to_compute<float>(c->out_dev, c->rho, c->u, c->v, c->w, c->q, c->sc.n, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(colv_dev);
+    if (e != cudaSuccess) {
+        c->have_state = false;
+        return fail(EHD_ERR_CUDA, "state from column: %s", cudaGetErrorString(e));
+    }
+    c->have_state = true;
+    c->pops_local = false;
+    c->e_arrays = false;
+    c->out_valid = false;
+    c->step = 0;
+    c->t = 0.0;
+    return EHD_OK;
+}
+
 int ehd_hydrostatic_profile(const ehd_params *params, const ehd_config *config, int nsteps,
                             double *profile, double *i0) {
     if (!params || !profile) return fail(EHD_ERR_INVALID, "NULL argument");

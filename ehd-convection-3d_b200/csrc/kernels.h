@@ -76,6 +76,16 @@ int lbm_rows_slots_per_plane(int nx, int ny);
 cudaError_t launch_seeded_state(double *const *out_dev, const double *prof_dev,
                                 unsigned long long seed, double amp, const StepConst &c,
                                 cudaStream_t s);
+// Populations of a state broadcast from a 1 x 1 x NZ column's: colv holds the
+// column's population values [(s Q + d) NZ + z] (s = 0: f, 1: g), prof its
+// nine fields [k][z]; out_dev the seeded fields (velocity = the perturbation,
+// replaced by column velocity + perturbation); ref the per-plane references
+// the populations are stored against; phip (compute type) receives the
+// column's phi - phi00 (ehd_set_state_from_column).
+template <typename T, typename R>
+cudaError_t launch_column_state(void *f, void *h, double *const *out_dev, const double *prof_dev,
+                                const double *colv_dev, const double *ref, void *phip,
+                                const double *phi00, const StepConst &c, cudaStream_t s);
 
 // ---- Poisson solve ---------------------------------------------------------
 

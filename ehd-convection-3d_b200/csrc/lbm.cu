@@ -1234,6 +1234,80 @@ __global__ void seeded_state_kernel(double *const *out, const double *__restrict
     }
 }
 
+// Equilibrium of population d of f (density rho, velocity u) and of g
+// (charge ch, advection velocity uc = u + K E): the formulas of
+// init_equilibrium_kernel (LBM.cu:110-276), FP64.
+__device__ __forceinline__ void eq_pair(int d, double rho, double ux, double uy, double uz,
+                                        double ch, double ucx, double ucy, double ucz,
+                                        const StepConst &c, double &fe, double &he) {
+    const double cs2 = c.cs2;
+    const double omusq = 1.0 - 0.5 * (ux * ux + uy * uy + uz * uz) / cs2;
+    const double omusq_c = 1.0 - 0.5 * (ucx * ucx + ucy * ucy + ucz * ucz) / cs2;
+    const double tux = ux / cs2 / c.cfl, tuy = uy / cs2 / c.cfl, tuz = uz / cs2 / c.cfl;
+    const double tcx = ucx / cs2 / c.cfl, tcy = ucy / cs2 / c.cfl, tcz = ucz / cs2 / c.cfl;
+    const double cu = ex_of(d) * tux + ey_of(d) * tuy + ez_of(d) * tuz;
+    const double cc = ex_of(d) * tcx + ey_of(d) * tcy + ez_of(d) * tcz;
+    fe = w_of(d) * rho * (omusq + cu * (1.0 + 0.5 * cu));
+    he = w_of(d) * ch * (omusq_c + cc * (1.0 + 0.5 * cc));
+}
+
+// A 3D state from a 1 x 1 x NZ column's: on every node of plane z the
+// column's populations colv[(s Q + d) nz + z] (s = 0: f, 1: g; the values,
+// not deviations), plus the change of their equilibrium that the seeded
+// velocity perturbation makes (u0 -> u0 + du with the plane's rho, q and E
+// from prof, the column's fields [k][z]), stored against the plane's
+// reference ref.  out[1..3] hold du on entry and u0 + du on exit.  The
+// potential's non-mean part phi' is the column's, phi - phi00 per plane.
+template <typename T, typename R>
+__global__ void column_state_kernel(T *__restrict__ f, T *__restrict__ h, double *const *out,
+                                    const double *__restrict__ prof,
+                                    const double *__restrict__ colv,
+                                    const double *__restrict__ ref, R *__restrict__ phip,
+                                    const double *__restrict__ phi00, StepConst c) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const int nz = c.nz, z = (int)(i / c.nxy);
+    const double rho = prof[z], ch = prof[4 * nz + z];
+    const double u0 = prof[nz + z], v0 = prof[2 * nz + z], w0 = prof[3 * nz + z];
+    const double kex = c.K * prof[6 * nz + z], key = c.K * prof[7 * nz + z],
+                 kez = c.K * prof[8 * nz + z];
+    const double u1 = u0 + out[1][i], v1 = v0 + out[2][i], w1 = w0 + out[3][i];
+    out[1][i] = u1;
+    out[2][i] = v1;
+    out[3][i] = w1;
+    phip[i] = (R)(prof[5 * nz + z] - phi00[z]);
+    const double rref = ref[2 * z], qref = ref[2 * z + 1];
+#pragma unroll
+    for (int d = 0; d < Q; ++d) {
+        double fe0, he0, fe1, he1;
+        eq_pair(d, rho, u0, v0, w0, ch, u0 + kex, v0 + key, w0 + kez, c, fe0, he0);
+        eq_pair(d, rho, u1, v1, w1, ch, u1 + kex, v1 + key, w1 + kez, c, fe1, he1);
+        const double fv = colv[(size_t)d * nz + z] + (fe1 - fe0);
+        const double hv = colv[(size_t)(Q + d) * nz + z] + (he1 - he0);
+        Store<T>::st(f + d * c.n + i, (decltype(Store<T>::ld(f)))(fv - w_of(d) * rref));
+        Store<T>::st(h + d * c.n + i, (decltype(Store<T>::ld(h)))(hv - w_of(d) * qref));
+    }
+}
+
+template <typename T, typename R>
+cudaError_t launch_column_state(void *f, void *h, double *const *out_dev, const double *prof_dev,
+                                const double *colv_dev, const double *ref, void *phip,
+                                const double *phi00, const StepConst &c, cudaStream_t s) {
+    const int bs = 128;
+    column_state_kernel<T, R><<<(unsigned)((c.n + bs - 1) / bs), bs, 0, s>>>(
+        (T *)f, (T *)h, out_dev, prof_dev, colv_dev, ref, (R *)phip, phi00, c);
+    return cudaGetLastError();
+}
+#define EHD_INST_COLUMN(T, R)                                                                  \
+    template cudaError_t launch_column_state<T, R>(void *, void *, double *const *,           \
+                                                   const double *, const double *,            \
+                                                   const double *, void *, const double *,    \
+                                                   const StepConst &, cudaStream_t);
+EHD_INST_COLUMN(double, double)
+EHD_INST_COLUMN(float, float)
+EHD_INST_COLUMN(__half, float)
+EHD_INST_COLUMN(__nv_bfloat16, float)
+
 cudaError_t launch_seeded_state(double *const *out_dev, const double *prof_dev,
                                 unsigned long long seed, double amp, const StepConst &c,
                                 cudaStream_t s) {

@@ -128,6 +128,9 @@ SIGNATURES = {
                                          ctypes.POINTER(ctypes.c_int32),
                                          ctypes.POINTER(ctypes.c_int64), _dp]),
     "ehd_batch_autotune": (_i, [_vp, _i]),
+    "ehd_hydrostatic_column": (_i, [ctypes.POINTER(Params), ctypes.POINTER(Config), _i,
+                                    ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_double)]),
+    "ehd_set_state_from_column": (_i, [_vp, _vp, ctypes.c_uint64, ctypes.c_double]),
 }
 
 _lib = None
@@ -188,6 +191,22 @@ def hydrostatic_profile(p: Params, nsteps: int, precision: str = "fp64", device:
     _check(lib().ehd_hydrostatic_profile(ctypes.byref(p), ctypes.byref(cfg), int(nsteps),
                                          _ptr(prof), ctypes.byref(i0)))
     return {k: prof[i * p.nz:(i + 1) * p.nz].copy() for i, k in enumerate(FIELDS)}, i0.value
+
+
+def hydrostatic_column(p: Params, nsteps: int, precision: str = "fp64", device: int = 0):
+    """ehd_hydrostatic_column: (the 1 x 1 x NZ column after nsteps + 1 steps
+    as a Simulation, I0 on the full NX x NY plane).  Close the column when
+    done with it."""
+    q = Params.from_dict(p.as_dict())
+    q.nx, q.ny, q.lx, q.ly = 1, 1, p.dx, p.dy
+    h = _vp()
+    i0 = ctypes.c_double()
+    cfg = Config(precision=PRECISIONS[precision], device=device)
+    _check(lib().ehd_hydrostatic_column(ctypes.byref(p), ctypes.byref(cfg), int(nsteps),
+                                        ctypes.byref(h), ctypes.byref(i0)))
+    col = Simulation._view(h, q)
+    col.owned = True
+    return col, i0.value
 
 
 def groups_of(p: Params):
@@ -308,6 +327,11 @@ class Simulation:
         prof = np.ascontiguousarray(np.concatenate([np.asarray(profile[k], np.float64)
                                                     for k in FIELDS]))
         _check(lib().ehd_set_state_seeded(self.h, _ptr(prof), int(seed), float(amp)))
+
+    def set_state_from_column(self, column: "Simulation", seed: int = 0, amp: float = 1e-3):
+        """ehd_set_state_from_column: the column's state broadcast over x, y
+        plus the seeded velocity perturbation."""
+        _check(lib().ehd_set_state_from_column(self.h, column.h, int(seed), float(amp)))
 
     def run_to_saturation(self, sample_every=1000, tol=1e-3, hold=3, max_steps=10**7):
         nu = ctypes.c_double()

@@ -13,8 +13,8 @@ Pipeline, all on one GPU:
      electrode nodes); rho comes from the fine hydrostatic column, and phi and
      E from a Poisson solve of the interpolated charge;
   4. from that state the fine grid runs `steps` steps with FP16 deviation
-     storage, and, for the storage error, in FP32; a cold start (fine
-     hydrostatic column plus seeded noise) runs the same steps in FP32.
+     storage, and, for the storage error, in FP32; a cold start (the fine
+     hydrostatic column's state plus seeded noise) runs the same steps in FP32.
      Diagnostics (kinetic energy, Nu_e, total charge) every `sample` steps.
 
 Fields are in the solver's physical units (velocity, charge density and
@@ -122,11 +122,13 @@ def predict(ehd, net, mean, std, group: dict, coarse_grid, transits=4.0, device=
     import sweep
     import warmstart as W
     p = W.params_of(ehd, group, *coarse_grid)
-    [(prof, i0)] = sweep.hydrostatic_profiles(ehd, [p], [sweep.hydrostatic_steps(p, transits)],
-                                              device=device)
+    cbs, [(col, i0)] = sweep.hydrostatic_columns(ehd, [p], [sweep.hydrostatic_steps(p, transits)],
+                                                 device=device)
     with ehd.Simulation(p, "fp32", device=device) as sim:
-        sim.set_state_seeded(prof, seed=group["seed"], amp=1e-3)
+        sim.set_state_from_column(col, seed=group["seed"], amp=1e-3)
         f0 = sim.get_fields()
+    for cb in cbs:
+        cb.close()
     x = torch.tensor(W.channels(f0, p, group)[None], device=torch.device("cuda", device))
     u = net.forward(x).cpu().numpy()[0].astype(np.float64) * std + mean
     pred = {"u": u[..., 0], "v": u[..., 1], "w": u[..., 2], "q": u[..., 3] * p.charge0,
@@ -184,8 +186,10 @@ def compare(ehd, coarse_p, pred: dict, group: dict, tiles: int, factor: int, ste
     """The fine-grid runs of step 4 of the pipeline for one prediction."""
     import sweep
     fp = fine_params(ehd, coarse_p, tiles, factor)
-    [(fprof, i0)] = sweep.hydrostatic_profiles(ehd, [fp], [sweep.hydrostatic_steps(fp, transits)],
-                                               device=device)
+    cbs, [(fcol, i0)] = sweep.hydrostatic_columns(ehd, [fp],
+                                                  [sweep.hydrostatic_steps(fp, transits)],
+                                                  device=device)
+    fprof = {"rho": np.asarray(fcol.get_fields(("rho",))["rho"]).reshape(-1)}
     start = warm_fields(pred, fprof, tiles, factor)
     nodes = fp.nx * fp.ny * fp.nz
     res = {"fine_grid": [fp.nx, fp.ny, fp.nz], "fine_lx": fp.lx, "steps": steps,
@@ -201,7 +205,7 @@ def compare(ehd, coarse_p, pred: dict, group: dict, tiles: int, factor: int, ste
                 sim.set_fields(start)
                 sim.poisson()  # phi and E of the interpolated charge
             else:
-                sim.set_state_seeded(fprof, seed=group["seed"], amp=1e-3)
+                sim.set_state_from_column(fcol, seed=group["seed"], amp=1e-3)
             sim.set_reference_current(i0)
             d0 = sim.diagnostics()
             r = run(sim, steps, sample)
@@ -215,6 +219,8 @@ def compare(ehd, coarse_p, pred: dict, group: dict, tiles: int, factor: int, ste
             last = r["history"][-1]
             log(f"{name}: KE {r['initial']['kinetic_energy']:.3e} -> {last['kinetic_energy']:.3e}, "
                 f"Nu_e {last['nu_e']:.5f}, {r['mlups']:.0f} MLUPS")
+    for cb in cbs:
+        cb.close()
     if warm_precision in ends and "fp32" in ends and warm_precision != "fp32":
         res["warm_storage_error"] = field_errors(ends[warm_precision], ends["fp32"])
     return res

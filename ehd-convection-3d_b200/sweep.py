@@ -7,7 +7,8 @@ compile-time grid (LBM.h:34-36).  A sweep is a list of instances (T, grid,
 seed).  Each rank of a torch.distributed job takes a share of them, balanced
 by node count, runs its share as one ehd_batch (one CUDA graph launch per step
 over all of its instances, launch shapes from the batch autotuner) from the
-hydrostatic state plus seeded noise until each instance's Nu_e saturates, and
+hydrostatic column's own state (ehd_set_state_from_column) plus seeded noise
+until each instance's Nu_e saturates, and
 the per-instance results are gathered on every rank.  The only exchange
 between ranks is that gather (a few numbers per instance).
 
@@ -107,6 +108,36 @@ def hydrostatic_profiles(ehd, params: list, nsteps: list, device=0):
     return out
 
 
+def hydrostatic_columns(ehd, params: list, nsteps: list, device=0):
+    """ehd_hydrostatic_column for many instances at once: the 1 x 1 x NZ
+    columns of all instances with the same step count run as one FP64 batch,
+    left after n + 1 steps.  Returns the batches (close them when done) and,
+    per instance, (column, I0) with I0 the mean of the currents after n and
+    n + 1 steps, as ehd_hydrostatic_column has them."""
+    out = [None] * len(params)
+    batches = []
+    by_steps = {}
+    for i, n in enumerate(nsteps):
+        by_steps.setdefault(int(n), []).append(i)
+    for n, idx in by_steps.items():
+        cols = []
+        for i in idx:
+            q = ehd.Params.from_dict(params[i].as_dict())
+            q.nx, q.ny, q.lx, q.ly = 1, 1, params[i].dx, params[i].dy
+            cols.append(q)
+        b = ehd.Batch(cols, "fp64", device=device)
+        batches.append(b)
+        for sim in b:
+            sim.initialize()
+        b.step(n)
+        cur = [sim.diagnostics()["current"] for sim in b]
+        b.step(1)
+        for i, sim, c0 in zip(idx, b, cur):
+            i0 = 0.5 * (c0 + sim.diagnostics()["current"]) * params[i].nx * params[i].ny
+            out[i] = (sim, i0)
+    return batches, out
+
+
 def run_share(share: list[dict], precision="fp16", device=0, amp=1.0e-3, sample_every=1000,
               tol=1e-3, hold=3, max_steps=200000, min_steps=0, autotune=True,
               hydrostatic_transits=16.0, **groups) -> list[dict]:
@@ -122,17 +153,18 @@ def run_share(share: list[dict], precision="fp16", device=0, amp=1.0e-3, sample_
 
     t0 = time.perf_counter()
     params = [instance_params(ehd, s, **groups) for s in share]
-    starts = hydrostatic_profiles(ehd, params,
-                                  [hydrostatic_steps(p, hydrostatic_transits) for p in params],
-                                  device=device)
+    col_batches, starts = hydrostatic_columns(
+        ehd, params, [hydrostatic_steps(p, hydrostatic_transits) for p in params], device=device)
     t1 = time.perf_counter()
     batch = ehd.Batch(params, precision, device=device)
     try:
         if autotune:
             batch.autotune(trial_steps=10)
-        for sim, s, (prof, i0) in zip(batch, share, starts):
-            sim.set_state_seeded(prof, seed=s["seed"], amp=amp)
+        for sim, s, (col, i0) in zip(batch, share, starts):
+            sim.set_state_from_column(col, seed=s["seed"], amp=amp)
             sim.set_reference_current(i0)
+        for b in col_batches:
+            b.close()
         t2 = time.perf_counter()
         if min_steps > 0:
             batch.step(min_steps)
@@ -149,6 +181,8 @@ def run_share(share: list[dict], precision="fp16", device=0, amp=1.0e-3, sample_
         return out
     finally:
         batch.close()
+        for b in col_batches:
+            b.close()
 
 
 def gather(results: list[dict], dist=None) -> list[dict]:

@@ -5,7 +5,7 @@ past the linear-growth transient.  No reference counterpart.
 
 Pipeline, all on one GPU:
   1. trajectories: instances with T, M, C drawn uniformly, each from its
-     hydrostatic column plus seeded noise, run `horizon` steps as batches
+     hydrostatic column's state plus seeded noise, run `horizon` steps as batches
      (one graph launch per step for a whole batch);
   2. training: Adam on the mean-square error of standardised fields;
   3. evaluation on held-out instances: the prediction against the plain
@@ -79,17 +79,19 @@ def trajectories(ehd, groups, horizon, chunk=64, transits=4.0, precision="fp32",
     for c0 in range(0, len(groups), chunk):
         gs = groups[c0:c0 + chunk]
         ps = [params_of(ehd, g, *grid) for g in gs]
-        starts = sweep.hydrostatic_profiles(ehd, ps, [sweep.hydrostatic_steps(p, transits)
-                                                      for p in ps], device=device)
+        cbs, starts = sweep.hydrostatic_columns(ehd, ps, [sweep.hydrostatic_steps(p, transits)
+                                                          for p in ps], device=device)
         with ehd.Batch(ps, precision, device=device) as b:
             firsts = []
-            for sim, g, (prof, i0) in zip(b, gs, starts):
-                sim.set_state_seeded(prof, seed=g["seed"], amp=1e-3)
+            for sim, g, (col, i0) in zip(b, gs, starts):
+                sim.set_state_from_column(col, seed=g["seed"], amp=1e-3)
                 sim.set_reference_current(i0)
                 firsts.append(sim.get_fields())
+            for cb in cbs:
+                cb.close()
             keep = []
-            for sim, g, p, f0, (prof, i0), d in zip(b, gs, ps, firsts, starts,
-                                                    b.step_sampled(horizon)):
+            for sim, g, p, f0, (col, i0), d in zip(b, gs, ps, firsts, starts,
+                                                   b.step_sampled(horizon)):
                 if d["nonfinite"]:
                     keep.append(False)
                     continue
@@ -177,28 +179,32 @@ def main(argv=None):
     t_train = time.perf_counter() - t1
     # held-out: prediction against the plain run's state at the horizon
     errs, base = [], []
+    errs_v, base_v = [], []  # the velocity channels alone
     preds = []
     for k in range(len(ite)):
         u = net.forward(torch.tensor(xte[k:k + 1], device=dev)).cpu().numpy()[0] * std + mean
         preds.append(u)
         errs.append(rel_l2(u, yte[k]))
         base.append(rel_l2(xte[k][..., :COUT], yte[k]))
+        errs_v.append(rel_l2(u[..., :3], yte[k][..., :3]))
+        base_v.append(rel_l2(xte[k][..., :3], yte[k][..., :3]))
     # warm start: a short run from the prediction against the plain run
     # continued by the same number of steps
     nu_warm, nu_cold, nu_none = [], [], []
     import sweep
     m = min(len(ite), 16)
     ps = [params_of(ehd, ite[k], *grid) for k in range(m)]
-    starts = sweep.hydrostatic_profiles(ehd, ps, [sweep.hydrostatic_steps(p, 4.0) for p in ps])
+    cbs, starts = sweep.hydrostatic_columns(ehd, ps, [sweep.hydrostatic_steps(p, 4.0) for p in ps])
     with ehd.Batch(ps, "fp32") as bw, ehd.Batch(ps, "fp32") as bn:
         for k in range(m):
-            p, (prof, i0) = ps[k], starts[k]
+            p, (col, i0) = ps[k], starts[k]
+            rho = np.asarray(col.get_fields(("rho",))["rho"]).reshape(-1)
             u = preds[k]
             shape = u.shape[:3]
             f = {"u": u[..., 0].astype(np.float64), "v": u[..., 1].astype(np.float64),
                  "w": u[..., 2].astype(np.float64), "q": u[..., 3] * p.charge0,
                  "phi": u[..., 4] * p.voltage,
-                 "rho": np.broadcast_to(prof["rho"][:, None, None], shape).copy(),
+                 "rho": np.broadcast_to(rho[:, None, None], shape).copy(),
                  "ex": np.zeros(shape), "ey": np.zeros(shape), "ez": np.zeros(shape)}
             for key in ("u", "v", "w"):
                 f[key][0] = 0.0
@@ -206,8 +212,10 @@ def main(argv=None):
             bw[k].set_fields({key: np.ascontiguousarray(v, np.float64) for key, v in f.items()})
             bw[k].poisson()  # phi and E consistent with the predicted charge
             bw[k].set_reference_current(i0)
-            bn[k].set_state_seeded(prof, seed=ite[k]["seed"], amp=1e-3)
+            bn[k].set_state_from_column(col, seed=ite[k]["seed"], amp=1e-3)
             bn[k].set_reference_current(i0)
+        for cb in cbs:
+            cb.close()
         dw = bw.step_sampled(a.relax)
         dn = bn.step_sampled(a.relax)
         for k in range(m):
@@ -220,6 +228,9 @@ def main(argv=None):
         "loss_first": hist[0], "loss_last": hist[-1],
         "pred_rel_l2_mean": float(np.mean(errs)), "initial_rel_l2_mean": float(np.mean(base)),
         "gain": float(np.mean(base) / max(np.mean(errs), 1e-30)),
+        "pred_rel_l2_velocity": float(np.mean(errs_v)),
+        "initial_rel_l2_velocity": float(np.mean(base_v)),
+        "gain_velocity": float(np.mean(base_v) / max(np.mean(errs_v), 1e-30)),
         "nu_e_plain_at_horizon_plus_relax": nu_cold,
         "nu_e_warm_after_relax": nu_warm,
         "nu_e_plain_after_relax_from_start": nu_none,

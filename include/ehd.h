@@ -191,6 +191,23 @@ int ehd_hydrostatic_profile(const ehd_params *params, const ehd_config *config, 
  * reference (its perturbation, LBM.cu:389-415, is a disabled sinusoid). */
 int ehd_set_state_seeded(ehd_ctx *ctx, const double *profile, uint64_t seed, double amp);
 
+/* The hydrostatic state as a live 1 x 1 x NZ context: the column of
+ * ehd_hydrostatic_profile, left after nsteps + 1 steps (*column, freed with
+ * ehd_destroy), with *i0 as there.  Not in the reference. */
+int ehd_hydrostatic_column(const ehd_params *params, const ehd_config *config, int nsteps,
+                           ehd_ctx **column, double *i0);
+
+/* Sets the state to a 1 x 1 x NZ column's state broadcast over x, y: its
+ * populations (not equilibria rebuilt from its fields), reference tables,
+ * potential and fields, plus the seeded velocity perturbation of
+ * ehd_set_state_seeded, added to the populations as the change of their
+ * equilibrium.  With amp = 0 every plane then evolves as the column does; a
+ * start from the column's fields through ehd_set_state_seeded perturbs the
+ * planes next to the injector instead.  The column (FP64 or FP32, the
+ * context's parameters but for nx, ny, lx, ly) must have stepped at least
+ * once since its upload.  Not in the reference. */
+int ehd_set_state_from_column(ehd_ctx *ctx, ehd_ctx *column, uint64_t seed, double amp);
+
 /* Steps until the electric Nusselt number Nu_e = I / I0 (I0 from
  * ehd_set_reference_current) changes by less than tol relative between
  * consecutive samples every sample_every steps, hold times in a row, or until

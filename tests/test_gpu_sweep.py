@@ -1,6 +1,7 @@
 """A small T-sweep share on one GPU through sweep.run_share: every instance
-runs from the hydrostatic state plus its seeded noise, in one batch, and its
-result equals the same instance run alone with the same launch shapes."""
+runs from its hydrostatic column's state plus its seeded noise, in one batch,
+and its result equals the same instance run alone with the same launch
+shapes."""
 import importlib.util
 
 import pytest
@@ -28,9 +29,10 @@ def test_share_runs_and_matches_lone_instances():
     for s, r in zip(insts, res):
         assert not r["nonfinite"] and 0 < r["steps"] <= 300
         p = S.instance_params(ehd, s)
-        prof, i0 = ehd.hydrostatic_profile(p, S.hydrostatic_steps(p, 2.0))
+        col, i0 = ehd.hydrostatic_column(p, S.hydrostatic_steps(p, 2.0))
         with ehd.Simulation(p, "fp32") as sim:  # the same instance alone
-            sim.set_state_seeded(prof, seed=s["seed"], amp=1e-3)
+            sim.set_state_from_column(col, seed=s["seed"], amp=1e-3)
+            col.close()
             sim.set_reference_current(i0)
             alone = sim.run_to_saturation(sample_every=50, tol=1e-3, hold=2, max_steps=300)
         assert (r["nu_e"], r["steps"], r["saturated"]) == (alone["nu_e"], alone["steps"],
