@@ -156,12 +156,15 @@ int main(int argc, char **argv) {
     } else if (o.restart) {
         if (ehd_read_data_end(ctx, "data_end.dat") != EHD_OK) return die("read data_end.dat");
     } else if (o.hydrostatic >= 0) {
-        std::vector<double> prof(9 * (size_t)P.nz);
+        // the column's own state broadcast over the plane, plus seeded noise
         ehd_config c64{};
         c64.precision = EHD_PREC_FP64;
-        if (ehd_hydrostatic_profile(&P, &c64, (int)o.hydrostatic, prof.data(), &i0) != EHD_OK)
-            return die("hydrostatic profile");
-        if (ehd_set_state_seeded(ctx, prof.data(), o.seed, o.amp) != EHD_OK) return die("seeded state");
+        ehd_ctx *col = nullptr;
+        if (ehd_hydrostatic_column(&P, &c64, (int)o.hydrostatic, &col, &i0) != EHD_OK)
+            return die("hydrostatic column");
+        const int rc = ehd_set_state_from_column(ctx, col, o.seed, o.amp);
+        ehd_destroy(col);
+        if (rc != EHD_OK) return die("state from column");
         ehd_set_reference_current(ctx, i0);
     } else if (ehd_initialize(ctx) != EHD_OK) {
         return die("initialize");
