@@ -75,11 +75,24 @@ __global__ void mix_kernel(const float *__restrict__ re, const float *__restrict
     for (int md = blockIdx.x * nw + warp; md < modes; md += gridDim.x * nw) {
         const float *pr = re + (size_t)md * WW, *pi = im + (size_t)md * WW;
         __syncwarp();
-        for (int t = lane; t < W * W; t += 32) {
-            const int o = t / W, i = t - o * W;
-            const int r = adj ? i : o, c = adj ? o : i;
-            Rr[r * WP + c] = __ldg(pr + t);
-            Ri[r * WP + c] = adj ? -__ldg(pi + t) : __ldg(pi + t);
+        // eight rows of 32 weights of each part in flight per lane at a time
+        for (int t0 = 0; t0 < W * W; t0 += 256) {
+            float vr[8], vi[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int t = t0 + 32 * u + lane;
+                vr[u] = t < W * W ? __ldg(pr + t) : 0.f;
+                vi[u] = t < W * W ? __ldg(pi + t) : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int t = t0 + 32 * u + lane;
+                if (t >= W * W) break;
+                const int o = t / W, i = t - o * W;
+                const int r = adj ? i : o, c = adj ? o : i;
+                Rr[r * WP + c] = vr[u];
+                Ri[r * WP + c] = adj ? -vi[u] : vi[u];
+            }
         }
         for (int b0 = 0; b0 < B; b0 += 4) {
             const int nb = min(4, B - b0);
@@ -139,18 +152,31 @@ __global__ void mix_wgrad_kernel(const float *__restrict__ dout, const float *__
                 X[t] = bb < nb ? __ldg(x + o) : 0.f;
             }
             __syncwarp();
-            for (int t = lane; t < W * W; t += 32) {
-                const int o = t / W, i = t - o * W;
-                float sr = 0.f, sm = 0.f;
+            // the gradient rows read eight at a time per lane, then updated
+            for (int t0 = 0; t0 < W * W; t0 += 256) {
+                float og[8], om[8];
 #pragma unroll
-                for (int bb = 0; bb < 4; ++bb) {
-                    const float dr = D[bb * 2 * W + o], di = D[bb * 2 * W + W + o];
-                    const float xr = X[bb * 2 * W + i], xi = X[bb * 2 * W + W + i];
-                    sr = fmaf(dr, xr, fmaf(di, xi, sr));
-                    sm = fmaf(di, xr, fmaf(-dr, xi, sm));
+                for (int u = 0; u < 8; ++u) {
+                    const int t = t0 + 32 * u + lane;
+                    og[u] = t < W * W ? gr[t] : 0.f;
+                    om[u] = t < W * W ? gm[t] : 0.f;
                 }
-                gr[t] += sr;
-                gm[t] += sm;
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int t = t0 + 32 * u + lane;
+                    if (t >= W * W) break;
+                    const int o = t / W, i = t - o * W;
+                    float sr = 0.f, sm = 0.f;
+#pragma unroll
+                    for (int bb = 0; bb < 4; ++bb) {
+                        const float dr = D[bb * 2 * W + o], di = D[bb * 2 * W + W + o];
+                        const float xr = X[bb * 2 * W + i], xi = X[bb * 2 * W + W + i];
+                        sr = fmaf(dr, xr, fmaf(di, xi, sr));
+                        sm = fmaf(di, xr, fmaf(-dr, xi, sm));
+                    }
+                    gr[t] = og[u] + sr;
+                    gm[t] = om[u] + sm;
+                }
             }
         }
     }
