@@ -964,7 +964,15 @@ int ehd_bf16_gemm(int M, int N, int K, int batch, const float *A, int64_t a_row,
     g.alpha = alpha;
     g.beta = beta;
     // the caller's arrays are taken to span exactly the largest offsets
-    g.a_n = g.b_n = g.c_n = (long long)1 << 62;
+    // (negative strides are rejected by gemm())
+    auto span = [](long long n0, long long s0, long long n1, long long s1, long long n2,
+                   long long s2) {
+        return (n0 - 1) * std::max<long long>(s0, 0) + (n1 - 1) * std::max<long long>(s1, 0) +
+               (n2 - 1) * std::max<long long>(s2, 0) + 1;
+    };
+    g.a_n = span(M, a_row, K, a_col, batch, ab);
+    g.b_n = span(K, b_row, N, b_col, batch, bb);
+    g.c_n = span(M, c_row, N, c_col, batch, cb);
     cudaError_t e = gemm(g, (cudaStream_t)stream);
     return e == cudaSuccess ? EHD_OK : cuda_fail("ehd_bf16_gemm", e);
 }

@@ -721,12 +721,13 @@ LeftKern left_kernel_nt(int mt) {
     }
 }
 
-// 8 NT columns per warp unit: the widest unit (at most 64 accumulators a
-// thread, MT NT <= 16) that still gives 4096 units, so that every warp of
-// a full GPU has several to interleave
+// 8 NT columns per warp unit: the widest unit (at most 32 accumulators a
+// thread, MT NT <= 8: more blocks per SM measured faster than wider units)
+// that still gives 4096 units, so that every warp of a full GPU has several
+// to interleave
 int left_nt(int mt, long long batch, int N) {
     for (int nt = 4; nt > 1; nt /= 2)
-        if (mt * nt <= 16 && batch * ((N + 8 * nt - 1) / (8 * nt)) >= 4096) return nt;
+        if (mt * nt <= 8 && batch * ((N + 8 * nt - 1) / (8 * nt)) >= 4096) return nt;
     return 1;
 }
 

@@ -26,8 +26,9 @@ def rel(a, b):
 # 32, 64, 128, N <= 128) for the first four and (24, 32, 64), (1000, 32, 64),
 # (16, 8, 16): partial 16-row tiles, odd C rows (single-element stores),
 # batches; the small-left-matrix one (one A, M, K <= 128, B with unit stride
-# along n) for the last four: M = 9..128, K = 5..128 (partial K steps), odd N;
-# the tiled one for the rest (K = 112 and 200, transposed batched A, K = 1000)
+# along n) for (17, 9, 112) and the last four: M = 9..128, K = 5..128
+# (partial K steps), odd N; the tiled one for the rest (K = 200, a transposed
+# A per product, K = 1000)
 @pytest.mark.parametrize("M,N,K,batch,ta,tb", [(64, 64, 32, 1, False, False),
                                                (37, 5, 128, 2, False, False),
                                                (300, 128, 32, 1, False, False),
@@ -50,6 +51,24 @@ def test_gemm_matches_float64_products_of_bf16_operands(M, N, K, batch, ta, tb):
         torch.randn(batch, M, K, generator=g).cuda()
     B = torch.randn(batch, N, K, generator=g).cuda().transpose(1, 2) if tb else \
         torch.randn(batch, K, N, generator=g).cuda()
+    C0 = torch.randn(batch, M, N, generator=g).cuda()
+    C = C0.clone()
+    fno.gemm(A, B, C, alpha=0.5, beta=2.0)
+    ref = 0.5 * (A.bfloat16().double() @ B.bfloat16().double()) + 2.0 * C0.double()
+    err = (C.double() - ref).abs().max().item() / ref.abs().max().item()
+    assert err < 1e-5, err
+
+
+@pytest.mark.parametrize("M,N,K,batch", [(24, 8192, 64, 16), (64, 8192, 48, 8),
+                                         (128, 4096, 40, 8)])
+def test_gemm_with_one_left_matrix_for_the_batch(M, N, K, batch):
+    """The small-left-matrix kernel with 32-, 16- and 8-column warp units (it
+    takes the widest that still leaves 4096 units): one A for every product
+    of the batch, as the truncated DFTs have it."""
+    import torch
+    g = torch.Generator().manual_seed(M + N + K)
+    A = torch.randn(1, M, K, generator=g).cuda().expand(batch, M, K)
+    B = torch.randn(batch, K, N, generator=g).cuda()
     C0 = torch.randn(batch, M, N, generator=g).cuda()
     C = C0.clone()
     fno.gemm(A, B, C, alpha=0.5, beta=2.0)
