@@ -1,10 +1,20 @@
-// gemm_bf16.cu -- the batched BF16 tensor-core product of gemm_bf16.cuh.
+// gemm_bf16.cu -- the batched BF16 tensor-core product of gemm_bf16.cuh, and
+// the weight and bias gradients of pointwise layers.
 //
-// 64 x 64 output tiles, K in steps of 32, 128 threads: each warp owns a
-// 32 x 32 quarter as 2 x 4 tiles of mma.sync.m16n8k16 (BF16 in, FP32 out).
-// Operands are staged in shared memory as BF16, A as [m][k] and B as [n][k],
-// so that every fragment register is one aligned 32-bit load of two
-// consecutive k.
+// gemm() sends a product to one of three kernels by its shape (all of them
+// mma.sync.m16n8k16, BF16 operands, FP32 accumulation):
+//  - rowwise_kernel: A FP32 with unit stride along k, 16 | K <= 128, N <= 128
+//    (pointwise layers and their input gradients): B resident in shared
+//    memory, A fragments straight from global memory, warps streaming 16-row
+//    tiles;
+//  - leftmul_kernel: one A for the whole batch, M, K <= 128, B FP32 with unit
+//    stride along n (the truncated DFTs): A resident in shared memory, B
+//    fragments straight from global memory in warp units of 8-32 columns;
+//  - gemm_kernel, the general tiled product: 64 x 64 output tiles, K in steps
+//    of 32, 128 threads, each warp a 32 x 32 quarter as 2 x 4 mma tiles;
+//    operands staged in shared memory as BF16, A as [m][k] and B as [n][k],
+//    so that every fragment register is one aligned 32-bit load of two
+//    consecutive k.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
