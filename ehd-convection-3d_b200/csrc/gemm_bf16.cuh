@@ -4,12 +4,13 @@
 // C[m][n] = alpha * sum_k A[m][k] B[k][n] (+ beta C) (+ bias[n]), optionally
 // with a second output gelu(C), over a batch of independent products.  Every
 // index of every operand goes through a two-level map i -> (i / g) s1 +
-// (i % g) s0, so one kernel serves transposed operands and the layouts of the
-// FNO's truncated transforms, whose real/imaginary index sits above the
-// transformed axis.  A and B are read as FP32 or BF16 and rounded to BF16 in
-// shared memory; products accumulate in FP32 (mma.sync m16n8k16).  With
-// ksplit > 1 the K range is split over blocks that add into C atomically
-// (beta must then be 1, no bias, no second output).
+// (i % g) s0, so one interface serves transposed operands and the layouts of
+// the FNO's truncated transforms, whose real/imaginary index sits above the
+// transformed axis.  A and B are read as FP32 or BF16 and rounded to BF16;
+// products accumulate in FP32 (mma.sync m16n8k16).  gemm() picks one of three
+// kernels by the product's shape (gemm_bf16.cu).  With ksplit > 1 the K range
+// is split over blocks that add into C atomically (beta must then be 1, no
+// bias, no second output).
 #pragma once
 
 #include <cuda_bf16.h>
