@@ -1,8 +1,9 @@
 // io.cu -- the reference's text formats on the host, over the C ABI.
 //
 // data_end.dat (save_data_end, LBM.cu:1506-1566, and read_data,
-// LBM.cu:1597-1643) and the Tecplot ASCII file (save_data_tecplot,
-// LBM.cu:1427-1503), so a driver that replaces the reference's time loop
+// LBM.cu:1597-1643), the Tecplot ASCII file (save_data_tecplot,
+// LBM.cu:1427-1503) and the uz file for DMD post-processing (save_data_dmd,
+// LBM.cu:1569-1594), so a driver that replaces the reference's time loop
 // keeps its output and restart files.
 #include <cstdio>
 #include <vector>
@@ -65,6 +66,30 @@ extern "C" int ehd_write_data_end(ehd_ctx *c, const char *path) {
                              f.a[6][i], f.a[7][i], f.a[8][i]);
             }
     if (std::fclose(fp) != 0) return ehd::set_error(EHD_ERR_IO, "writing the data_end file failed");
+    return EHD_OK;
+}
+
+// save_data_dmd (LBM.cu:1569-1594): "t uz" per node, %10.6f, uz extrapolated
+// onto both walls from the two planes inside
+extern "C" int ehd_write_dmd(ehd_ctx *c, const char *path) {
+    if (!c || !path) return ehd::set_error(EHD_ERR_INVALID, "NULL argument");
+    const ehd_params *p = ehd::ctx_params(c);
+    const int nx = p->nx, ny = p->ny, nz = p->nz;
+    if (nz < 3) return ehd::set_error(EHD_ERR_INVALID, "the DMD file needs nz >= 3");
+    const size_t nxy = (size_t)nx * ny;
+    std::vector<double> w(nxy * nz);
+    int r = ehd_get_fields(c, nullptr, nullptr, nullptr, w.data(), nullptr, nullptr, nullptr,
+                           nullptr, nullptr);
+    if (r != EHD_OK) return r;
+    for (size_t i = 0; i < nxy; ++i) {
+        w[i] = 2.0 * w[nxy + i] - w[2 * nxy + i];
+        w[(nz - 1) * nxy + i] = 2.0 * w[(nz - 2) * nxy + i] - w[(nz - 3) * nxy + i];
+    }
+    FILE *fp = std::fopen(path, "w");
+    if (!fp) return ehd::set_error(EHD_ERR_IO, "cannot open the DMD file for writing");
+    const double t = *ehd::ctx_time(c);
+    for (size_t i = 0; i < w.size(); ++i) std::fprintf(fp, "%10.6f %10.6f\n", t, w[i]);
+    if (std::fclose(fp) != 0) return ehd::set_error(EHD_ERR_IO, "writing the DMD file failed");
     return EHD_OK;
 }
 

@@ -3,14 +3,15 @@
 //
 // The reference fixes everything at compile time (LBM.h:30-86); here the same
 // quantities are options.  The loop keeps main.cu's structure and output
-// files: data.dat (Tecplot zones, main.cu:167-168, 210-212, 268), umax.dat
+// files: data.dat (Tecplot zones, main.cu:167-168, 210-212, 268), the "<t>.dat"
+// uz files for DMD every --dmd-every steps (main.cu:213-224), umax.dat
 // (record_umax, main.cu:236), the "Current = " line (main.cu:227-231), the
 // performance report (main.cu:242-266) and data_end.dat (main.cu:275-277).
 //
 //   ehd_sim [--nx 122] [--ny 122] [--nz 101] [--lx L] [--ly L]
 //           [--T t --M m --C c --Fe fe | --nu .. --K .. --charge0 .. --diffu ..]
 //           [--lambda-f 1/12] [--lambda-g 1e-6] [--uw 0] [--exf 0]
-//           [--steps 1000] [--save-every N] [--current-every 1000]
+//           [--steps 1000] [--save-every N] [--current-every 1000] [--dmd-every 50000]
 //           [--precision fp64|fp32|fp16|bf16] [--restart] [--hydrostatic NSTEPS]
 //           [--seed 0] [--amp 1e-3] [--checkpoint PATH] [--resume PATH] [--no-output]
 #include <chrono>
@@ -32,7 +33,7 @@ struct Options {
     double T = -1, M = -1, C = -1, Fe = -1;
     double nu = 0.0251004, K = 2.5e-5, charge0 = 10.0, diffu = 6.25e-5;
     double lambda_f = 1.0 / 12.0, lambda_g = 1.0e-6, uw = 0.0, exf = 0.0;
-    long long steps = 1000, save_every = 0, current_every = 1000;
+    long long steps = 1000, save_every = 0, current_every = 1000, dmd_every = 50000;
     int precision = EHD_PREC_FP64;
     bool restart = false, no_output = false;
     long long hydrostatic = -1;
@@ -81,6 +82,7 @@ bool parse(int argc, char **argv, Options &o) {
         else if (a == "--steps" && ival(v)) o.steps = v;
         else if (a == "--save-every" && ival(v)) o.save_every = v;
         else if (a == "--current-every" && ival(v)) o.current_every = v;
+        else if (a == "--dmd-every" && ival(v)) o.dmd_every = v;
         else if (a == "--hydrostatic" && ival(v)) o.hydrostatic = v;
         else if (a == "--seed" && ival(v)) o.seed = (unsigned long long)v;
         else if (a == "--amp" && val(d)) o.amp = d;
@@ -178,6 +180,14 @@ int main(int argc, char **argv) {
         if (ehd_step(ctx, 1) != EHD_OK) return die("step");
         if (o.save_every > 0 && i % o.save_every == 1 && !o.no_output)
             if (ehd_write_tecplot(ctx, "data.dat", 0) != EHD_OK) return die("data.dat");
+        if (o.dmd_every > 0 && i % o.dmd_every == 1 && !o.no_output) {
+            ehd_diag dd{};
+            if (ehd_diagnostics(ctx, &dd) != EHD_OK) return die("diagnostics");
+            std::printf("Iteration: %lld, physical time: %g.\n", i, dd.time);
+            char name[128];
+            std::snprintf(name, sizeof(name), "%g.dat", dd.time);
+            if (ehd_write_dmd(ctx, name) != EHD_OK) return die("DMD file");
+        }
         if (o.current_every > 0 && i % o.current_every == 1) {
             if (ehd_diagnostics(ctx, &d) != EHD_OK) return die("diagnostics");
             if (i0 != 0.0) std::printf("Current = %g  Nu_e = %g\n", d.current, d.nu_e);

@@ -131,6 +131,7 @@ SIGNATURES = {
     "ehd_hydrostatic_column": (_i, [ctypes.POINTER(Params), ctypes.POINTER(Config), _i,
                                     ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_double)]),
     "ehd_set_state_from_column": (_i, [_vp, _vp, ctypes.c_uint64, ctypes.c_double]),
+    "ehd_write_dmd": (_i, [_vp, ctypes.c_char_p]),
 }
 
 _lib = None
@@ -353,6 +354,9 @@ class Simulation:
 
     def read_data_end(self, path):
         _check(lib().ehd_read_data_end(self.h, str(path).encode()))
+
+    def write_dmd(self, path):
+        _check(lib().ehd_write_dmd(self.h, str(path).encode()))
 
     def write_tecplot(self, path, first=True):
         _check(lib().ehd_write_tecplot(self.h, str(path).encode(), int(bool(first))))

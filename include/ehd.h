@@ -230,10 +230,13 @@ int ehd_restore(ehd_ctx *ctx, const char *path);
  * LBM.cu:1506-1566: ten %10.6f columns t u v w rho q phi Ex Ey Ez, rho q u v w
  * extrapolated onto the walls), and its reader (read_data, LBM.cu:1597-1643)
  * followed by the equilibrium rebuild; the Tecplot writer (save_data_tecplot,
- * LBM.cu:1427-1503; first != 0 writes the VARIABLES header). */
+ * LBM.cu:1427-1503; first != 0 writes the VARIABLES header); the uz file for
+ * DMD post-processing (save_data_dmd, LBM.cu:1569-1594: "%10.6f %10.6f" t, uz
+ * per node, uz extrapolated onto the walls). */
 int ehd_write_data_end(ehd_ctx *ctx, const char *path);
 int ehd_read_data_end(ehd_ctx *ctx, const char *path);
 int ehd_write_tecplot(ehd_ctx *ctx, const char *path, int first);
+int ehd_write_dmd(ehd_ctx *ctx, const char *path);
 
 /* --- information -------------------------------------------------------- */
 

@@ -13,10 +13,18 @@ def test_driver_matches_the_api(tmp_path):
     exe = PKG / "ehd_sim"
     assert exe.exists(), "build with make -C ehd-convection-3d_b200"
     r = subprocess.run([str(exe), "--nx", "16", "--ny", "16", "--nz", "9", "--steps", "20",
-                        "--current-every", "5", "--save-every", "10", "--precision", "fp64"],
+                        "--current-every", "5", "--save-every", "10", "--dmd-every", "10",
+                        "--precision", "fp64"],
                        cwd=tmp_path, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     assert "speed:" in r.stdout and r.stdout.count("Current = ") == 4
+    # uz files for DMD at i % 10 == 1, named by the time after that step
+    assert r.stdout.count("Iteration: ") == 2
+    dmd = sorted(f.name for f in tmp_path.glob("*.dat")
+                 if f.name not in ("data.dat", "data_end.dat", "umax.dat"))
+    assert len(dmd) == 2, dmd
+    for f in dmd:
+        assert np.loadtxt(tmp_path / f).shape == (16 * 16 * 9, 2)
     # the same run through the API: the reference defaults, its initialization
     p = O.reference_default_params(16, 16, 9)
     with ehd.Simulation(ehd.Params.from_dict(p.as_dict()), "fp64") as sim:

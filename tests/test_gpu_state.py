@@ -127,6 +127,24 @@ def test_tecplot_writer(tmp_path):
     assert len(lines) == 1 + 2 * (2 + p.nx * p.ny * p.nz)
 
 
+def test_dmd_writer(tmp_path):
+    """save_data_dmd's file: "t uz" per node, uz extrapolated onto the walls."""
+    M, p, g = config0()
+    prof = {k: g[f"prof_{k}"] for k in O.FIELDS}
+    path = tmp_path / "dmd.dat"
+    with ehd.Simulation(to_ehd(p), "fp64") as sim:
+        sim.set_state_seeded(prof, seed=2)
+        sim.step(3)
+        w = sim.get_fields()["w"].copy()
+        sim.write_dmd(path)
+    a = np.loadtxt(path)
+    assert a.shape == (p.nx * p.ny * p.nz, 2)
+    assert np.allclose(a[:, 0], 3 * p.dt, atol=1e-6)
+    w[0] = 2 * w[1] - w[2]
+    w[-1] = 2 * w[-2] - w[-3]
+    assert np.allclose(a[:, 1], w.ravel(), atol=6e-7, rtol=0)
+
+
 def test_run_to_saturation_mechanics():
     """Sampling, hold count and the step budget of ehd_run_to_saturation."""
     M, p, g = config0()
