@@ -236,3 +236,35 @@ def test_params_groups_roundtrip():
         assert abs(g[k] - v) < 1e-9 * v
     ref = O.groups_of(O.reference_default_params())
     assert abs(ref["T"] - 996.0) < 1.0 and abs(ref["M"] - 10) < 1e-9  # LBM.cu:1375-1378
+
+
+def test_column_state_broadcast_evolves_as_the_column_and_its_fields_do_not():
+    """The restatement behind ehd_set_state_from_column, in the reference's own
+    scheme: a 1 x 1 x NZ column's populations broadcast over x, y evolve as the
+    column does; equilibrium populations rebuilt from its fields do not (the
+    injector alternates with period two, and its planes carry non-equilibrium
+    parts the rebuild drops)."""
+    p = O.params_from_groups(4, 4, 9, 0.5, 0.5, T=300, M=10, C=10, Fe=4000,
+                             lambda_f=1.0 / 12.0, lambda_g=1e-6)
+    q = O.Params(**{k: getattr(p, k) for k, _ in O.Params._fields_})
+    q.nx, q.ny, q.lx, q.ly = 1, 1, p.dx, p.dy
+    col = O.Oracle(q)
+    col.initialization()
+    col.step(2000)
+    f = col.get_fields()
+    f0, f1, h0, h1 = col.get_pops()
+    shape = (p.nz, p.ny, p.nx)
+    bc = {k: np.broadcast_to(v, shape) for k, v in f.items()}
+    a = O.Oracle(p)
+    a.set_fields(bc)
+    a.set_pops(np.broadcast_to(f0, shape), np.broadcast_to(f1, (26,) + shape),
+               np.broadcast_to(h0, shape), np.broadcast_to(h1, (26,) + shape))
+    b = O.Oracle(p)
+    b.set_fields(bc)
+    for o in (a, b, col):
+        o.step(50)
+    ref = {k: np.broadcast_to(v, shape) for k, v in col.get_fields().items()}
+    ga, gb = a.get_fields(), b.get_fields()
+    for k in ("rho", "q", "phi"):
+        assert relerr(ga[k], ref[k]) < 1e-12, k
+    assert relerr(gb["q"], ref["q"]) > 1e-3
