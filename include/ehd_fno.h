@@ -2,7 +2,7 @@
  * EHD step from its initial fields and dimensionless groups, as a warm start
  * that skips the linear-growth transient.  No counterpart in the reference
  * (gyf135/EHD-convection-3D has no learned component); the plain step stays
- * the judge of every warm start.
+ * the arbiter of every warm start: each one is run on by the step itself.
  *
  * Architecture (the published Fourier neural operator, Li et al. 2021):
  *   v0 = a P + p                                  (lift, pointwise)
