@@ -241,7 +241,7 @@ def test_diagnostics_match_host_reductions(prec):
 @pytest.mark.parametrize("prec", ["fp16", "bf16"])
 def test_reduced_storage_runs_and_stays_close(prec):
     """FP16/BF16 population storage: finite, and close to FP64 over 200 steps
-    (longer runs are compared per field by the benchmark's accuracy mode)."""
+    (longer runs are compared field by field by precision.py)."""
     _, p, _, f = config0_inputs()
     res = {}
     for pr in ("fp64", prec):
