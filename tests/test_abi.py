@@ -74,6 +74,9 @@ def test_null_arguments_are_errors_not_crashes():
     assert L.ehd_synchronize(None) == -1
     assert L.ehd_diagnostics(None, None) == -1
     assert L.ehd_create(None, None, None) == -1
+    assert L.ehd_hydrostatic_column(None, None, 10, None, None) == -1
+    assert L.ehd_set_state_from_column(None, None, 0, 0.0) == -1
+    assert L.ehd_write_dmd(None, b"x.dat") == -1
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-GPU error path")
