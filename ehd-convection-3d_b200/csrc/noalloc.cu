@@ -29,7 +29,7 @@ namespace {
 
 // The working storage.  In host code this name is a host-side stand-in, not a
 // device address: host code obtains the address with cudaGetSymbolAddress.
-__device__ __align__(256) unsigned char g_noalloc_scratch[EHD_NOALLOC_SCRATCH_BYTES];
+static __device__ __align__(256) unsigned char g_noalloc_scratch[EHD_NOALLOC_SCRATCH_BYTES];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
