@@ -52,13 +52,6 @@ struct DeviceGuard {
     }
 };
 
-bool only_235(int n) {
-    if (n < 1) return false;
-    for (int f : {2, 3, 5})
-        while (n % f == 0) n /= f;
-    return n == 1;
-}
-
 FftPlan make_plan(int n) {
     FftPlan p{};
     p.n = n;
@@ -67,6 +60,8 @@ FftPlan make_plan(int n) {
     while (n % 2 == 0) { p.rad[p.nrad++] = 2; n /= 2; }
     while (n % 3 == 0) { p.rad[p.nrad++] = 3; n /= 3; }
     while (n % 5 == 0) { p.rad[p.nrad++] = 5; n /= 5; }
+    for (int f = 7; n > 1; f += 2)  // remaining odd primes: direct radix-f passes
+        while (n % f == 0) { p.rad[p.nrad++] = f; n /= f; }
     return p;
 }
 
@@ -155,9 +150,6 @@ int validate(const ehd_params *p) {
     if (!p) return fail(EHD_ERR_INVALID, "params is NULL");
     if (p->nx < 1 || p->ny < 1) return fail(EHD_ERR_INVALID, "nx, ny must be >= 1");
     if (p->nz < 4) return fail(EHD_ERR_INVALID, "nz must be >= 4 (got %d)", p->nz);
-    if (!only_235(p->nx) || !only_235(p->ny))
-        return fail(EHD_ERR_INVALID, "nx and ny must factor into 2, 3 and 5 (got %d, %d)", p->nx,
-                    p->ny);
     if ((long long)p->nx * p->ny * p->nz > (1LL << 31))
         return fail(EHD_ERR_INVALID, "grid too large: nx*ny*nz must be <= 2^31");
     const double pos[] = {p->lx, p->ly, p->lz, p->dx, p->dy, p->dz, p->dt, p->cfl,

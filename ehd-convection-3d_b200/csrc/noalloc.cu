@@ -12,9 +12,14 @@
 // allocating.  It calls no cudaMalloc, cudaFree or other allocating routine,
 // on the device or on the host.
 //
-// The array costs EHD_NOALLOC_SCRATCH_BYTES of device memory on every GPU
-// that loads the library, until the process exits, whether or not the entry
-// point is called.
+// The array costs EHD_NOALLOC_SCRATCH_BYTES of device memory on each GPU the
+// entry point is used on, until the process exits.  Under CUDA's lazy module
+// loading (the default) the driver commits it when the first call on a device
+// looks up its address, so that first call is itself a device allocation by
+// the driver: make it at start-up, before any stream capture.  With
+// CUDA_MODULE_LOADING=EAGER the array is committed on every GPU when the
+// library's module loads.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -33,7 +38,30 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[EHD_NOALLOC_SCR
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
+// per device: the array's address and the context it was looked up in (a
+// cudaDeviceReset makes a new primary context, where the module reloads and
+// the array may move)
 void *g_scratch_addr[kMaxDevices] = {};
+CUcontext g_scratch_ctx[kMaxDevices] = {};
+
+// The calling thread's current driver context, through the runtime's driver
+// entry point (the library links only the runtime).
+CUcontext current_context() {
+    using Fn = CUresult (*)(CUcontext *);
+    static Fn fn = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult st{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &st) ==
+                cudaSuccess && st == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<Fn>(p);
+        looked_up = true;
+    }
+    CUcontext c = nullptr;
+    if (fn && fn(&c) != CUDA_SUCCESS) c = nullptr;
+    return c;
+}
 
 size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 
@@ -144,18 +172,29 @@ extern "C" int ehd_poisson_noalloc(const ehd_params *p, const double *q, double 
     if ((size_t)2 * nx * 16 > 200 * 1024 || (size_t)2 * ny * 16 > 200 * 1024)
         return set_error(EHD_ERR_INVALID, "ehd_poisson_noalloc: nx or ny too large");
 
+    {
+        // an error left pending by the caller's earlier work is reported as
+        // such, and left pending (not consumed by this call's launch checks)
+        const cudaError_t pending = cudaPeekAtLastError();
+        if (pending != cudaSuccess)
+            return set_error(EHD_ERR_CUDA, "ehd_poisson_noalloc: a CUDA error from earlier work "
+                                           "is pending; nothing was launched");
+    }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
         return set_error(EHD_ERR_CUDA, "ehd_poisson_noalloc: no usable current device");
     unsigned char *base = nullptr;
     {
-        // first call on this device: the device address of the array
+        // first call on this device (in this context): the device address of
+        // the array
         std::lock_guard<std::mutex> lk(g_mu);
-        if (!g_scratch_addr[dev]) {
+        const CUcontext ctx = current_context();
+        if (!g_scratch_addr[dev] || g_scratch_ctx[dev] != ctx) {
             void *ptr = nullptr;
             if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr)
                 return set_error(EHD_ERR_CUDA, "ehd_poisson_noalloc: cudaGetSymbolAddress failed");
             g_scratch_addr[dev] = ptr;
+            g_scratch_ctx[dev] = ctx;
         }
         base = (unsigned char *)g_scratch_addr[dev];
     }

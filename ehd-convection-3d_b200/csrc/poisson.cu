@@ -34,8 +34,9 @@
 //
 // FFTs: for N = 64, 128, 256, 512 the x and y transforms use compile-time
 // Stockham passes of radix 8/16 (fft.cuh), two real x-rows packed into one
-// complex transform; other sizes of the form 2^a 3^b 5^c use run-time
-// radix-2/3/4/5 passes.  Twiddles come from an FP64-accurate table.
+// complex transform; other sizes use run-time passes of radix 2/3/4/5 and,
+// for any other prime factor p, a direct radix-p pass over symmetric pairs
+// of outputs.  Twiddles come from an FP64-accurate table.
 #include <cmath>
 
 #include "common.cuh"
@@ -77,6 +78,64 @@ __device__ typename Cplx<R>::T *fft_smem(typename Cplx<R>::T *a, typename Cplx<R
         const int nb = N / Rr;
         const int tstep = N / (Ns * Rr);
         const int total = batch * nb;
+        if (Rr > 5) {
+            // Odd prime radix p: the inputs are twiddled in place first, then
+            // each work item forms one pair of outputs (q, p - q) from the
+            // symmetric sums s_r = x_r + x_{p-r} and differences
+            // d_r = x_r - x_{p-r}:  out_q = A + i sign B, out_{p-q} = A - i sign B,
+            // A = x_0 + sum_r s_r cos(2 pi r q / p), B = sum_r d_r sin(2 pi r q / p),
+            // r = 1..(p-1)/2; item q = 0 forms the plain sum.
+            for (int t = tid; t < batch * N; t += nthr) {
+                const int line = t / N, e = t - line * N;
+                const int r = e / nb, j = e - r * nb;
+                const int k = j % Ns;
+                if (r > 0 && k > 0) {
+                    R2 w = __ldg(tw + r * k * tstep);
+                    w.y *= -sign;
+                    a[t] = cmul(a[t], w);
+                }
+            }
+            __syncthreads();
+            const int h = Rr / 2;
+            const int per = nb * (h + 1);
+            const int pstep = N / Rr;  // table index of exp(-2 pi i / p)
+            for (int t = tid; t < batch * per; t += nthr) {
+                const int line = t / per, rem = t - line * per;
+                const int j = rem / (h + 1), qq = rem - j * (h + 1);
+                const int k = j % Ns;
+                const R2 *in = a + (size_t)line * N;
+                R2 *out = b + (size_t)line * N;
+                const int base = (j / Ns) * Ns * Rr + k;
+                const R2 x0 = in[j];
+                if (qq == 0) {
+                    R2 sum = x0;
+                    for (int r = 1; r < Rr; ++r) sum = cadd(sum, in[j + r * nb]);
+                    out[base] = sum;
+                } else {
+                    R2 A = x0, B = R2{(R)0, (R)0};
+                    int m = qq;  // r qq mod p
+                    for (int r = 1; r <= h; ++r) {
+                        const R2 xr = in[j + r * nb], xm = in[j + (Rr - r) * nb];
+                        const R2 w = __ldg(tw + m * pstep);  // (cos, -sin) of 2 pi m / p
+                        A.x += (xr.x + xm.x) * w.x;
+                        A.y += (xr.y + xm.y) * w.x;
+                        B.x -= (xr.x - xm.x) * w.y;
+                        B.y -= (xr.y - xm.y) * w.y;
+                        m += qq;
+                        if (m >= Rr) m -= Rr;
+                    }
+                    const R2 iB = cis(B, sign);
+                    out[base + qq * Ns] = cadd(A, iB);
+                    out[base + (Rr - qq) * Ns] = csub(A, iB);
+                }
+            }
+            __syncthreads();
+            R2 *tsw = a;
+            a = b;
+            b = tsw;
+            Ns *= Rr;
+            continue;
+        }
         for (int t = tid; t < total; t += nthr) {
             const int line = t / nb;
             const int j = t - line * nb;
@@ -143,7 +202,7 @@ __device__ typename Cplx<R>::T *fft_smem(typename Cplx<R>::T *a, typename Cplx<R
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// run-time radix kernels (any 2^a 3^b 5^c)
+// run-time radix kernels (any size)
 // ---------------------------------------------------------------------------
 
 // K1: s' = -(q - q_m)/eps on the planes z = 1..NZ-2 (odd_extension's interior

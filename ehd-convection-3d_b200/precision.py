@@ -3,6 +3,15 @@ FP16 or BF16 storage, compared field by field (max-norm error relative to the
 FP64 field's largest magnitude) and diagnostic by diagnostic (relative error of
 Nu_e, kinetic energy and total charge), at several step counts.
 
+Every one of the nine fields is reported on its own scale.  Two vector forms
+are reported beside them: the velocity (u, v, w) and the field (Ex, Ey, Ez),
+each component's error relative to the largest component of its vector.  A
+component that vanishes in exact arithmetic (u and v of a flow that is still
+almost z-directed, Ex and Ey of a charge that is still almost x,y-uniform)
+carries only round-off and noise on its own scale, which the raw per-field
+number shows and the vector number puts on the scale of the vector.  rho is
+also reported against its deviation scale max|rho - rho0| ("rho_dev").
+
 Every run starts from the same state: the hydrostatic column (its own state,
 or equilibria rebuilt from its fields with --start fields) plus the seeded
 velocity perturbation.  Nu_e is the two-step mean of the saturation loop.
@@ -21,13 +30,20 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE))
 
-FIELDS = ("rho", "u", "v", "w", "q", "phi", "ez")
+FIELDS = ("rho", "u", "v", "w", "q", "phi", "ex", "ey", "ez")
+VECTORS = {"vel": ("u", "v", "w"), "E": ("ex", "ey", "ez")}
 DIAGS = ("nu_e", "kinetic_energy", "total_charge")
 
 
 def relerr(a: np.ndarray, b: np.ndarray) -> float:
     s = float(np.abs(b).max())
     return float(np.abs(a - b).max() / (s if s > 0 else 1.0))
+
+
+def vec_err(a: dict, b: dict, comps) -> float:
+    """Largest component error relative to the largest component of b."""
+    s = max(float(np.abs(b[k]).max()) for k in comps)
+    return max(float(np.abs(a[k] - b[k]).max()) for k in comps) / (s if s > 0 else 1.0)
 
 
 def transit_steps(p, transits: float) -> int:
@@ -64,12 +80,16 @@ def run(ehd, p, precisions, steps, seed=0, amp=1e-3, transits=16.0, start="colum
             snap = {}
             for prec, sim in sims.items():
                 d = sim.step_sampled(s - done) if s > done else sim.diagnostics()
-                snap[prec] = (sim.get_fields(FIELDS[:6] + ("ez",)), d)
+                snap[prec] = (sim.get_fields(FIELDS), d)
             done = s
             ref_f, ref_d = snap["fp64"]
             for prec in precisions:
                 f, d = snap[prec]
                 row = {k: relerr(f[k], ref_f[k]) for k in FIELDS}
+                for v, comps in VECTORS.items():
+                    row[v] = vec_err(f, ref_f, comps)
+                dev = float(np.abs(ref_f["rho"] - p.rho0).max())
+                row["rho_dev"] = float(np.abs(f["rho"] - ref_f["rho"]).max()) / (dev if dev > 0 else 1.0)
                 for k in DIAGS:
                     row[k] = abs(d[k] - ref_d[k]) / max(abs(ref_d[k]), 1e-300)
                 row["nonfinite"] = int(d["nonfinite"])
@@ -81,7 +101,7 @@ def run(ehd, p, precisions, steps, seed=0, amp=1e-3, transits=16.0, start="colum
 
 
 def markdown(res) -> str:
-    cols = ("rho", "w", "q", "phi", "ez") + DIAGS
+    cols = FIELDS + ("vel", "E", "rho_dev") + DIAGS
     head = "| storage | step | " + " | ".join(cols) + " |"
     lines = [head, "|" + "---|" * (len(cols) + 2)]
     for prec, by_step in res.items():

@@ -301,8 +301,11 @@ int ehd_abi_version(void);
 
 /* --- no device allocation -------------------------------------------------- */
 
-/* Bytes of device memory held, on every GPU that loads this library, by the
- * file-scope working array of ehd_poisson_noalloc, until the process exits. */
+/* Bytes of device memory held by the file-scope working array of
+ * ehd_poisson_noalloc on each GPU it is used on, until the process exits.
+ * Under CUDA's lazy module loading (the default) the driver commits the array
+ * at the first call on a device; with CUDA_MODULE_LOADING=EAGER, on every GPU
+ * when the library loads. */
 #define EHD_NOALLOC_SCRATCH_BYTES (64u << 20)
 
 /* No counterpart in the reference.  For callers that cannot allocate device
@@ -314,12 +317,15 @@ int ehd_abi_version(void);
  * cudaFree or other allocating routine; its working storage is one
  * file-scope device array of EHD_NOALLOC_SCRATCH_BYTES, so grids whose
  * working set exceeds it are rejected with EHD_ERR_INVALID (about
- * 128 x 128 x 129 nodes fit).  The first call on each device looks up the
- * array's device address; make that first call before any stream capture.
- * All calls on a device share the array and each call leaves its contents
- * behind: calls whose GPU work overlaps (different streams, host threads)
- * race on it.  Runs on `stream` (NULL: the legacy default stream) on the
- * current device; asynchronous. */
+ * 128 x 128 x 129 nodes fit).  The first call on each device (and again
+ * after a cudaDeviceReset) looks up the array's device address, which under
+ * lazy module loading is when the driver commits the array: make that first
+ * call at start-up, before any stream capture.  A CUDA error already pending
+ * from the caller's earlier work is returned as EHD_ERR_CUDA before anything
+ * is launched, and left pending.  All calls on a device share the array and
+ * each call leaves its contents behind: calls whose GPU work overlaps
+ * (different streams, host threads) race on it.  Runs on `stream` (NULL: the
+ * legacy default stream) on the current device; asynchronous. */
 int ehd_poisson_noalloc(const ehd_params *params, const double *q, double *phi, double *ex,
                         double *ey, double *ez, void *stream);
 

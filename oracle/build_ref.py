@@ -15,7 +15,9 @@ except, in every case:
 
 * NSTEPS is read from the environment variable EHD_REF_NSTEPS (LBM.h:82);
 * NSAVE = NDMD = printCurrent = 1, so ``i % N == 1`` never fires and the
-  time loop runs without in-loop output (main.cu:210-237);
+  time loop runs without in-loop output (main.cu:210-237); a case may keep
+  the collector-current print (``Current = %g`` every printCurrent steps,
+  main.cu:227-231) at a cadence of its own;
 * flag (LBM.h:30) selects the restart path (read data_end.dat) or the
   reference initialisation;
 * save_data_end writes %.17g instead of %10.6f (LBM.cu:1551) so the output
@@ -24,8 +26,10 @@ except, in every case:
 and, for the timing-only case "bench", the whole-field text writers outside
 the timed loop (main.cu:168,268,273,277) are skipped.
 
-The GPU machine has no /root/reference; the binaries built here travel with
-the repository snapshot.  Run:  python oracle/build_ref.py [case ...]
+The reference sources are read from $EHD_REFERENCE_SRC, by default
+/root/reference.  The GPU machine has no reference sources; the binaries built
+here travel with the repository snapshot.
+Run:  python oracle/build_ref.py [case ...]
 """
 from __future__ import annotations
 
@@ -39,7 +43,7 @@ import tempfile
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF_SRC = Path("/root/reference")
+REF_SRC = Path(os.environ.get("EHD_REFERENCE_SRC", "/root/reference"))
 OUT = HERE / "_ref"
 
 # name -> constants.  Geometry: dx = dy = dz = 1/(nz-1), Lx = nx dx, Ly = ny dy.
@@ -62,6 +66,12 @@ CASES = {
                          charge0=10.0, diffu=6.25e-5, V=1.0 / 12.0, VC=1.0e-6),
     # timing only: 256 x 256 x 129, reference initialisation, no text output
     "bench": dict(nx=256, ny=256, nz=129, threads=128, flag=0, no_output=True, **_GROUPS),
+    # the reference's own default case (LBM.h:31-86: 122 x 122 x 101, dx = 1/100,
+    # T ~ 996, M = 10, C = 10, Fe = 4000, magic parameters 1/12 and 1e-6),
+    # started from data_end.dat, printing the collector current every 1000
+    # steps as it does by default (main.cu:227-231); no whole-field output
+    "authors": dict(nx=122, ny=122, nz=101, threads=61, flag=1, no_output=True,
+                    print_current=1000, **_DEFAULT),
 }
 
 
@@ -107,7 +117,7 @@ def patch(src_dir: Path, c: dict) -> None:
              '(unsigned)atoi(getenv("EHD_REF_NSTEPS") ? getenv("EHD_REF_NSTEPS") : "1")')
     h = _sub(h, r"const unsigned int NSAVE ", "1")
     h = _sub(h, r"const unsigned int NDMD  ", "1")
-    h = _sub(h, r"const unsigned int printCurrent", "1")
+    h = _sub(h, r"const unsigned int printCurrent", str(int(c.get("print_current", 1))))
     (src_dir / "LBM.h").write_text(h)
 
     cu = (src_dir / "LBM.cu").read_text()

@@ -143,12 +143,9 @@ def collect(indir: Path) -> None:
         for n in steps:
             a = np.load(indir / f"{name}_{n}_0.npz")
             b = np.load(indir / f"{name}_{n}_1.npz")
-            keep = O.FIELDS if name != "config0" else ("u", "v", "w", "q", "phi")
-            dt = np.float64 if name != "config0" else np.float32
-            if name == "config0" and n != steps[-1]:
-                keep = ("u", "w", "q", "phi")
-            for k in keep:
-                pack[f"out{n}_{k}"] = a[k].astype(dt)
+            # every field in FP64 (the reference's data_end.dat, %.17g)
+            for k in O.FIELDS:
+                pack[f"out{n}_{k}"] = a[k].astype(np.float64)
                 scale = max(np.abs(a[k]).max(), 1e-300)
                 pack[f"spread{n}_{k}"] = np.float64(np.abs(a[k] - b[k]).max() / scale)
             pack[f"current{n}"] = np.float64(O.current_of(p, a["q"], a["ez"]))

@@ -47,7 +47,7 @@ def test_params_from_groups_matches_reference_formula():
     assert g["T"] == pytest.approx(200) and g["Fe"] == pytest.approx(4000)
 
 
-@pytest.mark.parametrize("bad", [dict(nz=3), dict(nx=7), dict(ny=0), dict(dt=0.0), dict(nu=-1.0),
+@pytest.mark.parametrize("bad", [dict(nz=3), dict(nx=-4), dict(ny=0), dict(dt=0.0), dict(nu=-1.0),
                                  dict(lambda_g=0.0), dict(pad_=1), dict(nx=1 << 16, ny=1 << 16)])
 def test_create_rejects_bad_params(bad):
     p = ehd.params_from_groups(16, 16, 9, 2.0, 2.0, T=200, M=10, C=10, Fe=4000)
@@ -77,6 +77,8 @@ def test_null_arguments_are_errors_not_crashes():
     assert L.ehd_hydrostatic_column(None, None, 10, None, None) == -1
     assert L.ehd_set_state_from_column(None, None, 0, 0.0) == -1
     assert L.ehd_write_dmd(None, b"x.dat") == -1
+    # checked before any CUDA call
+    assert L.ehd_poisson_noalloc(None, None, None, None, None, None, None) == -1
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-GPU error path")

@@ -89,10 +89,13 @@ def random_fields(p, seed):
     return M.random_fields(p, seed)
 
 
-@pytest.mark.parametrize("shape", [(16, 12, 9), (48, 20, 11), (30, 25, 7), (1, 1, 17)])
+@pytest.mark.parametrize("shape", [(16, 12, 9), (48, 20, 11), (30, 25, 7), (1, 1, 17),
+                                   (22, 14, 9), (122, 122, 101)])
 def test_step_halves_match_oracle(shape):
     """The LBM half (stream_collide_save) and the Poisson half, separately and
-    then chained, against the oracle on grids with radix 2, 3 and 5 factors."""
+    then chained, against the oracle on grids with radix 2, 3 and 5 factors,
+    other primes (22 = 2 x 11, 14 = 2 x 7), and the reference's own default
+    grid 122 x 122 x 101 (LBM.h:34-36: 122 = 2 x 61, Thomas z solve)."""
     nx, ny, nz = shape
     dz = 1.0 / (nz - 1)
     p = O.params_from_groups(nx, ny, nz, nx * dz, ny * dz, T=200, M=10, C=10, Fe=4000,
@@ -123,12 +126,15 @@ def test_step_halves_match_oracle(shape):
 
 
 @pytest.mark.parametrize("shape", [(256, 128, 9), (128, 256, 7), (512, 64, 5), (64, 512, 5),
-                                   (256, 96, 6)])
+                                   (256, 96, 6), (122, 122, 7), (14, 77, 5), (61, 26, 6),
+                                   (127, 13, 5)])
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-11), ("fp32", 2e-6)])
 def test_poisson_fft_sizes_match_oracle(shape, prec, tol):
     """The compile-time-radix FFT paths (N = 64..512, two real rows per
-    transform) and the run-time radix path, against the oracle's
-    odd-extension DFT solve (poisson.cu:78-167) on random charge."""
+    transform) and the run-time radix path (radix 2/3/4/5 and the direct
+    radix-p passes for other primes: 122 = 2 x 61, the reference's own grid
+    width, LBM.h:34-35; 77 = 7 x 11; prime and odd widths), against the
+    oracle's odd-extension DFT solve (poisson.cu:78-167) on random charge."""
     nx, ny, nz = shape
     dz = 1.0 / (nz - 1)
     p = O.params_from_groups(nx, ny, nz, nx * dz, ny * dz, T=200, M=10, C=10, Fe=4000)

@@ -8,8 +8,9 @@ array.  This test calls it through the C ABI twice in a row, on two different
 charge fields, and checks each result against the context entry points
 (ehd_set_fields + ehd_poisson + ehd_get_fields) with the FP64 tolerance of the
 other Poisson tests.  The second call checks that nothing left in the shared
-array by the first call leaks into the next result.  Collected last on
-purpose.
+array by the first call leaks into the next result, and that it allocates
+nothing: the device's free memory and torch's reserved memory are the same
+before and after it.  Collected last on purpose.
 """
 import ctypes
 
@@ -46,11 +47,15 @@ def test_poisson_noalloc_matches_context_path_twice():
             ref = sim.get_fields()
         q = torch.from_numpy(np.ascontiguousarray(f["q"])).cuda()
         out = {k: torch.full_like(q, float("nan")) for k in ("phi", "ex", "ey", "ez")}
+        torch.cuda.synchronize()
+        before = (torch.cuda.mem_get_info()[0], torch.cuda.memory_reserved())
         rc = ehd.lib().ehd_poisson_noalloc(ctypes.byref(pe), q.data_ptr(),
                                            out["phi"].data_ptr(), out["ex"].data_ptr(),
                                            out["ey"].data_ptr(), out["ez"].data_ptr(), None)
         torch.cuda.synchronize()
         assert rc == 0, ehd.lib().ehd_last_error()
+        if seed == 12:  # the array is committed by the first call; later calls allocate nothing
+            assert (torch.cuda.mem_get_info()[0], torch.cuda.memory_reserved()) == before
         mine = {k: v.cpu().numpy() for k, v in out.items()}
         assert relerr(mine["phi"], ref["phi"]) < 1e-11
         assert vec_err(mine, ref, ("ex", "ey", "ez")) < 1e-11
