@@ -536,6 +536,55 @@ def run_reference_saturation(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args, rank, local_rank):
+    """The batched T-sweep's step rate: 64 instances with T uniform in
+    [100, 400] (seed 0), nz cells from {24, 32, 40, 48}, NX = NY = 2 nz, the
+    reference's magic parameters, each from its hydrostatic column's state plus
+    its own seeded noise, stepped together (ehd_batch_step).  MLUPS of the
+    whole batch: all instances' nodes per batch step over the time of a batch
+    step (device synchronised on both sides of K steps, wall clock)."""
+    if rank != 0:
+        return
+    import torch
+
+    ehd = load_ehd()
+    sys.path.insert(0, str(PKG))
+    import sweep
+
+    torch.cuda.set_device(local_rank)
+    insts = sweep.make_instances(64, 0)
+    params = [sweep.instance_params(ehd, s) for s in insts]
+    nodes = sum(p.nx * p.ny * p.nz for p in params)
+    cols, starts = sweep.hydrostatic_columns(
+        ehd, params, [sweep.hydrostatic_steps(p, 1.0) for p in params], device=local_rank)
+    K, W = args.steps, args.warmup
+    with ehd.Batch(params, args.precision, device=local_rank) as b:
+        if args.autotune:
+            b.autotune(trial_steps=10)
+        for sim, s, (col, i0) in zip(b, insts, starts):
+            sim.set_state_from_column(col, seed=s["seed"], amp=1e-3)
+            sim.set_reference_current(i0)
+        for cb in cols:
+            cb.close()
+        b.step(W)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.step(K)
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+        nonfinite = sum(int(sim.diagnostics()["nonfinite"] != 0) for sim in b)
+    line = {"metric": "MLUPS of a batched 64-instance T-sweep (uneven grids)",
+            "value": round(K * nodes / sec / 1e6, 1), "unit": "MLUPS", "n_gpus": 1,
+            "steps": K, "warmup": W, "ms_per_step": round(1e3 * sec / K, 4),
+            "higher_is_better": True, "dtype": args.precision, "vs_baseline": None,
+            "data": "synthetic: hydrostatic column states + seeded 1e-3 velocity noise",
+            "config": {"workload": "64 instances, T~U[100,400], nz in {24,32,40,48}, "
+                                   "NX=NY=2nz, TRT 1/12 and 1e-6", "nodes": nodes,
+                       "autotune": bool(args.autotune)},
+            "nonfinite_instances": nonfinite}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -551,9 +600,11 @@ def main():
                     help="storage of the headline run (profiling)")
     ap.add_argument("--grid", type=int, nargs=3, metavar=("NX", "NY", "NZ"),
                     help="smaller grid for profiling captures; not a bench line")
-    ap.add_argument("--workload", default="step", choices=["step", "saturation"],
+    ap.add_argument("--workload", default="step", choices=["step", "saturation", "batch"],
                     help="step: MLUPS of the full step (the default line); saturation: wall "
-                         "time to saturated Nu_e on the reference's default case")
+                         "time to saturated Nu_e on the reference's default case; batch: "
+                         "the 64-instance batched T-sweep's step rate")
+    ap.add_argument("--autotune", action="store_true", help="batch workload: autotune first")
     ap.add_argument("--sat-max-steps", type=int, default=6_000_000)
     ap.add_argument("--ref-window", type=int, default=20_000,
                     help="reference arm of the saturation workload: steps it runs")
@@ -570,7 +621,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.workload == "saturation":
+    if args.workload == "batch":
+        run_batch(args, rank, local_rank)
+    elif args.workload == "saturation":
         if args.impl == "reference":
             run_reference_saturation(args, rank)
         else:

@@ -508,6 +508,7 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
     pa.ny = ny;
     pa.nz = nz;
     pa.nxh = nx / 2 + 1;
+    pa.split = 1;
     pa.pitch = (pa.nxh + 15) / 16 * 16;
     const size_t c2 = 2 * c->rsize;  // complex compute type
     {
@@ -557,6 +558,11 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
     pa.eps = params->eps;
     pa.voltage = params->voltage;
     pa.dz = params->dz;
+    {
+        cudaError_t e = c->rsize == 8 ? prepare_poisson<double>(pa) : prepare_poisson<float>(pa);
+        if (e != cudaSuccess)
+            return bail(fail(EHD_ERR_CUDA, "Poisson set-up: %s", cudaGetErrorString(e)));
+    }
     {
         auto table = [&](int N, void *dst) -> cudaError_t {
             std::vector<double> t(2 * (size_t)N);
@@ -664,6 +670,8 @@ int ehd_get_tuning(const ehd_ctx *c, ehd_tuning *t) {
 int ehd_set_tuning(ehd_ctx *c, const ehd_tuning *t) {
     if (!c || !t) return fail(EHD_ERR_INVALID, "NULL argument");
     if (t->lbm_kernel != 0 && t->lbm_kernel != 1) return fail(EHD_ERR_INVALID, "lbm_kernel must be 0 or 1");
+    if (t->poisson_path != 0 && t->poisson_path != 1)
+        return fail(EHD_ERR_INVALID, "poisson_path must be 0 or 1");
     const int bx = t->node_block_x;
     if (bx != 16 && bx != 32 && bx != 64 && bx != 128)
         return fail(EHD_ERR_INVALID, "node_block_x must be 16, 32, 64 or 128 (got %d)", bx);
@@ -682,6 +690,7 @@ int ehd_set_tuning(ehd_ctx *c, const ehd_tuning *t) {
     c->psum_blocks = lbm_blocks_per_plane(c->p.nx, c->p.ny, bx);
     c->pa.rows_per_block = t->fft_rows;
     c->pa.cols_per_block = t->fft_cols;
+    c->pa.split = t->poisson_path == 0 ? 1 : 0;
     return EHD_OK;
 }
 

@@ -101,6 +101,7 @@ struct FftPlan {
 // [z-1][ky][kx] with kx pitch `pitch`; the z solve works on it in place.
 struct PoissonArgs {
     int nx, ny, nz, nxh, pitch;
+    int split;           // 1: the split-y three-kernel path where it applies
     int rows_per_block;  // x-row FFT batch per block (run-time radix path)
     int cols_per_block;  // y-column FFT batch per block (run-time radix path)
     FftPlan px, py;
@@ -123,6 +124,10 @@ struct PoissonArgs {
 
 template <typename R>
 cudaError_t launch_poisson(const PoissonArgs &a, cudaStream_t s);
+// sets the shared-memory attributes of the kernels a's grid will use (call
+// before any stream capture)
+template <typename R>
+cudaError_t prepare_poisson(const PoissonArgs &a);
 
 bool poisson_fast_size(int n);
 

@@ -752,6 +752,373 @@ poisson_zdst(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::T *
 }
 
 // ---------------------------------------------------------------------------
+// split-y path: three launches instead of five
+// ---------------------------------------------------------------------------
+//
+// For NY = 64 S (S = 1, 2, 4, 8) the y transform of length NY is split as
+// y = n + 64 m (n < 64, m < S), ky = S k' + j (k' < 64, j < S):
+//   forward   Y[S k' + j] = FFT64_n( a_j[n] )[k'],
+//             a_j[n] = W_NY^(j n) sum_m x[n + 64 m] W_S^(j m)
+//   inverse   x[n + 64 m] = sum_j W_S^(-j m) b_j[n],
+//             b_j[n] = W_NY^(-j n) IFFT64_k'( Y[S k' + j] )[n]
+// (W_N = exp(-2 pi i / N)).  The x-row kernels form a_j (after the forward x
+// transform) and consume b_j (before the inverse one); in between one slab
+// kernel per (kx, j) holds a_j for every plane z on chip and runs the forward
+// FFT64 along n, the sine-transform z solve of each of its 64 modes, and the
+// inverse FFT64, so the spectrum goes through L2 twice instead of four times.
+// The split spectrum is laid out [j][kx][z - 1][n], so that a slab is one
+// contiguous block.
+namespace {
+
+// rows (ya, yb) of transform tr of a split-row block (two real rows per
+// complex transform): S = 1 pairs consecutive rows; S >= 2 pairs
+// n + 64 a and n + 64 (a + S/2) of group n = block * GB + tr / (S/2)
+template <int S, int TB>
+__device__ __forceinline__ void split_rows(int tr, int &ya, int &yb, int &g, int &a) {
+    if constexpr (S == 1) {
+        g = 2 * tr;
+        a = 0;
+        ya = blockIdx.x * 2 * TB + 2 * tr;
+        yb = ya + 1;
+    } else {
+        constexpr int GB = 2 * TB / S;
+        g = tr / (S / 2);
+        a = tr - g * (S / 2);
+        ya = blockIdx.x * GB + g + 64 * a;
+        yb = ya + 32 * S;
+    }
+}
+
+// x-spectrum of row part (0: ya, 1: yb) of a packed transform at bin k < nxh
+template <typename R2, typename R>
+__device__ __forceinline__ R2 unpack_bin(const R2 *buf, int k, int part, int N) {
+    const R2 zk = buf[fft::pad(k)];
+    const R2 zn = buf[fft::pad((N - k) & (N - 1))];
+    return part == 0 ? R2{(R)0.5 * (zk.x + zn.x), (R)0.5 * (zk.y - zn.y)}
+                     : R2{(R)0.5 * (zk.y + zn.y), (R)0.5 * (zn.x - zk.x)};
+}
+
+}  // namespace
+
+// K1 of the split path: s' = -(q - q_m)/eps, x-FFT of two real rows per
+// transform, FP64 row sums, then the radix-S first stage of the y transform,
+// written as a_j[n] into spl[j][kx][z - 1][n].
+template <typename R, int N, int S>
+__global__ void __launch_bounds__(256)
+poisson_rows_fwd_split(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spl,
+                       double *__restrict__ rowsum, const typename Cplx<R>::T *__restrict__ tw,
+                       const typename Cplx<R>::T *__restrict__ twy,
+                       const double *__restrict__ qmean, int nzi, int nxh, double eps) {
+    using R2 = typename Cplx<R>::T;
+    constexpr int G = fft::Plan<N>::G, TB = per_block<N>(), P = tstride<N>();
+    constexpr int NY = 64 * S, GB = 2 * TB / S;
+    static_assert(GB >= 1, "a block holds whole row groups");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *tws = reinterpret_cast<R2 *>(smem_raw);
+    R2 *buf = tws + N;
+    const int zi = blockIdx.y;
+    const int tid = threadIdx.x;
+    const R *qp = q + (size_t)N * NY * (zi + 1);
+    const R qm = (R)qmean[2 * (zi + 1) + 1];
+    const R ieps = (R)(1.0 / eps);
+    load_twiddles<R, N>(tws, tw);
+    {
+        constexpr int IT = TB * N / 256;
+        R va[IT], vb[IT];
+#pragma unroll
+        for (int r = 0; r < IT; ++r) {
+            const int i = tid + 256 * r;
+            const int tr = i / N, x = i - tr * N;
+            int ya, yb, g, a;
+            split_rows<S, TB>(tr, ya, yb, g, a);
+            va[r] = qp[(size_t)N * ya + x];
+            vb[r] = qp[(size_t)N * yb + x];
+        }
+#pragma unroll
+        for (int r = 0; r < IT; ++r) {
+            const int i = tid + 256 * r;
+            const int tr = i / N, x = i - tr * N;
+            buf[tr * P + fft::pad(x)] = R2{-(va[r] - qm) * ieps, -(vb[r] - qm) * ieps};
+        }
+    }
+    {  // FP64 row sums, one warp per row, fixed order
+        const int warp = tid >> 5, lane = tid & 31;
+        for (int r = warp; r < 2 * TB; r += 8) {
+            int ya, yb, g, a;
+            split_rows<S, TB>(r >> 1, ya, yb, g, a);
+            const int y = (r & 1) ? yb : ya;
+            double sum = 0.0;
+            for (int x = lane; x < N; x += 32) sum += (double)qp[(size_t)N * y + x] - (double)qm;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            if (lane == 0) rowsum[(size_t)zi * NY + y] = -sum / eps;
+        }
+    }
+    __syncthreads();
+    {
+        const int tr = tid / G, jj = tid - tr * G;
+        fft::Plan<N>::template run<-1>(buf + tr * P, tws, jj);
+    }
+    // outputs (j, kx, g), g fastest: GB consecutive n per (j, kx)
+    const int nblk = S == 1 ? 2 * TB : GB;
+    const int n0 = blockIdx.x * nblk;
+    for (int i = tid; i < S * nxh * nblk; i += 256) {
+        const int g = i % nblk, rest = i / nblk;
+        const int kx = rest % nxh, j = rest / nxh;
+        const int n = n0 + g;
+        R2 acc;
+        if constexpr (S == 1) {
+            acc = unpack_bin<R2, R>(buf + (g >> 1) * P, kx, g & 1, N);
+        } else {
+            acc = R2{(R)0, (R)0};
+#pragma unroll
+            for (int m = 0; m < S; ++m) {
+                const int t = g * (S / 2) + (m < S / 2 ? m : m - S / 2);
+                R2 x = unpack_bin<R2, R>(buf + t * P, kx, m < S / 2 ? 0 : 1, N);
+                if (j * m != 0) x = cmul(x, __ldg(twy + ((j * m) % S) * 64));
+                acc = cadd(acc, x);
+            }
+            if (j * n != 0) acc = cmul(acc, __ldg(twy + (j * n) % NY));
+        }
+        spl[(((size_t)j * nxh + kx) * nzi + zi) * 64 + n] = acc;
+    }
+}
+
+// K2 of the split path, one block per (kx, j): the slab a_j[z - 1][n] of all
+// interior planes in shared memory; FFT64 along n (ky = S k' + j), the
+// sine-transform z solve of each of the 64 modes (as poisson_zdst: odd
+// extension of length L = 2 (NZ - 1), FFT, division by lambda_k + h dz^2,
+// FFT), inverse FFT64, the twiddle W_NY^(-j n), written back in place as b_j.
+// The block (kx, j) = (0, 0) also forms the FP64 plane sums of the source and
+// solves the (0,0) mode in closed form (as poisson_zdst), writing phi00 and
+// its Ez.
+template <typename R, int L, int S>
+__global__ void __launch_bounds__(256)
+poisson_slab(typename Cplx<R>::T *__restrict__ spl, const typename Cplx<R>::T *__restrict__ twy,
+             const typename Cplx<R>::T *__restrict__ twz, const R *__restrict__ lamz,
+             const double *__restrict__ rowsum, double *__restrict__ planesum,
+             const double *__restrict__ qmean, double *__restrict__ phi00,
+             double *__restrict__ ez00, int nx, int nxh, double dz, double eps,
+             double voltage, double kx0, double ky0) {
+    using R2 = typename Cplx<R>::T;
+    constexpr int NY = 64 * S;
+    constexpr int n = L / 2 - 1, nz = n + 2;
+    constexpr int G64 = fft::Plan<64>::G, T64 = 256 / G64, P64 = tstride<64>();
+    constexpr int NR = (n + T64 - 1) / T64 * T64;  // slab rows, whole FFT rounds
+    constexpr int GL = fft::Plan<L>::G, TBZ = 256 / GL, PL = tstride<L>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *tw64 = reinterpret_cast<R2 *>(smem_raw);
+    R2 *twl = tw64 + 64;
+    R2 *slab = twl + L;
+    R2 *zb = slab + NR * P64;
+    __shared__ double mrhs[n], mphi[nz];
+    __shared__ R hdz2[TBZ];
+    const int tid = threadIdx.x;
+    const int kx = blockIdx.x, j = blockIdx.y;
+    const bool mean_block = kx == 0 && j == 0;
+    const double dz2 = dz * dz;
+    R2 *base = spl + ((size_t)j * nxh + kx) * n * 64;
+    for (int i = tid; i < 64; i += 256) tw64[i] = twy[S * i];
+    for (int i = tid; i < L; i += 256) twl[i] = twz[i];
+    for (int i = tid; i < n * 64; i += 256) {
+        const int zi = i >> 6, nn = i & 63;
+        slab[zi * P64 + fft::pad(nn)] = base[i];
+    }
+    for (int i = n * 64 + tid; i < NR * 64; i += 256) {
+        const int zi = i >> 6, nn = i & 63;
+        slab[zi * P64 + fft::pad(nn)] = R2{(R)0, (R)0};
+    }
+    if (mean_block) {
+        // FP64 plane sums of the source (fixed order), then the right-hand
+        // side of the mean mode (poisson.cu:97 for the voltage on z = 1)
+        const int warp = tid >> 5, lane = tid & 31;
+        const double nxy = (double)nx * (double)NY;
+        for (int zi = warp; zi < n; zi += 8) {
+            double sum = 0.0;
+            for (int y = lane; y < NY; y += 32) sum += rowsum[(size_t)zi * NY + y];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            if (lane == 0) {
+                planesum[zi + 1] = sum;
+                double d = sum + nxy * (-(double)(R)qmean[2 * (zi + 1) + 1] / eps);
+                if (zi == 0) d += -voltage / dz2 * nxy;
+                mrhs[zi] = d * dz2;
+            }
+        }
+    }
+    __syncthreads();
+    {
+        const int tr = tid / G64, jj = tid - tr * G64;
+        for (int r0 = 0; r0 < NR; r0 += T64)
+            fft::Plan<64>::template run<-1>(slab + (r0 + tr) * P64, tw64, jj);
+    }
+    // z solve of the modes k' = b0 .. b0 + TBZ - 1
+    constexpr int YS = 256 / TBZ, IT = (n + YS - 1) / YS;
+    const R sc = (R)(dz2 / (double)L);
+    for (int b0 = 0; b0 < 64; b0 += TBZ) {
+        const int t = tid % TBZ, zt = tid / TBZ;
+        const int kp = b0 + t;
+        if (zt == 0) {
+            const int ky = S * kp + j;
+            const double wx = kx * kx0, wy = (ky <= NY / 2 ? ky : ky - NY) * ky0;
+            hdz2[t] = (kx == 0 && ky == 0) ? (R)-1 : (R)((wx * wx + wy * wy) * dz2);
+        }
+#pragma unroll
+        for (int r = 0; r < IT; ++r) {
+            const int zi = zt + YS * r;
+            if (zi < n) {
+                const R2 v = slab[zi * P64 + fft::pad(kp)];
+                zb[t * PL + fft::pad(zi + 1)] = v;
+                zb[t * PL + fft::pad(L - 1 - zi)] = R2{-v.x, -v.y};
+            }
+        }
+        if (tid < TBZ) {
+            zb[tid * PL + fft::pad(0)] = R2{(R)0, (R)0};
+            zb[tid * PL + fft::pad(L / 2)] = R2{(R)0, (R)0};
+        }
+        __syncthreads();
+        const int tr = tid / GL, jj = tid - tr * GL;
+        fft::Plan<L>::template run<-1>(zb + tr * PL, twl, jj);
+#pragma unroll
+        for (int u = 0; u < L / GL; ++u) {
+            const int k = jj + GL * u;
+            R2 &yv = zb[tr * PL + fft::pad(k)];
+            const R h = hdz2[tr];
+            if (k == 0 || k == L / 2 || h < (R)0) {
+                yv = R2{(R)0, (R)0};
+            } else {
+                const R f = rcp(lamz[k < L / 2 ? k : L - k] + h);
+                yv = R2{yv.x * f, yv.y * f};
+            }
+        }
+        __syncthreads();
+        fft::Plan<L>::template run<-1>(zb + tr * PL, twl, jj);
+#pragma unroll
+        for (int r = 0; r < IT; ++r) {
+            const int zi = zt + YS * r;
+            if (zi < n) {
+                const R2 w = zb[t * PL + fft::pad(zi + 1)];
+                slab[zi * P64 + fft::pad(kp)] = R2{w.x * sc, w.y * sc};
+            }
+        }
+        __syncthreads();
+    }
+    {
+        const int tr = tid / G64, jj = tid - tr * G64;
+        for (int r0 = 0; r0 < NR; r0 += T64)
+            fft::Plan<64>::template run<1>(slab + (r0 + tr) * P64, tw64, jj);
+    }
+    for (int i = tid; i < n * 64; i += 256) {
+        const int zi = i >> 6, nn = i & 63;
+        R2 v = slab[zi * P64 + fft::pad(nn)];
+        if (j * nn != 0) {
+            R2 w = __ldg(twy + (j * nn) % NY);
+            w.y = -w.y;
+            v = cmul(v, w);
+        }
+        base[i] = v;
+    }
+    if (mean_block) {
+        const double nxy = (double)nx * (double)NY;
+        for (int i = tid; i < nz; i += 256) {
+            double x = 0.0;
+            if (i == 0) {
+                x = voltage;
+            } else if (i < nz - 1) {
+                for (int jz = 1; jz <= n; ++jz) {
+                    const int lo = i < jz ? i : jz, hi = i < jz ? jz : i;
+                    x -= (double)(lo * (n + 1 - hi)) * mrhs[jz - 1];
+                }
+                x = x / (double)(n + 1) / nxy;
+            }
+            mphi[i] = x;
+            phi00[i] = x;
+        }
+        __syncthreads();
+        for (int z = tid; z < nz; z += 256) {
+            const int zc = z < 1 ? 1 : (z > nz - 2 ? nz - 2 : z);
+            ez00[z] = 0.5 * (mphi[zc - 1] - mphi[zc + 1]) / dz;
+        }
+    }
+}
+
+// K3 of the split path: x[n + 64 m] = sum_j W_S^(-j m) b_j[n] from
+// spl[j][kx][z - 1][n], Hermitian completion of two rows per transform,
+// inverse x-FFT, phi' = Re / (NX NY) (odd_extract, poisson.cu:154-167).
+template <typename R, int N, int S>
+__global__ void __launch_bounds__(256)
+poisson_rows_inv_split(const typename Cplx<R>::T *__restrict__ spl, R *__restrict__ phip,
+                       const typename Cplx<R>::T *__restrict__ tw,
+                       const typename Cplx<R>::T *__restrict__ twy, int nzi, int nxh) {
+    using R2 = typename Cplx<R>::T;
+    constexpr int G = fft::Plan<N>::G, TB = per_block<N>(), P = tstride<N>();
+    constexpr int NY = 64 * S, GB = 2 * TB / S;
+    constexpr int NB = S == 1 ? 2 * TB : GB;  // consecutive n per block
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *tws = reinterpret_cast<R2 *>(smem_raw);
+    R2 *buf = tws + N;
+    R2 *bs = buf + TB * P;  // b_j[n0 + g][kx] as bs[(j nxh + kx) NB + g]
+    const int zi = blockIdx.y;
+    const int tid = threadIdx.x;
+    const int n0 = blockIdx.x * NB;
+    load_twiddles<R, N>(tws, tw);
+    for (int i = tid; i < S * nxh * NB; i += 256) {
+        const int g = i % NB, jk = i / NB;
+        bs[i] = spl[((size_t)jk * nzi + zi) * 64 + n0 + g];
+    }
+    __syncthreads();
+    // packed inputs Z = A + i B over the full length
+    for (int i = tid; i < TB * N; i += 256) {
+        const int tr = i / N, k = i - tr * N;
+        int ya, yb, g, a;
+        split_rows<S, TB>(tr, ya, yb, g, a);
+        const int kk = k < nxh ? k : N - k;
+        R2 A, B;
+        if constexpr (S == 1) {
+            A = bs[(size_t)kk * NB + 2 * tr];
+            B = bs[(size_t)kk * NB + 2 * tr + 1];
+        } else {
+            A = R2{(R)0, (R)0};
+            B = R2{(R)0, (R)0};
+            const int ma = a, mb = a + S / 2;
+#pragma unroll
+            for (int j = 0; j < S; ++j) {
+                const R2 v = bs[((size_t)j * nxh + kk) * NB + g];
+                R2 wa = __ldg(twy + ((j * ma) % S) * 64), wb = __ldg(twy + ((j * mb) % S) * 64);
+                wa.y = -wa.y;  // W_S^(-j m)
+                wb.y = -wb.y;
+                A = cadd(A, cmul(v, wa));
+                B = cadd(B, cmul(v, wb));
+            }
+        }
+        if (kk == 0 || kk == N / 2) {
+            A.y = 0;
+            B.y = 0;
+        }
+        if (k >= nxh) {
+            A.y = -A.y;
+            B.y = -B.y;
+        }
+        buf[tr * P + fft::pad(k)] = R2{A.x - B.y, A.y + B.x};
+    }
+    __syncthreads();
+    {
+        const int tr = tid / G, jj = tid - tr * G;
+        fft::Plan<N>::template run<1>(buf + tr * P, tws, jj);
+    }
+    const R norm = (R)(1.0 / ((double)N * (double)NY));
+    R *pp = phip + (size_t)N * NY * (zi + 1);
+    for (int i = tid; i < TB * N; i += 256) {
+        const int t2 = i / N, x = i - t2 * N;
+        int ya, yb, g, a;
+        split_rows<S, TB>(t2, ya, yb, g, a);
+        const R2 zv = buf[t2 * P + fft::pad(x)];
+        pp[(size_t)N * ya + x] = zv.x * norm;
+        pp[(size_t)N * yb + x] = zv.y * norm;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // launcher
 // ---------------------------------------------------------------------------
 
@@ -885,10 +1252,166 @@ static cudaError_t zdst(const PoissonArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// ---- split-y path ----
+
+template <typename R, int L, int S>
+constexpr size_t slab_smem() {
+    constexpr int n = L / 2 - 1;
+    constexpr int T64 = 256 / fft::Plan<64>::G;
+    constexpr int NR = (n + T64 - 1) / T64 * T64;
+    constexpr int TBZ = 256 / fft::Plan<L>::G;
+    return sizeof(typename Cplx<R>::T) *
+           ((size_t)64 + L + (size_t)NR * tstride<64>() + (size_t)TBZ * tstride<L>());
+}
+template <typename R, int N, int S>
+constexpr size_t rows_inv_split_smem() {
+    constexpr int TB = per_block<N>();
+    return sizeof(typename Cplx<R>::T) *
+           ((size_t)N + (size_t)TB * tstride<N>() + (size_t)2 * TB * (N / 2 + 1));
+}
+
+template <typename R, int N, int S>
+static cudaError_t split_rows_fwd(const PoissonArgs &a, cudaStream_t s) {
+    using R2 = typename Cplx<R>::T;
+    constexpr int TB = per_block<N>(), NB = S == 1 ? 2 * TB : 2 * TB / S;
+    const size_t sm = sizeof(R2) * ((size_t)N + (size_t)TB * tstride<N>());
+    cudaError_t e = set_smem(poisson_rows_fwd_split<R, N, S>, sm, s);
+    if (e != cudaSuccess) return e;
+    poisson_rows_fwd_split<R, N, S><<<dim3(64 / NB, a.nz - 2), 256, sm, s>>>(
+        (const R *)a.q, (R2 *)a.spec, a.rowsum, (const R2 *)a.twx, (const R2 *)a.twy, a.qmean,
+        a.nz - 2, a.nxh, a.eps);
+    return cudaGetLastError();
+}
+template <typename R, int N, int S>
+static cudaError_t split_rows_inv(const PoissonArgs &a, cudaStream_t s) {
+    using R2 = typename Cplx<R>::T;
+    constexpr int TB = per_block<N>(), NB = S == 1 ? 2 * TB : 2 * TB / S;
+    constexpr size_t sm = rows_inv_split_smem<R, N, S>();
+    cudaError_t e = set_smem(poisson_rows_inv_split<R, N, S>, sm, s);
+    if (e != cudaSuccess) return e;
+    poisson_rows_inv_split<R, N, S><<<dim3(64 / NB, a.nz - 2), 256, sm, s>>>(
+        (const R2 *)a.spec, (R *)a.phip, (const R2 *)a.twx, (const R2 *)a.twy, a.nz - 2, a.nxh);
+    return cudaGetLastError();
+}
+template <typename R, int L, int S>
+static cudaError_t split_slab(const PoissonArgs &a, cudaStream_t s) {
+    using R2 = typename Cplx<R>::T;
+    constexpr size_t sm = slab_smem<R, L, S>();
+    cudaError_t e = set_smem(poisson_slab<R, L, S>, sm, s);
+    if (e != cudaSuccess) return e;
+    const R2 *tw = (const R2 *)a.twz;
+    poisson_slab<R, L, S><<<dim3(a.nxh, S), 256, sm, s>>>(
+        (R2 *)a.spec, (const R2 *)a.twy, tw, (const R *)(tw + L), a.rowsum, a.planesum, a.qmean,
+        a.phi00, a.ez00, a.nx, a.nxh, a.dz, a.eps, a.voltage, 2.0 * M_PI / a.lx,
+        2.0 * M_PI / a.ly);
+    return cudaGetLastError();
+}
+
+template <typename R, int N, int S>
+static cudaError_t split_all_n(const PoissonArgs &a, cudaStream_t s) {
+    cudaError_t e = split_rows_fwd<R, N, S>(a, s);
+    if (e != cudaSuccess) return e;
+    switch (2 * (a.nz - 1)) {
+        case 64: e = split_slab<R, 64, S>(a, s); break;
+        case 128: e = split_slab<R, 128, S>(a, s); break;
+        case 256: e = split_slab<R, 256, S>(a, s); break;
+        default: e = split_slab<R, 512, S>(a, s); break;
+    }
+    if (e != cudaSuccess) return e;
+    return split_rows_inv<R, N, S>(a, s);
+}
+template <typename R, int S>
+static cudaError_t split_all(const PoissonArgs &a, cudaStream_t s) {
+    switch (a.nx) {
+        case 64: return split_all_n<R, 64, S>(a, s);
+        case 128: return split_all_n<R, 128, S>(a, s);
+        case 256: return split_all_n<R, 256, S>(a, s);
+        default: return split_all_n<R, 512, S>(a, s);
+    }
+}
+
+template <typename R, int S>
+static size_t split_slab_smem(int L) {
+    switch (L) {
+        case 64: return slab_smem<R, 64, S>();
+        case 128: return slab_smem<R, 128, S>();
+        case 256: return slab_smem<R, 256, S>();
+        default: return slab_smem<R, 512, S>();
+    }
+}
+
+// whether the split-y path serves a grid: NX a compile-time FFT size,
+// NY = 64 S (S = 1, 2, 4, 8), the sine-transform z solve, and the slab in
+// shared memory
+template <typename R>
+bool poisson_split_usable(const PoissonArgs &a) {
+    if (!poisson_fast_size(a.nx) || !a.twz || !poisson_fast_size(2 * (a.nz - 1))) return false;
+    const int S = a.ny / 64;
+    if (a.ny % 64 != 0 || (S != 1 && S != 2 && S != 4 && S != 8)) return false;
+    const int L = 2 * (a.nz - 1);
+    size_t sm = 0;
+    switch (S) {
+        case 1: sm = split_slab_smem<R, 1>(L); break;
+        case 2: sm = split_slab_smem<R, 2>(L); break;
+        case 4: sm = split_slab_smem<R, 4>(L); break;
+        default: sm = split_slab_smem<R, 8>(L); break;
+    }
+    return sm + 4 * 1024 <= 227 * 1024;  // with the static shared arrays
+}
+
+// The split path's shared-memory attributes, set before any stream capture
+// (a launch inside a capture does not set them, see set_smem).
+template <typename R, int N, int L, int S>
+static cudaError_t prepare_split_nls() {
+    cudaError_t e = allow_max_dynamic_smem(poisson_rows_fwd_split<R, N, S>);
+    if (e == cudaSuccess) e = allow_max_dynamic_smem(poisson_slab<R, L, S>);
+    if (e == cudaSuccess) e = allow_max_dynamic_smem(poisson_rows_inv_split<R, N, S>);
+    return e;
+}
+template <typename R, int N, int S>
+static cudaError_t prepare_split_ns(int L) {
+    switch (L) {
+        case 64: return prepare_split_nls<R, N, 64, S>();
+        case 128: return prepare_split_nls<R, N, 128, S>();
+        case 256: return prepare_split_nls<R, N, 256, S>();
+        default: return prepare_split_nls<R, N, 512, S>();
+    }
+}
+template <typename R, int S>
+static cudaError_t prepare_split_s(int nx, int L) {
+    switch (nx) {
+        case 64: return prepare_split_ns<R, 64, S>(L);
+        case 128: return prepare_split_ns<R, 128, S>(L);
+        case 256: return prepare_split_ns<R, 256, S>(L);
+        default: return prepare_split_ns<R, 512, S>(L);
+    }
+}
+template <typename R>
+cudaError_t prepare_poisson(const PoissonArgs &a) {
+    if (!poisson_split_usable<R>(a)) return cudaSuccess;
+    const int L = 2 * (a.nz - 1);
+    switch (a.ny / 64) {
+        case 1: return prepare_split_s<R, 1>(a.nx, L);
+        case 2: return prepare_split_s<R, 2>(a.nx, L);
+        case 4: return prepare_split_s<R, 4>(a.nx, L);
+        default: return prepare_split_s<R, 8>(a.nx, L);
+    }
+}
+template cudaError_t prepare_poisson<float>(const PoissonArgs &);
+template cudaError_t prepare_poisson<double>(const PoissonArgs &);
+
 template <typename R>
 cudaError_t launch_poisson(const PoissonArgs &a, cudaStream_t s) {
     using R2 = typename Cplx<R>::T;
     cudaError_t e;
+    if (a.split && poisson_split_usable<R>(a)) {
+        switch (a.ny / 64) {
+            case 1: return split_all<R, 1>(a, s);
+            case 2: return split_all<R, 2>(a, s);
+            case 4: return split_all<R, 4>(a, s);
+            default: return split_all<R, 8>(a, s);
+        }
+    }
     if ((e = rows_fwd<R>(a, s)) != cudaSuccess) return e;
     if ((e = cols<R, -1>(a, s)) != cudaSuccess) return e;
     if (a.twz && poisson_fast_size(2 * (a.nz - 1))) {

@@ -90,7 +90,11 @@ typedef struct ehd_tuning {
                                 128, y extent 128 / node_block_x              */
     int32_t fft_rows;        /* run-time-radix x FFT: rows per block          */
     int32_t fft_cols;        /* run-time-radix y FFT: columns per block       */
-    int32_t reserved[4];     /* must be 0                                     */
+    int32_t poisson_path;    /* 0: the split-y three-kernel Poisson solve
+                                where it applies (NX a power of two 64..512,
+                                NY = 64, 128, 256 or 512, 2 (NZ-1) likewise),
+                                else the five-kernel one; 1: five-kernel     */
+    int32_t reserved[3];     /* must be 0                                     */
 } ehd_tuning;
 
 /* Scalar diagnostics, reduced on the device in FP64. */

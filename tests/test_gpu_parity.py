@@ -58,29 +58,45 @@ def vel_err(mine, ref, comps):
     return max(float(np.abs(mine[k] - ref[k]).max() / scale) for k in comps)
 
 
-# (steps, tolerance on q and phi, tolerance on velocity)
-CONFIG0_TOL = {"fp64": [(1000, 1e-6, 1e-6), (2000, 1e-6, 1e-6)],
-               "fp32": [(1000, 1e-5, 1e-5), (2000, 1e-4, 1e-4)]}
+# (steps, tolerance on q, phi, velocity, E and the rho deviation)
+CONFIG0_TOL = {"fp64": [(1000, 1e-8), (2000, 1e-8)],
+               "fp32": [(1000, 1e-5), (2000, 1e-4)]}
+
+
+def config0_errors(mine, ref, rho0):
+    """Per-field errors against the reference: q, phi relative to their
+    largest magnitude; velocity and E per component relative to the largest
+    component of the vector; rho relative to 1600 and, for FP64, its deviation
+    from rho0 relative to the largest deviation."""
+    err = {"q": relerr(mine["q"], ref["q"]), "phi": relerr(mine["phi"], ref["phi"]),
+           "velocity": vel_err(mine, ref, ("u", "v", "w")),
+           "E": vel_err(mine, ref, ("ex", "ey", "ez")), "rho": relerr(mine["rho"], ref["rho"])}
+    dev = np.abs(ref["rho"] - rho0).max()
+    err["rho_dev"] = float(np.abs(mine["rho"] - ref["rho"]).max() / dev)
+    return err
 
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 def test_config0_matches_reference(prec):
-    """64 x 64 x 33, hydrostatic start + seeded 1e-3 noise: q, phi, velocity and
+    """64 x 64 x 33, hydrostatic start + seeded 1e-3 noise: all nine fields and
     the collector current after 1000 and 2000 steps against the reference's own
-    build (fields as its data_end.dat writer reports them)."""
+    build (FP64 fixtures, fields as its data_end.dat writer reports them)."""
     M, p, g, f = config0_inputs()
     with ehd.Simulation(to_ehd(p), prec) as sim:
         sim.set_fields(f)
         done = 0
-        for n, tol, tol_u in CONFIG0_TOL[prec]:
+        for n, tol in CONFIG0_TOL[prec]:
             sim.step(n - done)
             done = n
             mine = O.data_end_view(sim.get_fields())
-            ref = {k[len(f"out{n}_"):]: g[k] for k in g.files if k.startswith(f"out{n}_")}
-            for k in ("q", "phi"):
-                assert relerr(mine[k], ref[k]) < tol, (prec, n, k, relerr(mine[k], ref[k]))
-            comps = [k for k in ("u", "v", "w") if k in ref]
-            assert vel_err(mine, ref, comps) < tol_u, (prec, n, vel_err(mine, ref, comps))
+            ref = {k: g[f"out{n}_{k}"] for k in O.FIELDS}
+            err = config0_errors(mine, ref, p.rho0)
+            for k in ("q", "phi", "velocity", "E"):
+                assert err[k] < tol, (prec, n, k, err)
+            if prec == "fp64":
+                assert err["rho_dev"] < tol, (prec, n, err)
+            else:  # FP32 rho: 1600 plus deviations of a few units
+                assert err["rho"] < 1e-6, (prec, n, err)
             assert sim.current() == pytest.approx(float(g[f"current{n}"]), rel=tol)
 
 
@@ -116,8 +132,11 @@ def test_step_halves_match_oracle(shape):
         o.poisson()
         o.efield()
         a, b = sim.get_fields(), o.get_fields()
+        # the z operator's condition number grows as NZ^2 (the FP64 solve of
+        # NZ = 101 loses a decade more than the small grids)
+        tol_p = 1e-11 * max(1.0, (nz / 33.0) ** 2)
         for k in ("phi", "ex", "ey", "ez"):
-            assert relerr(a[k], b[k]) < 1e-11, ("poisson", k)
+            assert relerr(a[k], b[k]) < tol_p, ("poisson", k, relerr(a[k], b[k]))
         sim.step(5)
         o.step(5)
         a, b = sim.get_fields(), o.get_fields()
@@ -150,6 +169,38 @@ def test_poisson_fft_sizes_match_oracle(shape, prec, tol):
         a = sim.get_fields()
     for k in ("phi", "ex", "ey", "ez"):
         assert relerr(a[k], b[k]) < tol, (k, relerr(a[k], b[k]))
+
+
+@pytest.mark.parametrize("shape", [(256, 256, 129), (64, 64, 33), (128, 256, 65), (512, 64, 17),
+                                   (64, 512, 33), (256, 128, 129), (128, 128, 257)])
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("fp32", 2e-6)])
+def test_poisson_split_path_matches_oracle_and_five_kernel_path(shape, prec, tol):
+    """The three-kernel split-y Poisson solve (the x-row kernels fold in the
+    radix-S first and last stages of the y transform, NY = 64 S; one slab
+    kernel per (kx, j) runs the 64-point y transforms and the sine-transform z
+    solve on chip) against the oracle's odd-extension DFT solve
+    (poisson.cu:78-167) and against the five-kernel path of the same context
+    type (ehd_tuning.poisson_path = 1), on random charge."""
+    nx, ny, nz = shape
+    dz = 1.0 / (nz - 1)
+    p = O.params_from_groups(nx, ny, nz, nx * dz, ny * dz, T=200, M=10, C=10, Fe=4000)
+    f = random_fields(p, 5)
+    o = O.Oracle(p)
+    o.set_fields(f)
+    o.poisson()
+    o.efield()
+    b = o.get_fields()
+    o.close()
+    out = {}
+    for path in (0, 1):
+        with ehd.Simulation(to_ehd(p), prec) as sim:
+            sim.set_tuning(poisson_path=path)
+            sim.set_fields(f)
+            sim.poisson()
+            out[path] = sim.get_fields()
+    for k in ("phi", "ex", "ey", "ez"):
+        assert relerr(out[0][k], b[k]) < tol, (k, "oracle", relerr(out[0][k], b[k]))
+        assert relerr(out[0][k], out[1][k]) < tol, (k, "five-kernel", relerr(out[0][k], out[1][k]))
 
 
 @pytest.mark.parametrize("shape", [(64, 48, 33), (96, 64, 65), (32, 20, 129), (16, 12, 257)])

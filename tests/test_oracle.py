@@ -50,6 +50,34 @@ def test_oracle_matches_reference_golden(case):
         assert abs(o.current() - float(g[f"current{n}"])) <= 1e-11 * abs(float(g[f"current{n}"]))
 
 
+def test_oracle_matches_reference_config0_1000_steps():
+    """The oracle against the reference's own build on config 0 (64 x 64 x 33,
+    hydrostatic start + seeded noise, FP64 fixtures from its data_end.dat):
+    every field after 1000 steps; velocity and E per component relative to
+    the largest component of the vector, rho as its deviation from rho0."""
+    import make_golden as M
+    g = golden("config0")
+    p = M.case_params("config0")
+    prof = {k: g[f"prof_{k}"] for k in O.FIELDS}
+    o = O.Oracle(p)
+    o.set_fields(O.state_from_profile(p, prof, seed=0, amp=1e-3))
+    o.step(1000)
+    mine = O.data_end_view(o.get_fields())
+    o.close()
+    ref = {k: g[f"out1000_{k}"] for k in O.FIELDS}
+
+    def vec(comps):
+        s = max(np.abs(ref[k]).max() for k in comps)
+        return max(float(np.abs(mine[k] - ref[k]).max() / s) for k in comps)
+
+    assert vec(("u", "v", "w")) < 1e-11
+    assert vec(("ex", "ey", "ez")) < 1e-11
+    for k in ("q", "phi"):
+        assert np.abs(mine[k] - ref[k]).max() / np.abs(ref[k]).max() < 1e-11, k
+    dev = np.abs(ref["rho"] - p.rho0).max()
+    assert np.abs(mine["rho"] - ref["rho"]).max() / dev < 1e-10
+
+
 def test_config0_inputs_regenerate():
     """The config-0 initial state (hydrostatic profile + seeded perturbation)
     is reproducible from the stored profile and the seed."""
