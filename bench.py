@@ -192,6 +192,8 @@ def run_ours(args, rank, world, local_rank):
     def device_mlups(prec, sampler_gpu=None):
         sim = ehd.Simulation(p, prec, device=local_rank, stream=stream.cuda_stream,
                              row_kernel=not args.node_kernel)
+        if args.poisson_path is not None:
+            sim.set_tuning(poisson_path=args.poisson_path)
         cs = ClockSampler(sampler_gpu) if sampler_gpu is not None else None
         try:
             sim.set_fields(fields)
@@ -596,6 +598,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--node-kernel", action="store_true",
                     help="profiling: every LBM step on the one-thread-per-node kernel")
+    ap.add_argument("--poisson-path", type=int, choices=[0, 1], default=None,
+                    help="profiling: 0 split-y three-kernel Poisson solve, 1 five-kernel")
     ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32", "fp16", "bf16"],
                     help="storage of the headline run (profiling)")
     ap.add_argument("--grid", type=int, nargs=3, metavar=("NX", "NY", "NZ"),

@@ -533,10 +533,21 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
     if ((r = dalloc(c, &twx, (size_t)nx * c2))) return bail(r);
     if ((r = dalloc(c, &twy, (size_t)ny * c2))) return bail(r);
     const size_t nmodes = (size_t)pa.nxh * ny;
-    // z solve: sine transform where 2 (nz - 1) is a compile-time FFT size,
-    // else the Thomas solve with its pivot table and sweep scratch
+    // z solve: sine transform, with compile-time FFT passes where 2 (nz - 1)
+    // is one of their sizes and run-time ones where the transforms of a few
+    // modes fit in shared memory; else the Thomas solve with its pivot table
+    // and sweep scratch
     const int lz2 = 2 * (nz - 1);
-    const bool zdst = poisson_fast_size(lz2);
+    bool zdst = poisson_fast_size(lz2);
+    if (!zdst) {
+        int tb = 16;
+        while (tb > 1 && zdst_rt_smem(lz2, tb, c->rsize) > 160 * 1024) tb >>= 1;
+        if (zdst_rt_smem(lz2, tb, c->rsize) <= 160 * 1024) {
+            zdst = true;
+            pa.ztb = tb;
+            pa.pz = make_plan(lz2);
+        }
+    }
     double *cpt = nullptr;
     void *twz = nullptr;
     if (zdst) {

@@ -106,6 +106,9 @@ struct PoissonArgs {
     int cols_per_block;  // y-column FFT batch per block (run-time radix path)
     FftPlan px, py;
     const void *twx, *twy;   // exp(-2 pi i k/N) tables in the compute type
+    FftPlan pz;              // run-time plan of length L = 2 (nz - 1) (sine-transform
+                             // z solve when L is not a compile-time FFT size)
+    int ztb;                 // modes per block of that solve
     const void *twz;         // sine-transform z solve, L = 2 (nz - 1), compute type:
                              // exp(-2 pi i k/L) (L complex), then 4 sin^2(pi k/L)
                              // (L/2 + 1 real); nullptr: Thomas solve
@@ -130,6 +133,9 @@ template <typename R>
 cudaError_t prepare_poisson(const PoissonArgs &a);
 
 bool poisson_fast_size(int n);
+// shared memory of the run-time-radix sine-transform z solve with tb modes
+// per block (compute type of rsize bytes)
+size_t zdst_rt_smem(int L, int tb, size_t rsize);
 
 // ---- diagnostics ---------------------------------------------------------
 

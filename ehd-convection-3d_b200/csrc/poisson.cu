@@ -61,8 +61,9 @@ template <typename R2, typename R> __device__ __forceinline__ R2 cscale(R2 a, R 
 }
 
 // One batch of `batch` length-N transforms held contiguously in `a`; `b` is
-// scratch of the same size.  Returns the buffer holding the result.  sign -1
-// forward (exp(-2 pi i jk/N)), +1 inverse, unnormalised.
+// scratch of the same size; `tw` the table exp(-2 pi i m/N), m < N (in shared
+// memory).  Returns the buffer holding the result.  sign -1 forward
+// (exp(-2 pi i jk/N)), +1 inverse, unnormalised.
 template <typename R>
 __device__ typename Cplx<R>::T *fft_smem(typename Cplx<R>::T *a, typename Cplx<R>::T *b,
                                          const FftPlan &pl,
@@ -90,7 +91,7 @@ __device__ typename Cplx<R>::T *fft_smem(typename Cplx<R>::T *a, typename Cplx<R
                 const int r = e / nb, j = e - r * nb;
                 const int k = j % Ns;
                 if (r > 0 && k > 0) {
-                    R2 w = __ldg(tw + r * k * tstep);
+                    R2 w = tw[r * k * tstep];
                     w.y *= -sign;
                     a[t] = cmul(a[t], w);
                 }
@@ -116,7 +117,7 @@ __device__ typename Cplx<R>::T *fft_smem(typename Cplx<R>::T *a, typename Cplx<R
                     int m = qq;  // r qq mod p
                     for (int r = 1; r <= h; ++r) {
                         const R2 xr = in[j + r * nb], xm = in[j + (Rr - r) * nb];
-                        const R2 w = __ldg(tw + m * pstep);  // (cos, -sin) of 2 pi m / p
+                        const R2 w = tw[m * pstep];  // (cos, -sin) of 2 pi m / p
                         A.x += (xr.x + xm.x) * w.x;
                         A.y += (xr.y + xm.y) * w.x;
                         B.x -= (xr.x - xm.x) * w.y;
@@ -149,7 +150,7 @@ __device__ typename Cplx<R>::T *fft_smem(typename Cplx<R>::T *a, typename Cplx<R
                 if (r < Rr) {
                     R2 x = in[j + r * nb];
                     if (r > 0 && k > 0) {
-                        R2 w = __ldg(tw + r * k * tstep);
+                        R2 w = tw[r * k * tstep];
                         w.y *= -sign;  // table holds exp(-2 pi i m/N): conjugate for inverse
                         x = cmul(x, w);
                     }
@@ -217,9 +218,11 @@ poisson_rows_fwd(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R2 *a = reinterpret_cast<R2 *>(smem_raw);
     R2 *b = a + (size_t)rows * nx;
+    R2 *tws = b + (size_t)rows * nx;
     const int zi = blockIdx.y;  // plane z = zi + 1
     const int y0 = blockIdx.x * rows;
     const int tid = threadIdx.x;
+    for (int i = tid; i < nx; i += blockDim.x) tws[i] = tw[i];
     const R *qp = q + (size_t)nx * ny * (zi + 1);
     const R qm = (R)qmean[2 * (zi + 1) + 1];
     for (int t = tid; t < rows * nx; t += blockDim.x) {
@@ -240,7 +243,7 @@ poisson_rows_fwd(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec
         if (lane == 0) rowsum[(size_t)zi * ny + y] = -sum / eps;
     }
     __syncthreads();
-    R2 *res = fft_smem<R>(a, b, pl, tw, (R)-1, rows);
+    R2 *res = fft_smem<R>(a, b, pl, tws, (R)-1, rows);
     R2 *sp = spec + (size_t)zi * ny * pitch;
     for (int t = tid; t < rows * nxh; t += blockDim.x) {
         const int r = t / nxh, k = t - r * nxh;
@@ -271,9 +274,11 @@ poisson_cols(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::T *
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R2 *a = reinterpret_cast<R2 *>(smem_raw);
     R2 *b = a + (size_t)cols * ny;
+    R2 *tws = b + (size_t)cols * ny;
     const int zi = blockIdx.y;
     const int k0 = blockIdx.x * cols;
     const int tid = threadIdx.x;
+    for (int i = tid; i < ny; i += blockDim.x) tws[i] = tw[i];
     const size_t off = (size_t)zi * ny * pitch;
     for (int t = tid; t < ny * cols; t += blockDim.x) {
         const int y = t / cols, cidx = t - y * cols;
@@ -284,7 +289,7 @@ poisson_cols(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::T *
     }
     if (planesum != nullptr && blockIdx.x == 0 && tid < 32) plane_sum_warp(rowsum, planesum, zi, ny);
     __syncthreads();
-    R2 *res = fft_smem<R>(a, b, pl, tw, sign, cols);
+    R2 *res = fft_smem<R>(a, b, pl, tws, sign, cols);
     for (int t = tid; t < ny * cols; t += blockDim.x) {
         const int y = t / cols, cidx = t - y * cols;
         const int k = k0 + cidx;
@@ -303,9 +308,11 @@ poisson_rows_inv(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ p
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R2 *a = reinterpret_cast<R2 *>(smem_raw);
     R2 *b = a + (size_t)rows * nx;
+    R2 *tws = b + (size_t)rows * nx;
     const int zi = blockIdx.y;
     const int y0 = blockIdx.x * rows;
     const int tid = threadIdx.x;
+    for (int i = tid; i < nx; i += blockDim.x) tws[i] = tw[i];
     const R2 *sp = spec + (size_t)zi * ny * pitch;
     for (int t = tid; t < rows * nx; t += blockDim.x) {
         const int r = t / nx, k = t - r * nx;
@@ -322,7 +329,7 @@ poisson_rows_inv(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ p
         a[t] = v;
     }
     __syncthreads();
-    R2 *res = fft_smem<R>(a, b, pl, tw, (R)1, rows);
+    R2 *res = fft_smem<R>(a, b, pl, tws, (R)1, rows);
     const R norm = (R)(1.0 / ((double)nx * (double)ny));
     R *pp = phip + (size_t)nx * ny * (zi + 1);
     for (int t = tid; t < rows * nx; t += blockDim.x) {
@@ -751,6 +758,116 @@ poisson_zdst(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::T *
     }
 }
 
+// K3 for any L = 2 (NZ - 1) whose transforms fit in shared memory: the
+// sine-transform z solve of poisson_zdst with run-time radix passes
+// (fft_smem) instead of compile-time ones.  tb modes per block, consecutive
+// in m = ky nxh + kx; the odd extensions of the block's modes are held as tb
+// contiguous length-L transforms (two buffers for the Stockham passes).  The
+// block holding m = 0 solves the (0,0) mode in FP64 in closed form.
+template <typename R>
+__global__ void __launch_bounds__(256)
+poisson_zdst_rt(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::T *__restrict__ twz,
+                const R *__restrict__ lamz, FftPlan pl, const double *__restrict__ planesum,
+                const double *__restrict__ qmean, double *__restrict__ phi00,
+                double *__restrict__ ez00, int nx, int ny, int nxh, int pitch, int tb, double dz,
+                double eps, double voltage, double kx0, double ky0) {
+    using R2 = typename Cplx<R>::T;
+    const int L = pl.n, n = L / 2 - 1, nz = n + 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *a = reinterpret_cast<R2 *>(smem_raw);
+    R2 *b = a + (size_t)tb * L;
+    R2 *tws = b + (size_t)tb * L;                                   // L
+    double *mrhs = reinterpret_cast<double *>(tws + L);             // n
+    double *mphi = mrhs + n;                                          // nz
+    R *hdz2 = reinterpret_cast<R *>(mphi + nz);                       // tb
+    const int tid = threadIdx.x;
+    const int modes = nxh * ny;
+    const int m0 = blockIdx.x * tb;
+    const size_t plane = (size_t)ny * pitch;
+    const double dz2 = dz * dz;
+    for (int i = tid; i < L; i += 256) tws[i] = twz[i];
+    for (int t = tid; t < tb; t += 256) {
+        const int m = m0 + t;
+        R h = (R)-1;
+        if (m < modes && m != 0) {
+            const int ky = m / nxh, kx = m - ky * nxh;
+            const double wx = kx * kx0, wy = (ky <= ny / 2 ? ky : ky - ny) * ky0;
+            h = (R)((wx * wx + wy * wy) * dz2);
+        }
+        hdz2[t] = h;
+        a[(size_t)t * L] = R2{(R)0, (R)0};
+        a[(size_t)t * L + L / 2] = R2{(R)0, (R)0};
+    }
+    for (int i = tid; i < tb * n; i += 256) {
+        const int zi = i / tb, t = i - zi * tb;
+        const int m = m0 + t;
+        R2 v = R2{(R)0, (R)0};
+        if (m < modes && m != 0) {
+            const int ky = m / nxh, kx = m - ky * nxh;
+            v = spec[(size_t)zi * plane + (size_t)ky * pitch + kx];
+        }
+        a[(size_t)t * L + zi + 1] = v;
+        a[(size_t)t * L + L - 1 - zi] = R2{-v.x, -v.y};
+    }
+    const bool mean_block = m0 == 0;
+    if (mean_block) {
+        const double nxy = (double)nx * (double)ny;
+        for (int i = tid; i < n; i += 256) {
+            double d = planesum[i + 1] + nxy * (-(double)(R)qmean[2 * (i + 1) + 1] / eps);
+            if (i == 0) d += -voltage / dz2 * nxy;
+            mrhs[i] = d * dz2;
+        }
+    }
+    __syncthreads();
+    R2 *r1 = fft_smem<R>(a, b, pl, tws, (R)-1, tb);
+    for (int i = tid; i < tb * L; i += 256) {
+        const int t = i / L, k = i - t * L;
+        const R h = hdz2[t];
+        R2 y = r1[i];
+        if (k == 0 || k == L / 2 || h < (R)0) {
+            y = R2{(R)0, (R)0};
+        } else {
+            const R f = rcp(lamz[k < L / 2 ? k : L - k] + h);
+            y = R2{y.x * f, y.y * f};
+        }
+        r1[i] = y;
+    }
+    __syncthreads();
+    R2 *r2 = fft_smem<R>(r1, r1 == a ? b : a, pl, tws, (R)-1, tb);
+    const R sc = (R)(dz2 / (double)L);
+    for (int i = tid; i < tb * n; i += 256) {
+        const int zi = i / tb, t = i - zi * tb;
+        const int m = m0 + t;
+        if (m < modes) {
+            const int ky = m / nxh, kx = m - ky * nxh;
+            const R2 w = r2[(size_t)t * L + zi + 1];
+            spec[(size_t)zi * plane + (size_t)ky * pitch + kx] = R2{w.x * sc, w.y * sc};
+        }
+    }
+    if (mean_block) {
+        const double nxy = (double)nx * (double)ny;
+        for (int i = tid; i < nz; i += 256) {
+            double x = 0.0;
+            if (i == 0) {
+                x = voltage;
+            } else if (i < nz - 1) {
+                for (int jz = 1; jz <= n; ++jz) {
+                    const int lo = i < jz ? i : jz, hi = i < jz ? jz : i;
+                    x -= (double)(lo * (n + 1 - hi)) * mrhs[jz - 1];
+                }
+                x = x / (double)(n + 1) / nxy;
+            }
+            mphi[i] = x;
+            phi00[i] = x;
+        }
+        __syncthreads();
+        for (int z = tid; z < nz; z += 256) {
+            const int zc = z < 1 ? 1 : (z > nz - 2 ? nz - 2 : z);
+            ez00[z] = 0.5 * (mphi[zc - 1] - mphi[zc + 1]) / dz;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // split-y path: three launches instead of five
 // ---------------------------------------------------------------------------
@@ -787,6 +904,29 @@ __device__ __forceinline__ void split_rows(int tr, int &ya, int &yb, int &g, int
         ya = blockIdx.x * GB + g + 64 * a;
         yb = ya + 32 * S;
     }
+}
+
+// x * exp(-2 pi i e / 8) for e = 0..7, by swaps, negations and one scale by
+// sqrt(1/2) (no multiplication by zero); in unrolled loops e is a constant
+template <typename R2>
+__device__ __forceinline__ R2 mul_w8(R2 x, int e) {
+    using R = decltype(x.x);
+    const R r = (R)0.70710678118654752440;
+    switch (e & 7) {
+        case 0: return x;
+        case 1: return R2{r * (x.x + x.y), r * (x.y - x.x)};
+        case 2: return R2{x.y, -x.x};
+        case 3: return R2{r * (x.y - x.x), -r * (x.x + x.y)};
+        case 4: return R2{-x.x, -x.y};
+        case 5: return R2{-r * (x.x + x.y), r * (x.x - x.y)};
+        case 6: return R2{-x.y, x.x};
+        default: return R2{r * (x.x - x.y), r * (x.x + x.y)};
+    }
+}
+// x * W_S^k = x * exp(-2 pi i k / S), S = 1, 2, 4, 8
+template <int S, typename R2>
+__device__ __forceinline__ R2 mul_ws(R2 x, int k) {
+    return mul_w8(x, (k % S) * (8 / S));
 }
 
 // x-spectrum of row part (0: ya, 1: yb) of a packed transform at bin k < nxh
@@ -859,28 +999,31 @@ poisson_rows_fwd_split(const R *__restrict__ q, typename Cplx<R>::T *__restrict_
         const int tr = tid / G, jj = tid - tr * G;
         fft::Plan<N>::template run<-1>(buf + tr * P, tws, jj);
     }
-    // outputs (j, kx, g), g fastest: GB consecutive n per (j, kx)
+    // items (g, kx), g fastest: the S rows n + 64 m of group g at bin kx, a
+    // radix-S DFT over m, the twiddle W_NY^(j n), S outputs of GB consecutive
+    // n per (j, kx)
     const int nblk = S == 1 ? 2 * TB : GB;
     const int n0 = blockIdx.x * nblk;
-    for (int i = tid; i < S * nxh * nblk; i += 256) {
-        const int g = i % nblk, rest = i / nblk;
-        const int kx = rest % nxh, j = rest / nxh;
+    for (int i = tid; i < nxh * nblk; i += 256) {
+        const int g = i % nblk, kx = i / nblk;
         const int n = n0 + g;
-        R2 acc;
         if constexpr (S == 1) {
-            acc = unpack_bin<R2, R>(buf + (g >> 1) * P, kx, g & 1, N);
+            spl[((size_t)kx * nzi + zi) * 64 + n] = unpack_bin<R2, R>(buf + (g >> 1) * P, kx, g & 1, N);
         } else {
-            acc = R2{(R)0, (R)0};
+            R2 x[S];
 #pragma unroll
-            for (int m = 0; m < S; ++m) {
-                const int t = g * (S / 2) + (m < S / 2 ? m : m - S / 2);
-                R2 x = unpack_bin<R2, R>(buf + t * P, kx, m < S / 2 ? 0 : 1, N);
-                if (j * m != 0) x = cmul(x, __ldg(twy + ((j * m) % S) * 64));
-                acc = cadd(acc, x);
+            for (int m = 0; m < S; ++m)
+                x[m] = unpack_bin<R2, R>(buf + (g * (S / 2) + (m % (S / 2))) * P, kx,
+                                         m < S / 2 ? 0 : 1, N);
+#pragma unroll
+            for (int j = 0; j < S; ++j) {
+                R2 acc = x[0];
+#pragma unroll
+                for (int m = 1; m < S; ++m) acc = cadd(acc, mul_ws<S>(x[m], j * m));
+                if (j != 0 && n != 0) acc = cmul(acc, __ldg(twy + j * n));
+                spl[(((size_t)j * nxh + kx) * nzi + zi) * 64 + n] = acc;
             }
-            if (j * n != 0) acc = cmul(acc, __ldg(twy + (j * n) % NY));
         }
-        spl[(((size_t)j * nxh + kx) * nzi + zi) * 64 + n] = acc;
     }
 }
 
@@ -1057,49 +1200,45 @@ poisson_rows_inv_split(const typename Cplx<R>::T *__restrict__ spl, R *__restric
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R2 *tws = reinterpret_cast<R2 *>(smem_raw);
     R2 *buf = tws + N;
-    R2 *bs = buf + TB * P;  // b_j[n0 + g][kx] as bs[(j nxh + kx) NB + g]
     const int zi = blockIdx.y;
     const int tid = threadIdx.x;
     const int n0 = blockIdx.x * NB;
     load_twiddles<R, N>(tws, tw);
-    for (int i = tid; i < S * nxh * NB; i += 256) {
-        const int g = i % NB, jk = i / NB;
-        bs[i] = spl[((size_t)jk * nzi + zi) * 64 + n0 + g];
-    }
-    __syncthreads();
-    // packed inputs Z = A + i B over the full length
-    for (int i = tid; i < TB * N; i += 256) {
-        const int tr = i / N, k = i - tr * N;
-        int ya, yb, g, a;
-        split_rows<S, TB>(tr, ya, yb, g, a);
-        const int kk = k < nxh ? k : N - k;
-        R2 A, B;
+    // items (g, kx), g fastest (S = 1: g a transform, rows n0 + 2g, + 1):
+    // b_j of the group's n at bin kx, the inverse radix-S DFT over j, and the
+    // packed inputs Z = A + i B of its transforms at k = kx and k = N - kx
+    // (Hermitian completion; the imaginary parts of the bins 0 and N/2 dropped)
+    constexpr int NI = S == 1 ? TB : GB;
+    for (int i = tid; i < nxh * NI; i += 256) {
+        const int g = i % NI, kx = i / NI;
+        R2 xm[S == 1 ? 2 : S];
         if constexpr (S == 1) {
-            A = bs[(size_t)kk * NB + 2 * tr];
-            B = bs[(size_t)kk * NB + 2 * tr + 1];
+            xm[0] = spl[((size_t)kx * nzi + zi) * 64 + n0 + 2 * g];
+            xm[1] = spl[((size_t)kx * nzi + zi) * 64 + n0 + 2 * g + 1];
         } else {
-            A = R2{(R)0, (R)0};
-            B = R2{(R)0, (R)0};
-            const int ma = a, mb = a + S / 2;
+            R2 b[S];
 #pragma unroll
-            for (int j = 0; j < S; ++j) {
-                const R2 v = bs[((size_t)j * nxh + kk) * NB + g];
-                R2 wa = __ldg(twy + ((j * ma) % S) * 64), wb = __ldg(twy + ((j * mb) % S) * 64);
-                wa.y = -wa.y;  // W_S^(-j m)
-                wb.y = -wb.y;
-                A = cadd(A, cmul(v, wa));
-                B = cadd(B, cmul(v, wb));
+            for (int j = 0; j < S; ++j) b[j] = spl[(((size_t)j * nxh + kx) * nzi + zi) * 64 + n0 + g];
+#pragma unroll
+            for (int m = 0; m < S; ++m) {
+                R2 acc = b[0];
+#pragma unroll
+                for (int j = 1; j < S; ++j) acc = cadd(acc, mul_ws<S>(b[j], S - (j * m) % S));
+                xm[m] = acc;
             }
         }
-        if (kk == 0 || kk == N / 2) {
-            A.y = 0;
-            B.y = 0;
+        constexpr int NT = S == 1 ? 1 : S / 2;  // transforms per item
+#pragma unroll
+        for (int a2 = 0; a2 < NT; ++a2) {
+            R2 A = S == 1 ? xm[0] : xm[a2], B = S == 1 ? xm[1] : xm[a2 + S / 2];
+            const int tr = S == 1 ? g : g * (S / 2) + a2;
+            if (kx == 0 || kx == N / 2) {
+                A.y = 0;
+                B.y = 0;
+            }
+            buf[tr * P + fft::pad(kx)] = R2{A.x - B.y, A.y + B.x};
+            if (kx != 0 && kx != N / 2) buf[tr * P + fft::pad(N - kx)] = R2{A.x + B.y, B.x - A.y};
         }
-        if (k >= nxh) {
-            A.y = -A.y;
-            B.y = -B.y;
-        }
-        buf[tr * P + fft::pad(k)] = R2{A.x - B.y, A.y + B.x};
     }
     __syncthreads();
     {
@@ -1137,6 +1276,12 @@ static cudaError_t set_smem(K kern, size_t bytes, cudaStream_t s) {
 }
 
 bool poisson_fast_size(int n) { return n == 64 || n == 128 || n == 256 || n == 512; }
+
+size_t zdst_rt_smem(int L, int tb, size_t rsize) {
+    const int n = L / 2 - 1, nz = n + 2;
+    return (size_t)(2 * tb + 1) * L * 2 * rsize + sizeof(double) * (size_t)(n + nz) +
+           (size_t)tb * rsize + 16;
+}
 
 template <typename R, int N>
 static cudaError_t rows_fwd_fast(const PoissonArgs &a, cudaStream_t s) {
@@ -1187,7 +1332,7 @@ static cudaError_t rows_fwd(const PoissonArgs &a, cudaStream_t s) {
         default: break;
     }
     const int rows = a.rows_per_block;
-    const size_t sm = (size_t)2 * rows * a.nx * sizeof(R2);
+    const size_t sm = (size_t)(2 * rows + 1) * a.nx * sizeof(R2);
     cudaError_t e = set_smem(poisson_rows_fwd<R>, sm, s);
     if (e != cudaSuccess) return e;
     dim3 grid((a.ny + rows - 1) / rows, a.nz - 2);
@@ -1207,7 +1352,7 @@ static cudaError_t rows_inv(const PoissonArgs &a, cudaStream_t s) {
         default: break;
     }
     const int rows = a.rows_per_block;
-    const size_t sm = (size_t)2 * rows * a.nx * sizeof(R2);
+    const size_t sm = (size_t)(2 * rows + 1) * a.nx * sizeof(R2);
     cudaError_t e = set_smem(poisson_rows_inv<R>, sm, s);
     if (e != cudaSuccess) return e;
     dim3 grid((a.ny + rows - 1) / rows, a.nz - 2);
@@ -1227,7 +1372,7 @@ static cudaError_t cols(const PoissonArgs &a, cudaStream_t s) {
         default: break;
     }
     const int cc = a.cols_per_block;
-    const size_t sm = (size_t)2 * cc * a.ny * sizeof(R2);
+    const size_t sm = (size_t)(2 * cc + 1) * a.ny * sizeof(R2);
     cudaError_t e = set_smem(poisson_cols<R>, sm, s);
     if (e != cudaSuccess) return e;
     dim3 grid((a.nxh + cc - 1) / cc, a.nz - 2);
@@ -1266,8 +1411,7 @@ constexpr size_t slab_smem() {
 template <typename R, int N, int S>
 constexpr size_t rows_inv_split_smem() {
     constexpr int TB = per_block<N>();
-    return sizeof(typename Cplx<R>::T) *
-           ((size_t)N + (size_t)TB * tstride<N>() + (size_t)2 * TB * (N / 2 + 1));
+    return sizeof(typename Cplx<R>::T) * ((size_t)N + (size_t)TB * tstride<N>());
 }
 
 template <typename R, int N, int S>
@@ -1422,6 +1566,17 @@ cudaError_t launch_poisson(const PoissonArgs &a, cudaStream_t s) {
             default: e = zdst<R, 512>(a, s); break;
         }
         if (e != cudaSuccess) return e;
+    } else if (a.twz) {
+        const int modes = a.nxh * a.ny;
+        const int L = 2 * (a.nz - 1);
+        const size_t sm = zdst_rt_smem(L, a.ztb, sizeof(R));
+        if ((e = set_smem(poisson_zdst_rt<R>, sm, s)) != cudaSuccess) return e;
+        const R2 *tw = (const R2 *)a.twz;
+        poisson_zdst_rt<R><<<(modes + a.ztb - 1) / a.ztb, 256, sm, s>>>(
+            (R2 *)a.spec, tw, (const R *)(tw + L), a.pz, a.planesum, a.qmean, a.phi00, a.ez00,
+            a.nx, a.ny, a.nxh, a.pitch, a.ztb, a.dz, a.eps, a.voltage, 2.0 * M_PI / a.lx,
+            2.0 * M_PI / a.ly);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
     } else {
         const int modes = a.nxh * a.ny;
         poisson_zsolve<R><<<(modes + 127) / 128, 128, 0, s>>>(

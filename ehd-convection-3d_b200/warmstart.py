@@ -147,6 +147,8 @@ def main(argv=None):
     ap.add_argument("--layers", type=int, default=4)
     ap.add_argument("--hidden", type=int, default=128)
     ap.add_argument("--grid", type=int, nargs=3, default=(64, 64, 33), metavar=("NX", "NY", "NZ"))
+    ap.add_argument("--t-range", type=float, nargs=2, default=(150.0, 400.0), metavar=("LO", "HI"),
+                    help="electric Rayleigh number T of the instances, uniform in [LO, HI]")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     grid = tuple(a.grid)
@@ -159,8 +161,8 @@ def main(argv=None):
         print(m, flush=True)
 
     t0 = time.perf_counter()
-    gtr = sample_groups(a.train, seed=1)
-    gte = sample_groups(a.test, seed=2)
+    gtr = sample_groups(a.train, seed=1, t_range=tuple(a.t_range))
+    gte = sample_groups(a.test, seed=2, t_range=tuple(a.t_range))
     xtr, ytr, itr = trajectories(ehd, gtr, a.horizon, grid=grid)
     xte, yte, ite = trajectories(ehd, gte, a.horizon, extra=a.relax, grid=grid)
     t_data = time.perf_counter() - t0
@@ -180,6 +182,8 @@ def main(argv=None):
     # held-out: prediction against the plain run's state at the horizon
     errs, base = [], []
     errs_v, base_v = [], []  # the velocity channels alone
+    errs_c = [[] for _ in range(COUT)]  # per output channel
+    base_c = [[] for _ in range(COUT)]
     preds = []
     for k in range(len(ite)):
         u = net.forward(torch.tensor(xte[k:k + 1], device=dev)).cpu().numpy()[0] * std + mean
@@ -188,6 +192,9 @@ def main(argv=None):
         base.append(rel_l2(xte[k][..., :COUT], yte[k]))
         errs_v.append(rel_l2(u[..., :3], yte[k][..., :3]))
         base_v.append(rel_l2(xte[k][..., :3], yte[k][..., :3]))
+        for c in range(COUT):
+            errs_c[c].append(rel_l2(u[..., c], yte[k][..., c]))
+            base_c[c].append(rel_l2(xte[k][..., c], yte[k][..., c]))
     # warm start: a short run from the prediction against the plain run
     # continued by the same number of steps
     nu_warm, nu_cold, nu_none = [], [], []
@@ -231,6 +238,10 @@ def main(argv=None):
         "pred_rel_l2_velocity": float(np.mean(errs_v)),
         "initial_rel_l2_velocity": float(np.mean(base_v)),
         "gain_velocity": float(np.mean(base_v) / max(np.mean(errs_v), 1e-30)),
+        "gain_channels": {name: float(np.mean(base_c[c]) / max(np.mean(errs_c[c]), 1e-30))
+                          for c, name in enumerate(("u", "v", "w", "q", "phi"))},
+        "initial_rel_l2_channels": {name: float(np.mean(base_c[c]))
+                                    for c, name in enumerate(("u", "v", "w", "q", "phi"))},
         "nu_e_plain_at_horizon_plus_relax": nu_cold,
         "nu_e_warm_after_relax": nu_warm,
         "nu_e_plain_after_relax_from_start": nu_none,

@@ -11,8 +11,8 @@ relative to the largest component of the vector):
   FP32 against the oracle (FP64) after 1 and 5 steps: 1e-5 (the bar for FP32
   fields), velocity and E 1e-5;
   FP32 against the product's own FP64 run after 1000 steps: 1e-5 on q and phi,
-  1e-4 on the rest (velocities grow from 1e-3 noise; rho is compared to its
-  deviation scale below).
+  1e-4 on velocity and E, 1e-6 on rho (1600 plus deviations that the FP32
+  field resolves to about 1e-4).
 """
 import importlib.util
 import os
@@ -85,9 +85,10 @@ def test_bench_case_fp32_matches_fp64_after_1000_steps(case):
             assert sim.diagnostics()["nonfinite"] == 0
     a, b = res["fp32"], res["fp64"]
     err = field_errors(a, b)
-    # rho is 1600 plus deviations of order 1e-2: compare them on their own scale
-    err["rho_dev"] = float(np.abs(a["rho"] - b["rho"]).max() / np.abs(b["rho"] - p.rho0).max())
     for k in ("q", "phi"):
         assert err[k] < 1e-5, (k, err)
-    for k in ("velocity", "E", "rho_dev"):
+    for k in ("velocity", "E"):
         assert err[k] < 1e-4, (k, err)
+    # rho is 1600 plus deviations of a few tenths: the FP32 field resolves it
+    # to about 1e-4 absolute
+    assert err["rho"] < 1e-6, err
