@@ -41,9 +41,9 @@ PKG = ROOT / "ehd-convection-3d_b200"
 NX, NY, NZ = 256, 256, 129  # the workload; --grid overrides it for profiling only
 NODES = NX * NY * NZ
 # kernels per step of the FP32 256-wide workload: lbm_step (plane z = 0), lbm_rows
-# (planes z >= 1), reduce_tables, and the Poisson's rows_fwd, cols, zdst, cols,
-# rows_inv
-KERNELS_PER_STEP = 8
+# (planes z >= 1), reduce_tables, and the split-y Poisson's rows_fwd_split, slab,
+# rows_inv_split
+KERNELS_PER_STEP = 6
 # Algorithmic bytes per node of one lbm_step launch (macros written, as
 # ehd_stream_collide_save does): 27 f + 27 g read and written, q written,
 # phi' read, rho/u/v/w written.  s = population bytes, p = field bytes.
@@ -561,6 +561,7 @@ def run_batch(args, rank, local_rank):
         ehd, params, [sweep.hydrostatic_steps(p, 1.0) for p in params], device=local_rank)
     K, W = args.steps, args.warmup
     with ehd.Batch(params, args.precision, device=local_rank) as b:
+        b.set_mode(args.batch_mode)
         if args.autotune:
             b.autotune(trial_steps=10)
         for sim, s, (col, i0) in zip(b, insts, starts):
@@ -582,7 +583,8 @@ def run_batch(args, rank, local_rank):
             "data": "synthetic: hydrostatic column states + seeded 1e-3 velocity noise",
             "config": {"workload": "64 instances, T~U[100,400], nz in {24,32,40,48}, "
                                    "NX=NY=2nz, TRT 1/12 and 1e-6", "nodes": nodes,
-                       "autotune": bool(args.autotune)},
+                       "autotune": bool(args.autotune),
+                       "launches": "grouped" if args.batch_mode == 0 else "per-instance"},
             "nonfinite_instances": nonfinite}
     print(json.dumps(line), flush=True)
 
@@ -609,6 +611,8 @@ def main():
                          "time to saturated Nu_e on the reference's default case; batch: "
                          "the 64-instance batched T-sweep's step rate")
     ap.add_argument("--autotune", action="store_true", help="batch workload: autotune first")
+    ap.add_argument("--batch-mode", type=int, choices=[0, 1], default=0,
+                    help="batch workload: 0 grouped launches, 1 per-instance graph branches")
     ap.add_argument("--sat-max-steps", type=int, default=6_000_000)
     ap.add_argument("--ref-window", type=int, default=20_000,
                     help="reference arm of the saturation workload: steps it runs")

@@ -381,6 +381,48 @@ int ctx_launch_step(ehd_ctx *c, bool macros) {
     return r;
 }
 unsigned ctx_generation(const ehd_ctx *c) { return c->generation; }
+void ctx_tuning(const ehd_ctx *c, ehd_tuning *t) { *t = c->tune; }
+int ctx_step_args(ehd_ctx *c, bool macros, LbmArgs *la, StepConst *sc, ReduceDesc *rd,
+                  PoissonArgs *pa) {
+    (void)macros;
+    const int p = c->cur;
+    LbmArgs a{};
+    a.fa = c->f[p];
+    a.ha = c->h[p];
+    a.fb = c->f[p ^ 1];
+    a.hb = c->h[p ^ 1];
+    a.phip = c->phip;
+    a.ez00 = c->ez00;
+    a.exa = c->out[6];
+    a.eya = c->out[7];
+    a.eza = c->out[8];
+    a.q = c->q;
+    a.rho = c->rho;
+    a.u = c->u;
+    a.v = c->v;
+    a.w = c->w;
+    a.zref = c->ktab[p];
+    a.psum = c->psum;
+    a.err = c->err;
+    a.rows_grid = 0;
+    a.node_bx = c->tune.node_block_x;
+    *la = a;
+    *sc = c->sc;
+    // the reduction of lbm() for the per-node kernel's plane-sum slots
+    rd->psum = c->psum;
+    rd->m = c->mean[p ^ 1];
+    rd->msrc = c->mean[p];
+    rd->wdst = c->wref[p];
+    rd->wread = c->wref[p ^ 1];
+    rd->ktab = c->ktab[p ^ 1];
+    rd->nxy = c->sc.nxy;
+    rd->nblk = lbm_blocks_per_plane(c->p.nx, c->p.ny, c->tune.node_block_x);
+    rd->nz = c->p.nz;
+    // poisson() after lbm() reads the plane means of the new state
+    *pa = c->pa;
+    pa->qmean = c->mean[p ^ 1];
+    return EHD_OK;
+}
 double ctx_reference_current(const ehd_ctx *c) { return c->i0; }
 void ctx_commit_step(ehd_ctx *c) {
     c->cur ^= 1;

@@ -26,12 +26,14 @@ using namespace ehd;
 
 struct ehd_batch {
     int device = 0;
+    int mode = 0;  // 0: grouped launches, 1: per-instance graph branches
     cudaStream_t stream = nullptr;
     std::vector<ehd_ctx *> inst;
     std::vector<char> active;
     cudaEvent_t fork = nullptr, done = nullptr;
     std::vector<cudaEvent_t> join;
     std::map<std::string, cudaGraphExec_t> graphs;
+    std::map<std::string, std::vector<void *>> graph_bufs;  // descriptor arrays of a graph
 };
 
 namespace {
@@ -59,6 +61,108 @@ void drop(ehd_batch *b) {
     for (auto &kv : b->graphs)
         if (kv.second) cudaGraphExecDestroy(kv.second);
     b->graphs.clear();
+    for (auto &kv : b->graph_bufs)
+        for (void *p : kv.second) cudaFree(p);
+    b->graph_bufs.clear();
+}
+
+// A device copy of n host elements, recorded in bufs for release with the
+// graph that uses it.
+template <typename X>
+int upload(const X *host, size_t n, std::vector<void *> &bufs, X **dev) {
+    void *d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sizeof(X) * (n > 0 ? n : 1));
+    if (e != cudaSuccess) return cuda_fail("batch descriptors", e);
+    bufs.push_back(d);
+    if ((e = cudaMemcpy(d, host, sizeof(X) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return cuda_fail("batch descriptors", e);
+    *dev = (X *)d;
+    return EHD_OK;
+}
+
+// One group of instances with the same grid and launch shapes, and the
+// device descriptors of its launches.
+struct Group {
+    int nx = 0, ny = 0, nz = 0, n = 0;
+    void *lbm = nullptr;
+    ReduceDesc *red = nullptr;
+    PoissonArgs pa{};
+};
+
+template <typename T, typename R>
+int build_group(ehd_batch *b, const std::vector<size_t> &members, bool macros,
+                std::vector<void *> &bufs, Group *g) {
+    const int n = (int)members.size();
+    std::vector<LbmArgs> la(n);
+    std::vector<StepConst> sc(n);
+    std::vector<ReduceDesc> rd(n);
+    std::vector<PoissonPtrs> pp(n);
+    PoissonArgs pa0{};
+    for (int m = 0; m < n; ++m) {
+        PoissonArgs pa{};
+        int r = ctx_step_args(b->inst[members[m]], macros, &la[m], &sc[m], &rd[m], &pa);
+        if (r != EHD_OK) return r;
+        pp[m] = PoissonPtrs{pa.spec, pa.rowsum, pa.planesum, pa.phi00, pa.ez00,
+                            pa.q, pa.qmean, pa.phip, pa.dpw};
+        if (m == 0) pa0 = pa;
+    }
+    std::vector<unsigned char> host(lbm_group_desc_bytes<T, R>(n));
+    build_lbm_group_desc<T, R>(la.data(), sc.data(), n, host.data());
+    unsigned char *ld = nullptr;
+    int r = upload(host.data(), host.size(), bufs, &ld);
+    if (r == EHD_OK) r = upload(rd.data(), rd.size(), bufs, &g->red);
+    PoissonPtrs *pd = nullptr;
+    if (r == EHD_OK) r = upload(pp.data(), pp.size(), bufs, &pd);
+    if (r != EHD_OK) return r;
+    const ehd_params *p = ctx_params(b->inst[members[0]]);
+    g->nx = p->nx;
+    g->ny = p->ny;
+    g->nz = p->nz;
+    g->n = n;
+    g->lbm = ld;
+    g->pa = pa0;
+    g->pa.grp = pd;
+    g->pa.ngrp = n;
+    return EHD_OK;
+}
+
+template <typename T, typename R>
+int capture_groups(ehd_batch *b, const std::vector<char> &act, bool macros,
+                   std::vector<void *> &bufs, cudaGraph_t *graph) {
+    // instances with the same grid and launch shapes form one group
+    std::map<std::vector<int>, std::vector<size_t>> groups;
+    for (size_t i = 0; i < b->inst.size(); ++i) {
+        if (!act[i]) continue;
+        const ehd_params *p = ctx_params(b->inst[i]);
+        ehd_tuning t{};
+        ctx_tuning(b->inst[i], &t);
+        groups[{p->nx, p->ny, p->nz, t.node_block_x, t.fft_rows, t.fft_cols, t.poisson_path}]
+            .push_back(i);
+    }
+    std::vector<Group> gl;
+    for (auto &kv : groups) {
+        Group g;
+        int r = build_group<T, R>(b, kv.second, macros, bufs, &g);
+        if (r != EHD_OK) return r;
+        gl.push_back(g);
+    }
+    cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail("batch capture", e);
+    for (const Group &g : gl)
+        if (e == cudaSuccess) e = launch_lbm_group<T, R>(g.lbm, g.n, g.nx, g.ny, g.nz, macros, b->stream);
+    for (const Group &g : gl)
+        if (e == cudaSuccess) e = launch_reduce_tables_group<R>(g.red, g.n, g.nz, b->stream);
+    for (const Group &g : gl)
+        if (e == cudaSuccess) e = launch_poisson<R>(g.pa, b->stream);
+    cudaGraph_t gr = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(b->stream, &gr);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (gr) cudaGraphDestroy(gr);
+        cudaGetLastError();
+        return cuda_fail("batch group capture", e != cudaSuccess ? e : e2);
+    }
+    *graph = gr;
+    return EHD_OK;
 }
 
 // the graph of one step of the active instances in their present parities
@@ -81,6 +185,32 @@ int step_graph(ehd_batch *b, const std::vector<char> &act, bool macros, cudaGrap
         return EHD_OK;
     }
     cudaGraph_t g = nullptr;
+    if (b->mode == 0) {
+        // grouped launches: one launch per kernel over each group of instances
+        std::vector<void *> bufs;
+        int r = EHD_OK;
+        switch (ctx_precision(b->inst[0])) {
+            case EHD_PREC_FP64: r = capture_groups<double, double>(b, act, macros, bufs, &g); break;
+            case EHD_PREC_FP32: r = capture_groups<float, float>(b, act, macros, bufs, &g); break;
+            case EHD_PREC_FP16: r = capture_groups<__half, float>(b, act, macros, bufs, &g); break;
+            default: r = capture_groups<__nv_bfloat16, float>(b, act, macros, bufs, &g); break;
+        }
+        if (r != EHD_OK) {
+            for (void *p : bufs) cudaFree(p);
+            return r;
+        }
+        cudaGraphExec_t ge = nullptr;
+        cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            for (void *p : bufs) cudaFree(p);
+            return cuda_fail("batch graph instantiate", e);
+        }
+        b->graphs[key] = ge;
+        b->graph_bufs[key] = bufs;
+        *out = ge;
+        return EHD_OK;
+    }
     cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_fail("batch capture", e);
     int r = EHD_OK;
@@ -217,6 +347,15 @@ int ehd_batch_destroy(ehd_batch *b) {
 
 int ehd_batch_size(const ehd_batch *b) { return b ? (int)b->inst.size() : 0; }
 
+int ehd_batch_set_mode(ehd_batch *b, int mode) {
+    if (!b || (mode != 0 && mode != 1)) return err(EHD_ERR_INVALID, "ehd_batch_set_mode: bad arguments");
+    Dev dg(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    drop(b);
+    b->mode = mode;
+    return EHD_OK;
+}
+
 int ehd_batch_instance(ehd_batch *b, int i, ehd_ctx **ctx) {
     if (!b || !ctx || i < 0 || i >= (int)b->inst.size())
         return err(EHD_ERR_INVALID, "ehd_batch_instance: bad arguments");
@@ -352,6 +491,7 @@ int ehd_batch_autotune(ehd_batch *b, int trial_steps) {
     ehd_batch *s = nullptr;
     int r = ehd_batch_create(ps.data(), (int)n, &cfg, &s);
     if (r != EHD_OK) return r;
+    s->mode = b->mode;
     const std::vector<char> all(n, 1);
     for (size_t i = 0; r == EHD_OK && i < n; ++i) r = ehd_initialize(s->inst[i]);
     if (r == EHD_OK) r = batch_step(s, all, 1);
@@ -384,13 +524,19 @@ int ehd_batch_autotune(ehd_batch *b, int trial_steps) {
             return EHD_OK;
         };
         const ehd_params &p = ps[g.second.front()];
-        for (int kern = 0; r == EHD_OK && kern <= 1; ++kern)
+        // grouped launches run the per-node kernel: no row-kernel trials
+        for (int kern = 0; r == EHD_OK && kern <= (b->mode == 0 ? 0 : 1); ++kern)
             for (int bx = 16; r == EHD_OK && bx <= 128; bx *= 2) {
                 ehd_tuning t = best;
                 t.lbm_kernel = kern;
                 t.node_block_x = bx;
                 if (t.lbm_kernel != best.lbm_kernel || t.node_block_x != best.node_block_x) r = trial(t);
             }
+        if (r == EHD_OK) {  // the split-y or the five-kernel Poisson solve
+            ehd_tuning t = best;
+            t.poisson_path = 1 - best.poisson_path;
+            r = trial(t);
+        }
         if (!poisson_fast_size(p.nx))
             for (int rows = 1; r == EHD_OK && rows <= 32; rows *= 2) {
                 ehd_tuning t = best;

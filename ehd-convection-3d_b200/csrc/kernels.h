@@ -58,6 +58,31 @@ template <typename R>
 cudaError_t launch_reduce_tables(const float2 *psum, double *m, int nblk, const double *msrc,
                                  double *wdst, const double *wread, void *ktab,
                                  const StepConst &c, cudaStream_t s);
+// ---- launches over a group of instances with the same grid ----------------
+// (batch steps, csrc/batch.cu): one launch per kernel covers every instance.
+template <typename T, typename R>
+size_t lbm_group_desc_bytes(int n);
+// the n instances' arguments of one per-node step (default block shape) into
+// host memory of lbm_group_desc_bytes(n) bytes, to be copied to the device
+template <typename T, typename R>
+void build_lbm_group_desc(const LbmArgs *la, const StepConst *c, int n, void *host);
+template <typename T, typename R>
+cudaError_t launch_lbm_group(const void *desc_dev, int n, int nx, int ny, int nz, bool macros,
+                             cudaStream_t s);
+// one instance's arguments of launch_reduce_tables
+struct ReduceDesc {
+    const float2 *psum;
+    double *m;
+    const double *msrc;
+    double *wdst;
+    const double *wread;
+    void *ktab;
+    long long nxy;
+    int nblk, nz;
+};
+template <typename R>
+cudaError_t launch_reduce_tables_group(const ReduceDesc *desc_dev, int n, int nz, cudaStream_t s);
+
 // psum slots per plane of the per-node kernel with blocks of bx x (128 / bx)
 int lbm_blocks_per_plane(int nx, int ny, int bx);
 // the per-node kernel's default block width for a grid nx wide
@@ -96,6 +121,18 @@ struct FftPlan {
     int rad[kMaxRadix];
 };
 
+// Per-instance buffers of one Poisson solve in a launch over a group of
+// instances with the same grid (blockIdx.z selects the instance); the tables
+// (twiddles, eigenvalues, pivots) are the same for the whole group.
+struct PoissonPtrs {
+    void *spec;
+    double *rowsum, *planesum, *phi00, *ez00;
+    const void *q;
+    const double *qmean;
+    void *phip;
+    double2 *dpw;
+};
+
 // Buffers and sizes of the FFT / tridiagonal Poisson solve.  spec holds the
 // x,y spectrum of the planes z = 1..NZ-2 in the compute type, layout
 // [z-1][ky][kx] with kx pitch `pitch`; the z solve works on it in place.
@@ -123,6 +160,8 @@ struct PoissonArgs {
     const double *qmean;     // plane means {rho, q} of the current state, FP64: q_m = [2z+1]
     void *phip;              // output phi' (compute type)
     double eps, voltage, dz;
+    const PoissonPtrs *grp = nullptr;  // device array: a launch over ngrp instances
+    int ngrp = 1;
 };
 
 template <typename R>
@@ -159,6 +198,7 @@ int set_error(int code, const char *msg);
 
 struct ehd_ctx;
 struct ehd_params;
+struct ehd_tuning;
 namespace ehd {
 // a context's parameters and its physical time (for the text writers)
 const ::ehd_params *ctx_params(const ::ehd_ctx *c);
@@ -179,6 +219,13 @@ void ctx_commit_step(::ehd_ctx *c);
 // changes whenever the context's launches change (ehd_set_tuning), so that
 // captured graphs holding them are rebuilt
 unsigned ctx_generation(const ::ehd_ctx *c);
+// the context's launch shapes
+void ctx_tuning(const ::ehd_ctx *c, ::ehd_tuning *t);
+// the arguments of one steady step at the context's present buffer parity,
+// with the LBM half on the per-node kernel (what a launch over a group of
+// instances runs); nothing is launched
+int ctx_step_args(::ehd_ctx *c, bool macros, LbmArgs *la, StepConst *sc, ReduceDesc *rd,
+                  PoissonArgs *pa);
 double ctx_reference_current(const ::ehd_ctx *c);
 
 }  // namespace ehd

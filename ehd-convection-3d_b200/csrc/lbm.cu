@@ -549,14 +549,17 @@ __device__ __forceinline__ void finish_node(R (&f)[Q], R (&h)[Q], const Moments<
 //               read in place, without pull or injection rule;
 //   e_arrays:   E comes from the uploaded FP64 arrays instead of phi.
 // One thread per node, 128-thread blocks.
+// One block of the per-node step: block (bxi, byi) of a gx x gy tiling of
+// plane z (the grid indices are arguments so that a launch over several
+// instances can map its blocks).
 template <typename T, typename R, bool GENERAL, bool MACROS>
-__global__ void __launch_bounds__(128, sizeof(R) == 8 ? 2 : 4)
-lbm_step_kernel(const StepArgs<T, R> a, const KConst<R> c, int local_pops, int e_arrays) {
+__device__ __forceinline__ void node_block(const StepArgs<T, R> &a, const KConst<R> &c, int bxi,
+                                           int byi, int z, int gx, int gy, int local_pops,
+                                           int e_arrays) {
     const bool local = GENERAL && local_pops;
     const bool earr = GENERAL && e_arrays;
-    int x = blockIdx.x * blockDim.x + threadIdx.x;
-    int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z;
+    int x = bxi * blockDim.x + threadIdx.x;
+    int y = byi * blockDim.y + threadIdx.y;
     const bool inside = x < c.nx && y < c.ny;
     // lanes outside the grid work on a valid node so that the whole warp can
     // take part in the plane sums; they store nothing
@@ -575,11 +578,17 @@ lbm_step_kernel(const StepArgs<T, R> a, const KConst<R> c, int local_pops, int e
         const int tid = threadIdx.x + blockDim.x * threadIdx.y;
         const int wpb = (blockDim.x * blockDim.y) >> 5;
         warp_plane_sum(inside ? (float)mo.rho : 0.f, inside ? (float)mo.charge : 0.f, a.psum,
-                       (((size_t)z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) * wpb +
-                           (tid >> 5));
+                       (((size_t)z * gy + byi) * gx + bxi) * wpb + (tid >> 5));
     }
     if (!inside) return;
     finish_node<T, R, MACROS>(f, h, mo, x, y, z, node, zr, a, c, local, earr);
+}
+
+template <typename T, typename R, bool GENERAL, bool MACROS>
+__global__ void __launch_bounds__(128, sizeof(R) == 8 ? 2 : 4)
+lbm_step_kernel(const StepArgs<T, R> a, const KConst<R> c, int local_pops, int e_arrays) {
+    node_block<T, R, GENERAL, MACROS>(a, c, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x,
+                                      gridDim.y, local_pops, e_arrays);
 }
 
 // ---- bulk-copy row kernel ------------------------------------------------------
@@ -921,8 +930,7 @@ template cudaError_t prepare_lbm_rows<__half, float>(int, int, int, int *);
 template cudaError_t prepare_lbm_rows<__nv_bfloat16, float>(int, int, int, int *);
 
 template <typename T, typename R>
-cudaError_t launch_lbm_step(const LbmArgs &la, const StepConst &c, int local_pops, int e_arrays,
-                            bool macros, cudaStream_t s) {
+static StepArgs<T, R> make_step_args(const LbmArgs &la, const StepConst &c) {
     StepArgs<T, R> a;
     for (int d = 0; d < Q; ++d) {
         a.pp.fa[d] = (const T *)la.fa + (size_t)d * c.n;
@@ -943,6 +951,68 @@ cudaError_t launch_lbm_step(const LbmArgs &la, const StepConst &c, int local_pop
     a.zref = (const R *)la.zref;
     a.psum = la.psum;
     a.err = la.err;
+    return a;
+}
+
+// ---- launches over a group of instances with the same grid ----------------
+//
+// One launch of the per-node step covers every instance of the group: block
+// z = instance * NZ + plane.  Each block copies its instance's arguments and
+// constants (about 1.3 KB) into shared memory and runs the same node_block as
+// lbm_step_kernel, so an instance's result is bitwise that of a lone context
+// on the per-node kernel with the default block shape.
+template <typename T, typename R>
+struct LbmGroupDesc {
+    StepArgs<T, R> a;
+    KConst<R> k;
+};
+
+template <typename T, typename R, bool MACROS>
+__global__ void __launch_bounds__(128, sizeof(R) == 8 ? 2 : 4)
+lbm_group_kernel(const LbmGroupDesc<T, R> *__restrict__ desc, int nz) {
+    __shared__ LbmGroupDesc<T, R> sd;
+    const int inst = blockIdx.z / nz, z = blockIdx.z - inst * nz;
+    {
+        static_assert(sizeof(LbmGroupDesc<T, R>) % 8 == 0, "copied as 8-byte words");
+        constexpr int W = sizeof(LbmGroupDesc<T, R>) / 8;
+        const unsigned long long *src = reinterpret_cast<const unsigned long long *>(desc + inst);
+        unsigned long long *dst = reinterpret_cast<unsigned long long *>(&sd);
+        for (int i = threadIdx.x + blockDim.x * threadIdx.y; i < W; i += blockDim.x * blockDim.y)
+            dst[i] = src[i];
+    }
+    __syncthreads();
+    node_block<T, R, false, MACROS>(sd.a, sd.k, blockIdx.x, blockIdx.y, z, gridDim.x, gridDim.y,
+                                    0, 0);
+}
+
+template <typename T, typename R>
+size_t lbm_group_desc_bytes(int n) {
+    return sizeof(LbmGroupDesc<T, R>) * (size_t)n;
+}
+template <typename T, typename R>
+void build_lbm_group_desc(const LbmArgs *la, const StepConst *c, int n, void *host) {
+    LbmGroupDesc<T, R> *d = reinterpret_cast<LbmGroupDesc<T, R> *>(host);
+    for (int i = 0; i < n; ++i) {
+        d[i].a = make_step_args<T, R>(la[i], c[i]);
+        d[i].k = make_kconst<R>(c[i]);
+    }
+}
+template <typename T, typename R>
+cudaError_t launch_lbm_group(const void *desc_dev, int n, int nx, int ny, int nz, bool macros,
+                             cudaStream_t s) {
+    const int bx = lbm_default_block_x(nx);
+    const dim3 block(bx, 128 / bx, 1);
+    const dim3 grid((nx + bx - 1) / bx, (ny + block.y - 1) / block.y, nz * n);
+    const auto *d = reinterpret_cast<const LbmGroupDesc<T, R> *>(desc_dev);
+    if (macros) lbm_group_kernel<T, R, true><<<grid, block, 0, s>>>(d, nz);
+    else lbm_group_kernel<T, R, false><<<grid, block, 0, s>>>(d, nz);
+    return cudaGetLastError();
+}
+
+template <typename T, typename R>
+cudaError_t launch_lbm_step(const LbmArgs &la, const StepConst &c, int local_pops, int e_arrays,
+                            bool macros, cudaStream_t s) {
+    StepArgs<T, R> a = make_step_args<T, R>(la, c);
     const KConst<R> k = make_kconst<R>(c);
     const bool general = local_pops || e_arrays;
     if (!general && la.rows_grid > 0) {
@@ -1001,7 +1071,10 @@ cudaError_t launch_materialize(const void *rho, const void *u, const void *v, co
 }
 
 #define EHD_INST_LBM(T, R) template cudaError_t launch_lbm_step<T, R>(const LbmArgs &, \
-    const StepConst &, int, int, bool, cudaStream_t);
+    const StepConst &, int, int, bool, cudaStream_t); \
+    template size_t lbm_group_desc_bytes<T, R>(int); \
+    template void build_lbm_group_desc<T, R>(const LbmArgs *, const StepConst *, int, void *); \
+    template cudaError_t launch_lbm_group<T, R>(const void *, int, int, int, int, bool, cudaStream_t);
 EHD_INST_LBM(double, double)
 EHD_INST_LBM(float, float)
 EHD_INST_LBM(__half, float)
@@ -1158,6 +1231,23 @@ reduce_tables_kernel(const float2 *__restrict__ psum, double *__restrict__ m, in
     if ((int)blockIdx.x < nz) psum_reduce_block(psum, m, nblk, nxy, blockIdx.x);
     else build_tables_block<R>(msrc, wdst, wread, ktab, nz);
 }
+
+// reduce_tables_kernel over a group of instances with the same NZ: block
+// (b, i) is block b of instance i's reduction.
+template <typename R>
+__global__ void __launch_bounds__(256)
+reduce_tables_group_kernel(const ReduceDesc *__restrict__ desc) {
+    const ReduceDesc &r = desc[blockIdx.y];
+    if ((int)blockIdx.x < r.nz) psum_reduce_block(r.psum, r.m, r.nblk, r.nxy, blockIdx.x);
+    else build_tables_block<R>(r.msrc, r.wdst, r.wread, (R *)r.ktab, r.nz);
+}
+template <typename R>
+cudaError_t launch_reduce_tables_group(const ReduceDesc *desc_dev, int n, int nz, cudaStream_t s) {
+    reduce_tables_group_kernel<R><<<dim3(nz + 1, n), 256, 0, s>>>(desc_dev);
+    return cudaGetLastError();
+}
+template cudaError_t launch_reduce_tables_group<float>(const ReduceDesc *, int, int, cudaStream_t);
+template cudaError_t launch_reduce_tables_group<double>(const ReduceDesc *, int, int, cudaStream_t);
 
 cudaError_t launch_fields_plane_mean(const double *rho, const double *q, double *m,
                                      const StepConst &c, cudaStream_t s) {

@@ -213,7 +213,15 @@ __global__ void __launch_bounds__(256)
 poisson_rows_fwd(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec,
                  double *__restrict__ rowsum, const typename Cplx<R>::T *__restrict__ tw,
                  const double *__restrict__ qmean, FftPlan pl, int nx, int ny, int nxh, int pitch,
-                 int rows, double eps) {
+                 int rows, double eps,
+    const PoissonPtrs *__restrict__ grp) {
+    if (grp) {  // one instance of a group launch per blockIdx.z
+        const PoissonPtrs &gp = grp[blockIdx.z];
+        q = (const R *)gp.q;
+        spec = (typename Cplx<R>::T *)gp.spec;
+        rowsum = (double *)gp.rowsum;
+        qmean = (const double *)gp.qmean;
+    }
     using R2 = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R2 *a = reinterpret_cast<R2 *>(smem_raw);
@@ -269,7 +277,14 @@ template <typename R>
 __global__ void __launch_bounds__(256)
 poisson_cols(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::T *__restrict__ tw,
              FftPlan pl, int ny, int nxh, int pitch, int cols, R sign,
-             const double *__restrict__ rowsum, double *__restrict__ planesum) {
+             const double *__restrict__ rowsum, double *__restrict__ planesum,
+    const PoissonPtrs *__restrict__ grp) {
+    if (grp) {  // one instance of a group launch per blockIdx.z
+        const PoissonPtrs &gp = grp[blockIdx.z];
+        spec = (typename Cplx<R>::T *)gp.spec;
+        if (rowsum) rowsum = (const double *)gp.rowsum;
+        if (planesum) planesum = (double *)gp.planesum;
+    }
     using R2 = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R2 *a = reinterpret_cast<R2 *>(smem_raw);
@@ -303,7 +318,13 @@ template <typename R>
 __global__ void __launch_bounds__(256)
 poisson_rows_inv(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ phip,
                  const typename Cplx<R>::T *__restrict__ tw, FftPlan pl, int nx, int ny,
-                 int nxh, int pitch, int rows) {
+                 int nxh, int pitch, int rows,
+    const PoissonPtrs *__restrict__ grp) {
+    if (grp) {  // one instance of a group launch per blockIdx.z
+        const PoissonPtrs &gp = grp[blockIdx.z];
+        spec = (const typename Cplx<R>::T *)gp.spec;
+        phip = (R *)gp.phip;
+    }
     using R2 = typename Cplx<R>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R2 *a = reinterpret_cast<R2 *>(smem_raw);
@@ -360,7 +381,15 @@ template <typename R, int N>
 __global__ void __launch_bounds__(256)
 poisson_rows_fwd_fast(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec,
                       double *__restrict__ rowsum, const typename Cplx<R>::T *__restrict__ tw,
-                      const double *__restrict__ qmean, int ny, int nxh, int pitch, double eps) {
+                      const double *__restrict__ qmean, int ny, int nxh, int pitch, double eps,
+    const PoissonPtrs *__restrict__ grp) {
+    if (grp) {  // one instance of a group launch per blockIdx.z
+        const PoissonPtrs &gp = grp[blockIdx.z];
+        q = (const R *)gp.q;
+        spec = (typename Cplx<R>::T *)gp.spec;
+        rowsum = (double *)gp.rowsum;
+        qmean = (const double *)gp.qmean;
+    }
     using R2 = typename Cplx<R>::T;
     constexpr int G = fft::Plan<N>::G, TB = per_block<N>(), P = tstride<N>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -425,7 +454,14 @@ template <typename R, int N, int S>
 __global__ void __launch_bounds__(256)
 poisson_cols_fast(typename Cplx<R>::T *__restrict__ spec,
                   const typename Cplx<R>::T *__restrict__ tw, int nxh, int pitch,
-                  const double *__restrict__ rowsum, double *__restrict__ planesum) {
+                  const double *__restrict__ rowsum, double *__restrict__ planesum,
+    const PoissonPtrs *__restrict__ grp) {
+    if (grp) {  // one instance of a group launch per blockIdx.z
+        const PoissonPtrs &gp = grp[blockIdx.z];
+        spec = (typename Cplx<R>::T *)gp.spec;
+        if (rowsum) rowsum = (const double *)gp.rowsum;
+        if (planesum) planesum = (double *)gp.planesum;
+    }
     using R2 = typename Cplx<R>::T;
     constexpr int G = fft::Plan<N>::G, TB = per_block<N>(), P = tstride<N>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -467,7 +503,13 @@ poisson_cols_fast(typename Cplx<R>::T *__restrict__ spec,
 template <typename R, int N>
 __global__ void __launch_bounds__(256)
 poisson_rows_inv_fast(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ phip,
-                      const typename Cplx<R>::T *__restrict__ tw, int ny, int nxh, int pitch) {
+                      const typename Cplx<R>::T *__restrict__ tw, int ny, int nxh, int pitch,
+    const PoissonPtrs *__restrict__ grp) {
+    if (grp) {  // one instance of a group launch per blockIdx.z
+        const PoissonPtrs &gp = grp[blockIdx.z];
+        spec = (const typename Cplx<R>::T *)gp.spec;
+        phip = (R *)gp.phip;
+    }
     using R2 = typename Cplx<R>::T;
     constexpr int G = fft::Plan<N>::G, TB = per_block<N>(), P = tstride<N>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -543,7 +585,17 @@ poisson_zsolve(typename Cplx<R>::T *__restrict__ spec, const double *__restrict_
                double2 *__restrict__ dpw, const double *__restrict__ planesum,
                const double *__restrict__ qmean, double *__restrict__ phi00,
                double *__restrict__ ez00, int nx, int ny, int nz, int nxh, int pitch,
-               double dz, double eps, double voltage) {
+               double dz, double eps, double voltage,
+    const PoissonPtrs *__restrict__ grp) {
+    if (grp) {  // one instance of a group launch per blockIdx.z
+        const PoissonPtrs &gp = grp[blockIdx.z];
+        spec = (typename Cplx<R>::T *)gp.spec;
+        dpw = (double2 *)gp.dpw;
+        planesum = (const double *)gp.planesum;
+        qmean = (const double *)gp.qmean;
+        phi00 = (double *)gp.phi00;
+        ez00 = (double *)gp.ez00;
+    }
     using R2 = typename Cplx<R>::T;
     const int modes = nxh * ny;
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -646,7 +698,16 @@ poisson_zdst(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::T *
              const R *__restrict__ lamz, const double *__restrict__ planesum,
              const double *__restrict__ qmean, double *__restrict__ phi00,
              double *__restrict__ ez00, int nx, int ny, int nxh, int pitch, double dz,
-             double eps, double voltage, double kx0, double ky0) {
+             double eps, double voltage, double kx0, double ky0,
+    const PoissonPtrs *__restrict__ grp) {
+    if (grp) {  // one instance of a group launch per blockIdx.z
+        const PoissonPtrs &gp = grp[blockIdx.z];
+        spec = (typename Cplx<R>::T *)gp.spec;
+        planesum = (const double *)gp.planesum;
+        qmean = (const double *)gp.qmean;
+        phi00 = (double *)gp.phi00;
+        ez00 = (double *)gp.ez00;
+    }
     using R2 = typename Cplx<R>::T;
     constexpr int G = fft::Plan<L>::G, TB = 256 / G, P = tstride<L>();
     constexpr int n = L / 2 - 1, nz = n + 2;
@@ -770,7 +831,16 @@ poisson_zdst_rt(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::
                 const R *__restrict__ lamz, FftPlan pl, const double *__restrict__ planesum,
                 const double *__restrict__ qmean, double *__restrict__ phi00,
                 double *__restrict__ ez00, int nx, int ny, int nxh, int pitch, int tb, double dz,
-                double eps, double voltage, double kx0, double ky0) {
+                double eps, double voltage, double kx0, double ky0,
+    const PoissonPtrs *__restrict__ grp) {
+    if (grp) {  // one instance of a group launch per blockIdx.z
+        const PoissonPtrs &gp = grp[blockIdx.z];
+        spec = (typename Cplx<R>::T *)gp.spec;
+        planesum = (const double *)gp.planesum;
+        qmean = (const double *)gp.qmean;
+        phi00 = (double *)gp.phi00;
+        ez00 = (double *)gp.ez00;
+    }
     using R2 = typename Cplx<R>::T;
     const int L = pl.n, n = L / 2 - 1, nz = n + 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -948,7 +1018,15 @@ __global__ void __launch_bounds__(256)
 poisson_rows_fwd_split(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spl,
                        double *__restrict__ rowsum, const typename Cplx<R>::T *__restrict__ tw,
                        const typename Cplx<R>::T *__restrict__ twy,
-                       const double *__restrict__ qmean, int nzi, int nxh, double eps) {
+                       const double *__restrict__ qmean, int nzi, int nxh, double eps,
+    const PoissonPtrs *__restrict__ grp) {
+    if (grp) {  // one instance of a group launch per blockIdx.z
+        const PoissonPtrs &gp = grp[blockIdx.z];
+        q = (const R *)gp.q;
+        spl = (typename Cplx<R>::T *)gp.spec;
+        rowsum = (double *)gp.rowsum;
+        qmean = (const double *)gp.qmean;
+    }
     using R2 = typename Cplx<R>::T;
     constexpr int G = fft::Plan<N>::G, TB = per_block<N>(), P = tstride<N>();
     constexpr int NY = 64 * S, GB = 2 * TB / S;
@@ -1042,7 +1120,17 @@ poisson_slab(typename Cplx<R>::T *__restrict__ spl, const typename Cplx<R>::T *_
              const double *__restrict__ rowsum, double *__restrict__ planesum,
              const double *__restrict__ qmean, double *__restrict__ phi00,
              double *__restrict__ ez00, int nx, int nxh, double dz, double eps,
-             double voltage, double kx0, double ky0) {
+             double voltage, double kx0, double ky0,
+    const PoissonPtrs *__restrict__ grp) {
+    if (grp) {  // one instance of a group launch per blockIdx.z
+        const PoissonPtrs &gp = grp[blockIdx.z];
+        spl = (typename Cplx<R>::T *)gp.spec;
+        rowsum = (const double *)gp.rowsum;
+        planesum = (double *)gp.planesum;
+        qmean = (const double *)gp.qmean;
+        phi00 = (double *)gp.phi00;
+        ez00 = (double *)gp.ez00;
+    }
     using R2 = typename Cplx<R>::T;
     constexpr int NY = 64 * S;
     constexpr int n = L / 2 - 1, nz = n + 2;
@@ -1192,7 +1280,13 @@ template <typename R, int N, int S>
 __global__ void __launch_bounds__(256)
 poisson_rows_inv_split(const typename Cplx<R>::T *__restrict__ spl, R *__restrict__ phip,
                        const typename Cplx<R>::T *__restrict__ tw,
-                       const typename Cplx<R>::T *__restrict__ twy, int nzi, int nxh) {
+                       const typename Cplx<R>::T *__restrict__ twy, int nzi, int nxh,
+    const PoissonPtrs *__restrict__ grp) {
+    if (grp) {  // one instance of a group launch per blockIdx.z
+        const PoissonPtrs &gp = grp[blockIdx.z];
+        spl = (const typename Cplx<R>::T *)gp.spec;
+        phip = (R *)gp.phip;
+    }
     using R2 = typename Cplx<R>::T;
     constexpr int G = fft::Plan<N>::G, TB = per_block<N>(), P = tstride<N>();
     constexpr int NY = 64 * S, GB = 2 * TB / S;
@@ -1290,10 +1384,10 @@ static cudaError_t rows_fwd_fast(const PoissonArgs &a, cudaStream_t s) {
     const size_t sm = sizeof(R2) * ((size_t)N + (size_t)TB * tstride<N>());
     cudaError_t e = set_smem(poisson_rows_fwd_fast<R, N>, sm, s);
     if (e != cudaSuccess) return e;
-    dim3 grid((a.ny + 2 * TB - 1) / (2 * TB), a.nz - 2);
+    dim3 grid((a.ny + 2 * TB - 1) / (2 * TB), a.nz - 2, a.ngrp);
     poisson_rows_fwd_fast<R, N><<<grid, 256, sm, s>>>((const R *)a.q, (R2 *)a.spec, a.rowsum,
                                                        (const R2 *)a.twx, a.qmean,
-                                                       a.ny, a.nxh, a.pitch, a.eps);
+                                                       a.ny, a.nxh, a.pitch, a.eps, a.grp);
     return cudaGetLastError();
 }
 template <typename R, int N>
@@ -1303,9 +1397,9 @@ static cudaError_t rows_inv_fast(const PoissonArgs &a, cudaStream_t s) {
     const size_t sm = sizeof(R2) * ((size_t)N + (size_t)TB * tstride<N>());
     cudaError_t e = set_smem(poisson_rows_inv_fast<R, N>, sm, s);
     if (e != cudaSuccess) return e;
-    dim3 grid((a.ny + 2 * TB - 1) / (2 * TB), a.nz - 2);
+    dim3 grid((a.ny + 2 * TB - 1) / (2 * TB), a.nz - 2, a.ngrp);
     poisson_rows_inv_fast<R, N><<<grid, 256, sm, s>>>((const R2 *)a.spec, (R *)a.phip,
-                                                       (const R2 *)a.twx, a.ny, a.nxh, a.pitch);
+                                                       (const R2 *)a.twx, a.ny, a.nxh, a.pitch, a.grp);
     return cudaGetLastError();
 }
 template <typename R, int N, int S>
@@ -1315,9 +1409,9 @@ static cudaError_t cols_fast(const PoissonArgs &a, cudaStream_t s) {
     const size_t sm = sizeof(R2) * ((size_t)N + (size_t)TB * tstride<N>());
     cudaError_t e = set_smem(poisson_cols_fast<R, N, S>, sm, s);
     if (e != cudaSuccess) return e;
-    dim3 grid((a.nxh + TB - 1) / TB, a.nz - 2);
+    dim3 grid((a.nxh + TB - 1) / TB, a.nz - 2, a.ngrp);
     poisson_cols_fast<R, N, S><<<grid, 256, sm, s>>>((R2 *)a.spec, (const R2 *)a.twy, a.nxh,
-                                                      a.pitch, a.rowsum, a.planesum);
+                                                      a.pitch, a.rowsum, a.planesum, a.grp);
     return cudaGetLastError();
 }
 
@@ -1335,10 +1429,10 @@ static cudaError_t rows_fwd(const PoissonArgs &a, cudaStream_t s) {
     const size_t sm = (size_t)(2 * rows + 1) * a.nx * sizeof(R2);
     cudaError_t e = set_smem(poisson_rows_fwd<R>, sm, s);
     if (e != cudaSuccess) return e;
-    dim3 grid((a.ny + rows - 1) / rows, a.nz - 2);
+    dim3 grid((a.ny + rows - 1) / rows, a.nz - 2, a.ngrp);
     poisson_rows_fwd<R><<<grid, 256, sm, s>>>((const R *)a.q, (R2 *)a.spec, a.rowsum,
                                                (const R2 *)a.twx, a.qmean, a.px,
-                                               a.nx, a.ny, a.nxh, a.pitch, rows, a.eps);
+                                               a.nx, a.ny, a.nxh, a.pitch, rows, a.eps, a.grp);
     return cudaGetLastError();
 }
 template <typename R>
@@ -1355,10 +1449,10 @@ static cudaError_t rows_inv(const PoissonArgs &a, cudaStream_t s) {
     const size_t sm = (size_t)(2 * rows + 1) * a.nx * sizeof(R2);
     cudaError_t e = set_smem(poisson_rows_inv<R>, sm, s);
     if (e != cudaSuccess) return e;
-    dim3 grid((a.ny + rows - 1) / rows, a.nz - 2);
+    dim3 grid((a.ny + rows - 1) / rows, a.nz - 2, a.ngrp);
     poisson_rows_inv<R><<<grid, 256, sm, s>>>((const R2 *)a.spec, (R *)a.phip,
                                                (const R2 *)a.twx, a.px, a.nx, a.ny, a.nxh,
-                                               a.pitch, rows);
+                                               a.pitch, rows, a.grp);
     return cudaGetLastError();
 }
 template <typename R, int S>
@@ -1375,10 +1469,10 @@ static cudaError_t cols(const PoissonArgs &a, cudaStream_t s) {
     const size_t sm = (size_t)(2 * cc + 1) * a.ny * sizeof(R2);
     cudaError_t e = set_smem(poisson_cols<R>, sm, s);
     if (e != cudaSuccess) return e;
-    dim3 grid((a.nxh + cc - 1) / cc, a.nz - 2);
+    dim3 grid((a.nxh + cc - 1) / cc, a.nz - 2, a.ngrp);
     poisson_cols<R><<<grid, 256, sm, s>>>((R2 *)a.spec, (const R2 *)a.twy, a.py, a.ny, a.nxh,
                                            a.pitch, cc, (R)S, S < 0 ? a.rowsum : nullptr,
-                                           S < 0 ? a.planesum : nullptr);
+                                           S < 0 ? a.planesum : nullptr, a.grp);
     return cudaGetLastError();
 }
 
@@ -1391,9 +1485,9 @@ static cudaError_t zdst(const PoissonArgs &a, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     const int modes = a.nxh * a.ny;
     const R2 *tw = (const R2 *)a.twz;
-    poisson_zdst<R, L><<<(modes + TB - 1) / TB, 256, sm, s>>>(
+    poisson_zdst<R, L><<<dim3((modes + TB - 1) / TB, 1, a.ngrp), 256, sm, s>>>(
         (R2 *)a.spec, tw, (const R *)(tw + L), a.planesum, a.qmean, a.phi00, a.ez00, a.nx, a.ny,
-        a.nxh, a.pitch, a.dz, a.eps, a.voltage, 2.0 * M_PI / a.lx, 2.0 * M_PI / a.ly);
+        a.nxh, a.pitch, a.dz, a.eps, a.voltage, 2.0 * M_PI / a.lx, 2.0 * M_PI / a.ly, a.grp);
     return cudaGetLastError();
 }
 
@@ -1421,9 +1515,9 @@ static cudaError_t split_rows_fwd(const PoissonArgs &a, cudaStream_t s) {
     const size_t sm = sizeof(R2) * ((size_t)N + (size_t)TB * tstride<N>());
     cudaError_t e = set_smem(poisson_rows_fwd_split<R, N, S>, sm, s);
     if (e != cudaSuccess) return e;
-    poisson_rows_fwd_split<R, N, S><<<dim3(64 / NB, a.nz - 2), 256, sm, s>>>(
+    poisson_rows_fwd_split<R, N, S><<<dim3(64 / NB, a.nz - 2, a.ngrp), 256, sm, s>>>(
         (const R *)a.q, (R2 *)a.spec, a.rowsum, (const R2 *)a.twx, (const R2 *)a.twy, a.qmean,
-        a.nz - 2, a.nxh, a.eps);
+        a.nz - 2, a.nxh, a.eps, a.grp);
     return cudaGetLastError();
 }
 template <typename R, int N, int S>
@@ -1433,8 +1527,8 @@ static cudaError_t split_rows_inv(const PoissonArgs &a, cudaStream_t s) {
     constexpr size_t sm = rows_inv_split_smem<R, N, S>();
     cudaError_t e = set_smem(poisson_rows_inv_split<R, N, S>, sm, s);
     if (e != cudaSuccess) return e;
-    poisson_rows_inv_split<R, N, S><<<dim3(64 / NB, a.nz - 2), 256, sm, s>>>(
-        (const R2 *)a.spec, (R *)a.phip, (const R2 *)a.twx, (const R2 *)a.twy, a.nz - 2, a.nxh);
+    poisson_rows_inv_split<R, N, S><<<dim3(64 / NB, a.nz - 2, a.ngrp), 256, sm, s>>>(
+        (const R2 *)a.spec, (R *)a.phip, (const R2 *)a.twx, (const R2 *)a.twy, a.nz - 2, a.nxh, a.grp);
     return cudaGetLastError();
 }
 template <typename R, int L, int S>
@@ -1444,10 +1538,10 @@ static cudaError_t split_slab(const PoissonArgs &a, cudaStream_t s) {
     cudaError_t e = set_smem(poisson_slab<R, L, S>, sm, s);
     if (e != cudaSuccess) return e;
     const R2 *tw = (const R2 *)a.twz;
-    poisson_slab<R, L, S><<<dim3(a.nxh, S), 256, sm, s>>>(
+    poisson_slab<R, L, S><<<dim3(a.nxh, S, a.ngrp), 256, sm, s>>>(
         (R2 *)a.spec, (const R2 *)a.twy, tw, (const R *)(tw + L), a.rowsum, a.planesum, a.qmean,
         a.phi00, a.ez00, a.nx, a.nxh, a.dz, a.eps, a.voltage, 2.0 * M_PI / a.lx,
-        2.0 * M_PI / a.ly);
+        2.0 * M_PI / a.ly, a.grp);
     return cudaGetLastError();
 }
 
@@ -1572,16 +1666,16 @@ cudaError_t launch_poisson(const PoissonArgs &a, cudaStream_t s) {
         const size_t sm = zdst_rt_smem(L, a.ztb, sizeof(R));
         if ((e = set_smem(poisson_zdst_rt<R>, sm, s)) != cudaSuccess) return e;
         const R2 *tw = (const R2 *)a.twz;
-        poisson_zdst_rt<R><<<(modes + a.ztb - 1) / a.ztb, 256, sm, s>>>(
+        poisson_zdst_rt<R><<<dim3((modes + a.ztb - 1) / a.ztb, 1, a.ngrp), 256, sm, s>>>(
             (R2 *)a.spec, tw, (const R *)(tw + L), a.pz, a.planesum, a.qmean, a.phi00, a.ez00,
             a.nx, a.ny, a.nxh, a.pitch, a.ztb, a.dz, a.eps, a.voltage, 2.0 * M_PI / a.lx,
-            2.0 * M_PI / a.ly);
+            2.0 * M_PI / a.ly, a.grp);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     } else {
         const int modes = a.nxh * a.ny;
-        poisson_zsolve<R><<<(modes + 127) / 128, 128, 0, s>>>(
+        poisson_zsolve<R><<<dim3((modes + 127) / 128, 1, a.ngrp), 128, 0, s>>>(
             (R2 *)a.spec, a.cpt, a.dpw, a.planesum, a.qmean, a.phi00, a.ez00, a.nx, a.ny, a.nz,
-            a.nxh, a.pitch, a.dz, a.eps, a.voltage);
+            a.nxh, a.pitch, a.dz, a.eps, a.voltage, a.grp);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if ((e = cols<R, 1>(a, s)) != cudaSuccess) return e;

@@ -123,6 +123,7 @@ SIGNATURES = {
     "ehd_batch_size": (_i, [_vp]),
     "ehd_batch_instance": (_i, [_vp, _i, ctypes.POINTER(_vp)]),
     "ehd_batch_set_active": (_i, [_vp, _i, _i]),
+    "ehd_batch_set_mode": (_i, [_vp, _i]),
     "ehd_batch_step": (_i, [_vp, _i]),
     "ehd_batch_run_to_saturation": (_i, [_vp, _i, ctypes.c_double, _i, ctypes.c_int64,
                                          ctypes.POINTER(ctypes.c_int32),
@@ -403,6 +404,11 @@ class Batch:
 
     def set_active(self, i: int, active: bool):
         _check(lib().ehd_batch_set_active(self.h, int(i), int(bool(active))))
+
+    def set_mode(self, mode: int):
+        """ehd_batch_set_mode: 0 grouped launches (default), 1 per-instance
+        graph branches."""
+        _check(lib().ehd_batch_set_mode(self.h, int(mode)))
 
     def step(self, n: int = 1):
         _check(lib().ehd_batch_step(self.h, int(n)))

@@ -265,6 +265,15 @@ int ehd_batch_size(const ehd_batch *batch);
  * batch owns it. */
 int ehd_batch_instance(ehd_batch *batch, int i, ehd_ctx **ctx);
 int ehd_batch_set_active(ehd_batch *batch, int i, int active);
+/* How a batch step launches its instances (no reference counterpart).
+ * mode 0 (the default): instances with the same grid and launch shapes form a
+ * group, and each kernel of the step is one launch over every instance of a
+ * group (the LBM half on the per-node kernel, each instance's result bitwise
+ * that of a lone context on the per-node kernel with the same shapes); one
+ * CUDA graph per step holds the groups' launches.  mode 1: one graph per step
+ * with a branch per instance holding that instance's own launches (the row
+ * kernel where it applies). */
+int ehd_batch_set_mode(ehd_batch *batch, int mode);
 /* nsteps steps of every active instance.  Instances whose next step is the
  * first after an upload take that step on their own streams; after it, one
  * graph launch per step covers all active instances. */

@@ -1,8 +1,12 @@
 """Batches of independent instances (ehd_batch): one graph launch per step over
 every active instance, per-instance run to saturation, and the autotuner.
 
-A batch instance runs the same kernels with the same launch shapes as a lone
-context, so the checks are bitwise against lone contexts.
+Mode 0 (grouped launches, the default): each kernel of a step is one launch
+over every instance with the same grid, the LBM half on the per-node kernel,
+so an instance's result is bitwise that of a lone context on the per-node
+kernel.  Mode 1 (a graph branch per instance): an instance runs the same
+kernels with the same launch shapes as a lone context.  Both are checked
+bitwise against lone contexts.
 """
 import numpy as np
 import pytest
@@ -31,17 +35,21 @@ def fields(p, seed):
     return M.random_fields(p, seed)
 
 
-def test_batch_steps_match_lone_contexts_bitwise():
+@pytest.mark.parametrize("mode", [0, 1])
+def test_batch_steps_match_lone_contexts_bitwise(mode):
     ps = [params(s, T) for s, T in zip(SHAPES, (150.0, 250.0, 350.0))]
+    # a fourth instance on the first grid: a group of two in mode 0
+    ps.append(params(SHAPES[0], 300.0))
     fs = [fields(p, 30 + i) for i, p in enumerate(ps)]
     lone = []
     for p, f in zip(ps, fs):
-        with ehd.Simulation(to_ehd(p), "fp32") as sim:
+        with ehd.Simulation(to_ehd(p), "fp32", row_kernel=mode == 1) as sim:
             sim.set_fields(f)
             sim.step(4)
             sim.step(6)
             lone.append((sim.get_fields(), sim.diagnostics()))
     with ehd.Batch([to_ehd(p) for p in ps], "fp32") as b:
+        b.set_mode(mode)
         for sim, f in zip(b, fs):
             sim.set_fields(f)
         b.step(4)
@@ -72,7 +80,8 @@ def test_batch_inactive_instances_do_not_advance():
         assert b[1].diagnostics()["step"] == 5
 
 
-def test_batch_run_to_saturation_matches_lone_runs():
+@pytest.mark.parametrize("mode", [0, 1])
+def test_batch_run_to_saturation_matches_lone_runs(mode):
     """Each instance stops on its own: the same sampling and stopping as
     ehd_run_to_saturation on a lone context, instance by instance."""
     ps = [params(s, T) for s, T in zip(SHAPES, (150.0, 250.0, 350.0))]
@@ -83,11 +92,12 @@ def test_batch_run_to_saturation_matches_lone_runs():
     # tolerances that stop the instances after different numbers of samples
     lone = []
     for (prof, i0), p in zip(starts, ps):
-        with ehd.Simulation(to_ehd(p), "fp32") as sim:
+        with ehd.Simulation(to_ehd(p), "fp32", row_kernel=mode == 1) as sim:
             sim.set_state_seeded(prof, seed=3, amp=1e-3)
             sim.set_reference_current(i0)
             lone.append(sim.run_to_saturation(sample_every=20, tol=2e-2, hold=2, max_steps=200))
     with ehd.Batch([to_ehd(p) for p in ps], "fp32") as b:
+        b.set_mode(mode)
         for sim, (prof, i0) in zip(b, starts):
             sim.set_state_seeded(prof, seed=3, amp=1e-3)
             sim.set_reference_current(i0)
