@@ -86,7 +86,7 @@ struct ehd_ctx {
     StepConst sc{};
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    size_t tsize = 8, rsize = 8;  // storage / compute bytes
+    size_t fsize = 8, gsize = 8, rsize = 8;  // f and g storage, compute bytes
     std::vector<void *> allocs;
     size_t bytes = 0;
 
@@ -242,6 +242,7 @@ int lbm(ehd_ctx *c, bool macros) {
         case EHD_PREC_FP32: e = launch_lbm_step<float, float>(a, c->sc, loc, ea, macros, c->stream); break;
         case EHD_PREC_FP16: e = launch_lbm_step<__half, float>(a, c->sc, loc, ea, macros, c->stream); break;
         case EHD_PREC_BF16: e = launch_lbm_step<__nv_bfloat16, float>(a, c->sc, loc, ea, macros, c->stream); break;
+        case EHD_PREC_MIXED: e = launch_lbm_step<Mix16, float>(a, c->sc, loc, ea, macros, c->stream); break;
     }
     if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "LBM step launch: %s", cudaGetErrorString(e));
     // plane means of the new state, then the references of the next step:
@@ -335,6 +336,7 @@ int after_upload(ehd_ctx *c) {
         case EHD_PREC_FP64: e = launch_init_equilibrium<double>(c->f[c->cur], c->h[c->cur], c->out, c->wref[p], c->sc, c->stream); break;
         case EHD_PREC_FP32: e = launch_init_equilibrium<float>(c->f[c->cur], c->h[c->cur], c->out, c->wref[p], c->sc, c->stream); break;
         case EHD_PREC_FP16: e = launch_init_equilibrium<__half>(c->f[c->cur], c->h[c->cur], c->out, c->wref[p], c->sc, c->stream); break;
+        case EHD_PREC_MIXED: e = launch_init_equilibrium<Mix16>(c->f[c->cur], c->h[c->cur], c->out, c->wref[p], c->sc, c->stream); break;
         default: e = launch_init_equilibrium<__nv_bfloat16>(c->f[c->cur], c->h[c->cur], c->out, c->wref[p], c->sc, c->stream); break;
     }
     if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "init_equilibrium: %s", cudaGetErrorString(e));
@@ -469,7 +471,7 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
     if (r != EHD_OK) return r;
     ehd_config cfg{};
     if (config) cfg = *config;
-    if (cfg.precision < EHD_PREC_FP64 || cfg.precision > EHD_PREC_BF16)
+    if (cfg.precision < EHD_PREC_FP64 || cfg.precision > EHD_PREC_MIXED)
         return fail(EHD_ERR_INVALID, "unknown precision %d", cfg.precision);
     int ndev = 0;
     EHD_CK(cudaGetDeviceCount(&ndev));
@@ -485,7 +487,8 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
     c->device = cfg.device;
     c->sc = make_const(params);
     c->use_graphs = !(cfg.flags & EHD_FLAG_NO_GRAPH);
-    c->tsize = c->prec == EHD_PREC_FP64 ? 8 : (c->prec == EHD_PREC_FP32 ? 4 : 2);
+    c->fsize = c->prec == EHD_PREC_FP64 ? 8 : (c->prec == EHD_PREC_FP32 ? 4 : 2);
+    c->gsize = c->prec == EHD_PREC_FP64 ? 8 : (c->prec == EHD_PREC_FP32 || c->prec == EHD_PREC_MIXED ? 4 : 2);
     c->rsize = c->prec == EHD_PREC_FP64 ? 8 : 4;
     auto bail = [&](int code) {
         ehd_destroy(c);
@@ -504,8 +507,8 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
     const size_t n = (size_t)c->sc.n;
     const int nx = params->nx, ny = params->ny, nz = params->nz;
     for (int i = 0; i < 2; ++i) {
-        if ((r = dalloc(c, &c->f[i], (size_t)Q * n * c->tsize))) return bail(r);
-        if ((r = dalloc(c, &c->h[i], (size_t)Q * n * c->tsize))) return bail(r);
+        if ((r = dalloc(c, &c->f[i], (size_t)Q * n * c->fsize))) return bail(r);
+        if ((r = dalloc(c, &c->h[i], (size_t)Q * n * c->gsize))) return bail(r);
     }
     void **macro[] = {&c->q, &c->rho, &c->u, &c->v, &c->w, &c->phip};
     for (void **m : macro)
@@ -527,6 +530,7 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
             case EHD_PREC_FP64: e = prepare_lbm_rows<double, double>(nx, ny, nz, &c->rows_grid); break;
             case EHD_PREC_FP32: e = prepare_lbm_rows<float, float>(nx, ny, nz, &c->rows_grid); break;
             case EHD_PREC_FP16: e = prepare_lbm_rows<__half, float>(nx, ny, nz, &c->rows_grid); break;
+            case EHD_PREC_MIXED: e = prepare_lbm_rows<Mix16, float>(nx, ny, nz, &c->rows_grid); break;
             default: e = prepare_lbm_rows<__nv_bfloat16, float>(nx, ny, nz, &c->rows_grid); break;
         }
         if (e != cudaSuccess) return bail(fail(EHD_ERR_CUDA, "row kernel set-up: %s", cudaGetErrorString(e)));
@@ -979,7 +983,8 @@ int ehd_set_state_from_column(ehd_ctx *c, ehd_ctx *col, uint64_t seed, double am
         return fail(EHD_ERR_INVALID, "column: parameters differ from the context's");
     if (!col->have_state || col->pops_local || col->e_arrays)
         return fail(EHD_ERR_STATE, "column: needs a state stepped at least once since its upload");
-    if (col->tsize < 4) return fail(EHD_ERR_INVALID, "column: FP64 or FP32 populations needed");
+    if (col->fsize < 4 || col->gsize < 4)
+        return fail(EHD_ERR_INVALID, "column: FP64 or FP32 populations needed");
     const int nz = c->p.nz;
     const size_t nzs = (size_t)nz;
     // the column's fields, population values and tables, on the host
@@ -988,7 +993,7 @@ int ehd_set_state_from_column(ehd_ctx *c, ehd_ctx *col, uint64_t seed, double am
                            prof.data() + 3 * nzs, prof.data() + 4 * nzs, prof.data() + 5 * nzs,
                            prof.data() + 6 * nzs, prof.data() + 7 * nzs, prof.data() + 8 * nzs);
     if (r != EHD_OK) return r;
-    std::vector<unsigned char> fb(Q * nzs * col->tsize), hb(Q * nzs * col->tsize);
+    std::vector<unsigned char> fb(Q * nzs * col->fsize), hb(Q * nzs * col->gsize);
     std::vector<unsigned char> kt[2] = {std::vector<unsigned char>(10 * nzs * col->rsize),
                                         std::vector<unsigned char>(10 * nzs * col->rsize)};
     std::vector<double> wref[2] = {std::vector<double>(2 * nzs), std::vector<double>(2 * nzs)};
@@ -1011,8 +1016,8 @@ int ehd_set_state_from_column(ehd_ctx *c, ehd_ctx *col, uint64_t seed, double am
     std::vector<double> colv(2 * Q * nzs);
     for (int d = 0; d < Q; ++d)
         for (size_t z = 0; z < nzs; ++z) {
-            colv[d * nzs + z] = read_real(fb, d * nzs + z, col->tsize) + w_of(d) * wc[2 * z];
-            colv[(Q + d) * nzs + z] = read_real(hb, d * nzs + z, col->tsize) + w_of(d) * wc[2 * z + 1];
+            colv[d * nzs + z] = read_real(fb, d * nzs + z, col->fsize) + w_of(d) * wc[2 * z];
+            colv[(Q + d) * nzs + z] = read_real(hb, d * nzs + z, col->gsize) + w_of(d) * wc[2 * z + 1];
         }
     // the step kernel's tables in this context's compute type
     for (int k = 0; k < 2; ++k) {
@@ -1045,6 +1050,7 @@ int ehd_set_state_from_column(ehd_ctx *c, ehd_ctx *col, uint64_t seed, double am
             case EHD_PREC_FP64: e = launch_column_state<double, double>(f, h, c->out_dev, c->prof_dev, colv_dev, ref, c->phip, c->phi00, c->sc, c->stream); break;
             case EHD_PREC_FP32: e = launch_column_state<float, float>(f, h, c->out_dev, c->prof_dev, colv_dev, ref, c->phip, c->phi00, c->sc, c->stream); break;
             case EHD_PREC_FP16: e = launch_column_state<__half, float>(f, h, c->out_dev, c->prof_dev, colv_dev, ref, c->phip, c->phi00, c->sc, c->stream); break;
+            case EHD_PREC_MIXED: e = launch_column_state<Mix16, float>(f, h, c->out_dev, c->prof_dev, colv_dev, ref, c->phip, c->phi00, c->sc, c->stream); break;
             default: e = launch_column_state<__nv_bfloat16, float>(f, h, c->out_dev, c->prof_dev, colv_dev, ref, c->phip, c->phi00, c->sc, c->stream); break;
         }
     }
@@ -1160,7 +1166,7 @@ struct Blob {
 std::vector<Blob> state_blobs(ehd_ctx *c) {
     const size_t n = (size_t)c->sc.n, nz = (size_t)c->p.nz;
     std::vector<Blob> b = {
-        {c->f[c->cur], (size_t)Q * n * c->tsize}, {c->h[c->cur], (size_t)Q * n * c->tsize},
+        {c->f[c->cur], (size_t)Q * n * c->fsize}, {c->h[c->cur], (size_t)Q * n * c->gsize},
         {c->phip, n * c->rsize}, {c->q, n * c->rsize}, {c->rho, n * c->rsize},
         {c->u, n * c->rsize}, {c->v, n * c->rsize}, {c->w, n * c->rsize},
         {c->phi00, nz * 8}, {c->ez00, nz * 8},

@@ -193,7 +193,8 @@ int step_graph(ehd_batch *b, const std::vector<char> &act, bool macros, cudaGrap
             case EHD_PREC_FP64: r = capture_groups<double, double>(b, act, macros, bufs, &g); break;
             case EHD_PREC_FP32: r = capture_groups<float, float>(b, act, macros, bufs, &g); break;
             case EHD_PREC_FP16: r = capture_groups<__half, float>(b, act, macros, bufs, &g); break;
-            default: r = capture_groups<__nv_bfloat16, float>(b, act, macros, bufs, &g); break;
+            case EHD_PREC_BF16: r = capture_groups<__nv_bfloat16, float>(b, act, macros, bufs, &g); break;
+            default: r = capture_groups<Mix16, float>(b, act, macros, bufs, &g); break;
         }
         if (r != EHD_OK) {
             for (void *p : bufs) cudaFree(p);

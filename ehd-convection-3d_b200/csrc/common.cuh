@@ -67,14 +67,30 @@ struct StepConst {
 // weight class: 0 rest, 1 axis (2/27), 2 face diagonal (1/54), 3 body diagonal (1/216)
 __host__ __device__ constexpr int cls_of(int d) { return d == 0 ? 0 : (d <= 6 ? 1 : (d <= 18 ? 2 : 3)); }
 
+// Storage tag of the mixed mode: flow populations f as FP16 deviations,
+// charge populations g as FP32 deviations (the charge, the Poisson source,
+// keeps FP32 storage; see PopT).
+struct Mix16 {};
+
+// The storage types of the two population sets for a storage tag T: both T,
+// except for Mix16.
+template <typename T> struct PopT {
+    using F = T;
+    using G = T;
+};
+template <> struct PopT<Mix16> {
+    using F = __half;
+    using G = float;
+};
+
 // Per-direction base pointers of the two population buffers, passed by value
 // so each access is a 32-bit node offset from a kernel-parameter base.
 template <typename T>
 struct PopPtrs {
-    const T *fa[Q];
-    T *fb[Q];
-    const T *ha[Q];
-    T *hb[Q];
+    const typename PopT<T>::F *fa[Q];
+    typename PopT<T>::F *fb[Q];
+    const typename PopT<T>::G *ha[Q];
+    typename PopT<T>::G *hb[Q];
 };
 
 // The step constants in the compute type, with the per-weight-class factors
@@ -139,6 +155,22 @@ template <> struct Store<__nv_bfloat16> {
         *p = __float2bfloat16_rn(v);
     }
 };
+
+// Population loads and stores by pointer type: pld from global memory
+// (read-only path), plds from shared memory, pst to global memory; 16-bit
+// values widen to FP32 and round to nearest even on the way back.
+__device__ __forceinline__ double pld(const double *p) { return __ldg(p); }
+__device__ __forceinline__ float pld(const float *p) { return __ldg(p); }
+__device__ __forceinline__ float pld(const __half *p) { return __half2float(__ldg(p)); }
+__device__ __forceinline__ float pld(const __nv_bfloat16 *p) { return __bfloat162float(__ldg(p)); }
+__device__ __forceinline__ double plds(const double *p) { return *p; }
+__device__ __forceinline__ float plds(const float *p) { return *p; }
+__device__ __forceinline__ float plds(const __half *p) { return __half2float(*p); }
+__device__ __forceinline__ float plds(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
+__device__ __forceinline__ void pst(double *p, double v) { *p = v; }
+__device__ __forceinline__ void pst(float *p, float v) { *p = v; }
+__device__ __forceinline__ void pst(__half *p, float v) { *p = __float2half_rn(v); }
+__device__ __forceinline__ void pst(__nv_bfloat16 *p, float v) { *p = __float2bfloat16_rn(v); }
 
 template <typename R> struct Cplx;
 template <> struct Cplx<float> { using T = float2; };

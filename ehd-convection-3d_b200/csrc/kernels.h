@@ -88,7 +88,7 @@ int lbm_blocks_per_plane(int nx, int ny, int bx);
 // the per-node kernel's default block width for a grid nx wide
 int lbm_default_block_x(int nx);
 // whether the bulk-copy row kernel serves this grid and storage type
-bool lbm_rows_usable(int nx, size_t tsize);
+bool lbm_rows_usable(int nx, size_t fsize, size_t gsize);
 // sets the row kernel's shared-memory attribute (before any stream capture)
 // and returns its persistent grid size in *grid, 0 when it does not apply
 template <typename T, typename R>

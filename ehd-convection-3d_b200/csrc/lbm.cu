@@ -132,23 +132,23 @@ __device__ __forceinline__ void pull_global(R (&f)[Q], R (&h)[Q], const PopPtrs<
                                             const ZRef<R> &zr, const KConst<R> &c, bool local) {
 #pragma unroll
     for (int d = 0; d < Q; ++d) {
-        f[d] = Store<T>::ld(pp.fa[d] + (local ? node : pull_src(P, d))) +
+        f[d] = pld(pp.fa[d] + (local ? node : pull_src(P, d))) +
                c.w[cls_of(d)] * zr.dr(local ? 0 : ez_of(d));
     }
     if (local) {
 #pragma unroll
-        for (int d = 0; d < Q; ++d) h[d] = Store<T>::ld(pp.ha[d] + node) + c.w[cls_of(d)] * zr.dq0;
+        for (int d = 0; d < Q; ++d) h[d] = pld(pp.ha[d] + node) + c.w[cls_of(d)] * zr.dq0;
     } else if (z == 0) {
         // g_d = -g_opp(d) + 2 q0 w_d (LBM.cu:1320-1348), on deviations
-        h[0] = Store<T>::ld(pp.ha[0] + node) + c.w[0] * zr.dq0;
+        h[0] = pld(pp.ha[0] + node) + c.w[0] * zr.dq0;
         const R inj = (R)2 * (c.q0 - zr.qref) - zr.dq0;
 #pragma unroll
         for (int d = 1; d < Q; ++d)
-            h[d] = -Store<T>::ld(pp.ha[opp_of(d)] + node) + inj * c.w[cls_of(d)];
+            h[d] = -pld(pp.ha[opp_of(d)] + node) + inj * c.w[cls_of(d)];
     } else {
 #pragma unroll
         for (int d = 0; d < Q; ++d)
-            h[d] = Store<T>::ld(pp.ha[d] + pull_src(P, d)) + c.w[cls_of(d)] * zr.dq(ez_of(d));
+            h[d] = pld(pp.ha[d] + pull_src(P, d)) + c.w[cls_of(d)] * zr.dq(ez_of(d));
     }
 }
 
@@ -214,10 +214,10 @@ __device__ __forceinline__ void f_pair2(const float (&f)[Q], const PackF &p,
     B = __ffma2_rn(p.rm_hi, Y, B);
     const float2 od = __ffma2_rn(p.mone, __fadd2_rn(A, B), fd);
     const float2 oo = __ffma2_rn(p.mone, A, __fadd2_rn(fo, B));
-    Store<T>::st(pp.fb[D1] + node, od.x);
-    Store<T>::st(pp.fb[D2] + node, od.y);
-    Store<T>::st(pp.fb[D1 + 1] + node, oo.x);
-    Store<T>::st(pp.fb[D2 + 1] + node, oo.y);
+    pst(pp.fb[D1] + node, od.x);
+    pst(pp.fb[D2] + node, od.y);
+    pst(pp.fb[D1 + 1] + node, oo.x);
+    pst(pp.fb[D2 + 1] + node, oo.y);
 }
 
 struct PackG {
@@ -253,16 +253,16 @@ __device__ __forceinline__ void g_pair2(const float (&h)[Q], const PackG &p,
         od = __ffma2_rn(p.mone, __fadd2_rn(A, B), hd);
         oo = __ffma2_rn(p.mone, A, __fadd2_rn(ho, B));
     }
-    Store<T>::st(pp.hb[D1] + node, od.x);
-    Store<T>::st(pp.hb[D2] + node, od.y);
-    Store<T>::st(pp.hb[D1 + 1] + node, oo.x);
-    Store<T>::st(pp.hb[D2 + 1] + node, oo.y);
+    pst(pp.hb[D1] + node, od.x);
+    pst(pp.hb[D2] + node, od.y);
+    pst(pp.hb[D1 + 1] + node, oo.x);
+    pst(pp.hb[D2 + 1] + node, oo.y);
     if (dup) {
         const float2 ud = __fadd2_rn(od, p.wup[K]), uo = __fadd2_rn(oo, p.wup[K]);
-        Store<T>::st(pp.hb[D1] + nodeup, ud.x);
-        Store<T>::st(pp.hb[D2] + nodeup, ud.y);
-        Store<T>::st(pp.hb[D1 + 1] + nodeup, uo.x);
-        Store<T>::st(pp.hb[D2 + 1] + nodeup, uo.y);
+        pst(pp.hb[D1] + nodeup, ud.x);
+        pst(pp.hb[D2] + nodeup, ud.y);
+        pst(pp.hb[D1 + 1] + nodeup, uo.x);
+        pst(pp.hb[D2 + 1] + nodeup, uo.y);
     }
 }
 
@@ -321,14 +321,14 @@ __device__ __forceinline__ void finish_node(R (&f)[Q], R (&h)[Q], const Moments<
         PullIdx P1;
         make_pull(P1, x, y, 1, NX, NY, NZ);
         const unsigned node1 = node + c.nxy;
-        R dqm = Store<T>::ld(a.pp.ha[0] + node1) + c.w[0] * z1.dq0;
+        R dqm = pld(a.pp.ha[0] + node1) + c.w[0] * z1.dq0;
         R mxm = 0, mym = 0, mzm = 0;
 #pragma unroll
         for (int d = 1; d < Q; ++d) {
             const unsigned s1 = local ? node1 : pull_src(P1, d);
             const int e = local ? 0 : ez_of(d);
-            const R fm = Store<T>::ld(a.pp.fa[d] + s1) + c.w[cls_of(d)] * z1.dr(e);
-            const R hm = Store<T>::ld(a.pp.ha[d] + s1) + c.w[cls_of(d)] * z1.dq(e);
+            const R fm = pld(a.pp.fa[d] + s1) + c.w[cls_of(d)] * z1.dr(e);
+            const R hm = pld(a.pp.ha[d] + s1) + c.w[cls_of(d)] * z1.dq(e);
             dqm += hm;
             if (ex_of(d)) mxm += ex_of(d) > 0 ? fm : -fm;
             if (ey_of(d)) mym += ey_of(d) > 0 ? fm : -fm;
@@ -363,12 +363,12 @@ __device__ __forceinline__ void finish_node(R (&f)[Q], R (&h)[Q], const Moments<
 
     // ---- f: collide (interior) or wall rule ----
     if (z == 0 || z == NZ - 1) {
-        Store<T>::st(a.pp.fb[0] + node, f[0]);
+        pst(a.pp.fb[0] + node, f[0]);
 #pragma unroll
         for (int d = 1; d < Q; ++d) {
             R v = f[opp_of(d)];
             if (z == NZ - 1 && mw_sign_of(d) != 0) v += c.mw[d];
-            Store<T>::st(a.pp.fb[d] + node, v);
+            pst(a.pp.fb[d] + node, v);
         }
     } else {
         const R rp_hi = c.rate_hi[0], rp_lo = c.rate_lo[0];
@@ -383,7 +383,7 @@ __device__ __forceinline__ void finish_node(R (&f)[Q], R (&h)[Q], const Moments<
             PK[k] = WR[k] * usq - c.w[k] * drho;
             QK[k] = c.c3[k] * uF;
         }
-        Store<T>::st(a.pp.fb[0] + node, f[0] - relax(rp_hi, rp_lo, f[0] + PK[0]) - QK[0]);
+        pst(a.pp.fb[0] + node, f[0] - relax(rp_hi, rp_lo, f[0] + PK[0]) - QK[0]);
         if constexpr (sizeof(R) == 4) {
             PackF pk;
             pk.rp_hi = f2(rp_hi);
@@ -421,8 +421,8 @@ __device__ __forceinline__ void finish_node(R (&f)[Q], R (&h)[Q], const Moments<
                 const R A = relax(rp_hi, rp_lo, X) + QK[k] - c.c1[k] * cu * eF;
                 const R Y = (R)0.5 * (f[d] - f[o]) - WR[k] * cu;
                 const R B = relax(rm_hi, rm_lo, Y) - c.c2[k] * eF;
-                Store<T>::st(a.pp.fb[d] + node, f[d] - A - B);
-                Store<T>::st(a.pp.fb[o] + node, f[o] - A + B);
+                pst(a.pp.fb[d] + node, f[d] - A - B);
+                pst(a.pp.fb[o] + node, f[o] - A + B);
             }
         } else {
 #pragma unroll
@@ -434,8 +434,8 @@ __device__ __forceinline__ void finish_node(R (&f)[Q], R (&h)[Q], const Moments<
             const R A = relax(rp_hi, rp_lo, X) + QK[k] - c.c1[k] * cu * eF;
             const R Y = (R)0.5 * (f[d] - f[o]) - WR[k] * cu;
             const R B = relax(rm_hi, rm_lo, Y) - c.c2[k] * eF;
-            Store<T>::st(a.pp.fb[d] + node, f[d] - A - B);
-            Store<T>::st(a.pp.fb[o] + node, f[o] - A + B);
+            pst(a.pp.fb[d] + node, f[d] - A - B);
+            pst(a.pp.fb[o] + node, f[o] - A + B);
         }
         }
     }
@@ -459,8 +459,8 @@ __device__ __forceinline__ void finish_node(R (&f)[Q], R (&h)[Q], const Moments<
         }
         {
             const R out = h[0] - relax(cp_hi, cp_lo, h[0] + PQ[0]);
-            Store<T>::st(a.pp.hb[0] + node, z == 0 ? -out + (R)2 * (c.q0 - zr.qref) * c.w[0] : out);
-            if (dup) Store<T>::st(a.pp.hb[0] + nodeup, out + c.w[0] * up);
+            pst(a.pp.hb[0] + node, z == 0 ? -out + (R)2 * (c.q0 - zr.qref) * c.w[0] : out);
+            if (dup) pst(a.pp.hb[0] + nodeup, out + c.w[0] * up);
         }
         auto g_one = [&](auto dc) {
             constexpr int d = decltype(dc)::value, o = d + 1, k = cls_of(d);
@@ -478,11 +478,11 @@ __device__ __forceinline__ void finish_node(R (&f)[Q], R (&h)[Q], const Moments<
                 outd = h[d] - A - B;
                 outo = h[o] - A + B;
             }
-            Store<T>::st(a.pp.hb[d] + node, outd);
-            Store<T>::st(a.pp.hb[o] + node, outo);
+            pst(a.pp.hb[d] + node, outd);
+            pst(a.pp.hb[o] + node, outo);
             if (dup) {
-                Store<T>::st(a.pp.hb[d] + nodeup, outd + c.w[k] * up);
-                Store<T>::st(a.pp.hb[o] + nodeup, outo + c.w[k] * up);
+                pst(a.pp.hb[d] + nodeup, outd + c.w[k] * up);
+                pst(a.pp.hb[o] + nodeup, outo + c.w[k] * up);
             }
         };
         if constexpr (sizeof(R) == 4) {
@@ -531,11 +531,11 @@ __device__ __forceinline__ void finish_node(R (&f)[Q], R (&h)[Q], const Moments<
                     outd = h[d] - A - B;
                     outo = h[o] - A + B;
                 }
-                Store<T>::st(a.pp.hb[d] + node, outd);
-                Store<T>::st(a.pp.hb[o] + node, outo);
+                pst(a.pp.hb[d] + node, outd);
+                pst(a.pp.hb[o] + node, outo);
                 if (dup) {
-                    Store<T>::st(a.pp.hb[d] + nodeup, outd + c.w[k] * up);
-                    Store<T>::st(a.pp.hb[o] + nodeup, outo + c.w[k] * up);
+                    pst(a.pp.hb[d] + nodeup, outd + c.w[k] * up);
+                    pst(a.pp.hb[o] + nodeup, outo + c.w[k] * up);
                 }
             }
         }
@@ -667,9 +667,15 @@ lbm_rows_kernel(const StepArgs<T, R> a, const KConst<R> c) {
     __shared__ unsigned long long bar[2];
     __shared__ unsigned cnt[2];
     const int NX = c.nx, NY = c.ny, NZ = c.nz;
-    const size_t stage_elems = (size_t)2 * Q * NX;
-    T *const smem = reinterpret_cast<T *>(smem_raw);  // stage s at smem + s * stage_elems
-    const unsigned row_bytes = (unsigned)(NX * sizeof(T));
+    using F = typename PopT<T>::F;
+    using G = typename PopT<T>::G;
+    // stage s: the 27 f rows, then the 27 g rows
+    const size_t stage_bytes = (size_t)Q * NX * (sizeof(F) + sizeof(G));
+    auto stage_f = [&](int st) { return reinterpret_cast<F *>(smem_raw + (size_t)st * stage_bytes); };
+    auto stage_g = [&](int st) {
+        return reinterpret_cast<G *>(smem_raw + (size_t)st * stage_bytes + (size_t)Q * NX * sizeof(F));
+    };
+    const unsigned row_bytes_f = (unsigned)(NX * sizeof(F)), row_bytes_g = (unsigned)(NX * sizeof(G));
     const int x = threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned nw = (unsigned)(NX / 32);
@@ -686,7 +692,7 @@ lbm_rows_kernel(const StepArgs<T, R> a, const KConst<R> c) {
     // the calling warp issues the 54 row copies of row (yy, zz) into stage s;
     // lane d < 27 copies direction d
     auto issue = [&](int yy, int zz, int s) {
-        if (lane == 0) mbar_expect_tx(&bar[s], 2u * Q * row_bytes);
+        if (lane == 0) mbar_expect_tx(&bar[s], (unsigned)Q * (row_bytes_f + row_bytes_g));
         __syncwarp();
         if (lane < Q) {
             int ys = yy - ey_rt(lane), zs = zz - ez_rt(lane);
@@ -694,9 +700,8 @@ lbm_rows_kernel(const StepArgs<T, R> a, const KConst<R> c) {
             zs += zs < 0 ? NZ : (zs >= NZ ? -NZ : 0);
             // direction d's array starts d * NX * NY * NZ after direction 0's
             const size_t off = (size_t)lane * NX * NY * NZ + (size_t)NX * ((size_t)ys + (size_t)NY * zs);
-            T *dst = smem + (size_t)s * stage_elems + (size_t)lane * NX;
-            bulk_g2s(dst, a.pp.fa[0] + off, row_bytes, &bar[s]);
-            bulk_g2s(dst + (size_t)Q * NX, a.pp.ha[0] + off, row_bytes, &bar[s]);
+            bulk_g2s(stage_f(s) + (size_t)lane * NX, a.pp.fa[0] + off, row_bytes_f, &bar[s]);
+            bulk_g2s(stage_g(s) + (size_t)lane * NX, a.pp.ha[0] + off, row_bytes_g, &bar[s]);
         }
     };
     // bounded wait of the calling thread for the phase `parity` of bar[s]
@@ -750,13 +755,13 @@ lbm_rows_kernel(const StepArgs<T, R> a, const KConst<R> c) {
         }
         phases ^= 1u << s;
         {
-            const T *sf = smem + (size_t)s * stage_elems;
-            const T *sh = sf + (size_t)Q * NX;
+            const F *sf = stage_f(s);
+            const G *sh = stage_g(s);
 #pragma unroll
             for (int d = 0; d < Q; ++d) {
                 const int xs = P.xs[ex_of(d) + 1];
-                f[d] = Store<T>::lds(sf + (size_t)d * NX + xs) + c.w[cls_of(d)] * zr.dr(ez_of(d));
-                h[d] = Store<T>::lds(sh + (size_t)d * NX + xs) + c.w[cls_of(d)] * zr.dq(ez_of(d));
+                f[d] = plds(sf + (size_t)d * NX + xs) + c.w[cls_of(d)] * zr.dr(ez_of(d));
+                h[d] = plds(sh + (size_t)d * NX + xs) + c.w[cls_of(d)] * zr.dq(ez_of(d));
             }
         }
         const Moments<R> mo = moments(f, h, zr);
@@ -788,7 +793,8 @@ lbm_rows_kernel(const StepArgs<T, R> a, const KConst<R> c) {
 // LBM.cu:110-276), computed in FP64 and stored as deviations from the plane's
 // reference state.
 template <typename T>
-__global__ void init_equilibrium_kernel(T *__restrict__ f, T *__restrict__ h,
+__global__ void init_equilibrium_kernel(typename PopT<T>::F *__restrict__ f,
+                                        typename PopT<T>::G *__restrict__ h,
                                         const double *__restrict__ r,
                                         const double *__restrict__ u,
                                         const double *__restrict__ v,
@@ -815,8 +821,8 @@ __global__ void init_equilibrium_kernel(T *__restrict__ f, T *__restrict__ h,
         const double cc = ex_of(d) * tcx + ey_of(d) * tcy + ez_of(d) * tcz;
         const double fe = w_of(d) * rho * (omusq + cu * (1.0 + 0.5 * cu));
         const double he = w_of(d) * ch * (omusq_c + cc * (1.0 + 0.5 * cc));
-        Store<T>::st(f + d * c.n + i, (decltype(Store<T>::ld(f)))(fe - w_of(d) * rref));
-        Store<T>::st(h + d * c.n + i, (decltype(Store<T>::ld(h)))(he - w_of(d) * qref));
+        pst(f + d * c.n + i, (decltype(pld(f)))(fe - w_of(d) * rref));
+        pst(h + d * c.n + i, (decltype(pld(h)))(he - w_of(d) * qref));
     }
 }
 
@@ -893,20 +899,26 @@ __global__ void fields_to_compute_kernel(const double *const *out, R *rho, R *u,
 
 // ---- launchers ---------------------------------------------------------------
 
-size_t lbm_rows_smem(int nx, size_t tsize) { return (size_t)2 * 2 * Q * nx * tsize; }
+size_t lbm_rows_smem(int nx, size_t fsize, size_t gsize) {
+    return (size_t)2 * Q * nx * (fsize + gsize);
+}
 
-// FP32 and FP64 storage only: with 2-byte populations the per-node kernel
-// measured faster (0.73 vs 0.76 ms at 256 x 256 x 129, FP16)
-bool lbm_rows_usable(int nx, size_t tsize) {
-    return tsize >= 4 && nx >= 32 && nx <= 256 && nx % 32 == 0 && (nx * tsize) % 16 == 0 &&
-           lbm_rows_smem(nx, tsize) <= 220 * 1024;
+// FP32 and FP64 charge populations only: with both sets in 2 bytes the
+// per-node kernel measured faster (0.73 vs 0.76 ms at 256 x 256 x 129, FP16);
+// the mixed storage (2-byte f, 4-byte g) runs on it.  Rows are whole bulk
+// copies, so their bytes are multiples of 16.
+bool lbm_rows_usable(int nx, size_t fsize, size_t gsize) {
+    return gsize >= 4 && nx >= 32 && nx <= 256 && nx % 32 == 0 && (nx * fsize) % 16 == 0 &&
+           (nx * gsize) % 16 == 0 && lbm_rows_smem(nx, fsize, gsize) <= 220 * 1024;
 }
 
 template <typename T, typename R>
 cudaError_t prepare_lbm_rows(int nx, int ny, int nz, int *grid) {
     *grid = 0;
-    if (!lbm_rows_usable(nx, sizeof(T))) return cudaSuccess;
-    const int sm = (int)lbm_rows_smem(nx, sizeof(T));
+    using F = typename PopT<T>::F;
+    using G = typename PopT<T>::G;
+    if (!lbm_rows_usable(nx, sizeof(F), sizeof(G))) return cudaSuccess;
+    const int sm = (int)lbm_rows_smem(nx, sizeof(F), sizeof(G));
     cudaError_t e;
     if ((e = allow_max_dynamic_smem(lbm_rows_kernel<T, R, true>)) != cudaSuccess ||
         (e = allow_max_dynamic_smem(lbm_rows_kernel<T, R, false>)) != cudaSuccess)
@@ -928,15 +940,16 @@ template cudaError_t prepare_lbm_rows<double, double>(int, int, int, int *);
 template cudaError_t prepare_lbm_rows<float, float>(int, int, int, int *);
 template cudaError_t prepare_lbm_rows<__half, float>(int, int, int, int *);
 template cudaError_t prepare_lbm_rows<__nv_bfloat16, float>(int, int, int, int *);
+template cudaError_t prepare_lbm_rows<Mix16, float>(int, int, int, int *);
 
 template <typename T, typename R>
 static StepArgs<T, R> make_step_args(const LbmArgs &la, const StepConst &c) {
     StepArgs<T, R> a;
     for (int d = 0; d < Q; ++d) {
-        a.pp.fa[d] = (const T *)la.fa + (size_t)d * c.n;
-        a.pp.ha[d] = (const T *)la.ha + (size_t)d * c.n;
-        a.pp.fb[d] = (T *)la.fb + (size_t)d * c.n;
-        a.pp.hb[d] = (T *)la.hb + (size_t)d * c.n;
+        a.pp.fa[d] = (const typename PopT<T>::F *)la.fa + (size_t)d * c.n;
+        a.pp.ha[d] = (const typename PopT<T>::G *)la.ha + (size_t)d * c.n;
+        a.pp.fb[d] = (typename PopT<T>::F *)la.fb + (size_t)d * c.n;
+        a.pp.hb[d] = (typename PopT<T>::G *)la.hb + (size_t)d * c.n;
     }
     a.phip = (const R *)la.phip;
     a.ez00 = la.ez00;
@@ -1025,7 +1038,7 @@ cudaError_t launch_lbm_step(const LbmArgs &la, const StepConst &c, int local_pop
         const dim3 g0(c.nx / bx, c.ny, 1);
         if (macros) lbm_step_kernel<T, R, false, true><<<g0, bx, 0, s>>>(a, k, 0, 0);
         else lbm_step_kernel<T, R, false, false><<<g0, bx, 0, s>>>(a, k, 0, 0);
-        const size_t sm = lbm_rows_smem(c.nx, sizeof(T));
+        const size_t sm = lbm_rows_smem(c.nx, sizeof(typename PopT<T>::F), sizeof(typename PopT<T>::G));
         if (macros) lbm_rows_kernel<T, R, true><<<la.rows_grid, c.nx, sm, s>>>(a, k);
         else lbm_rows_kernel<T, R, false><<<la.rows_grid, c.nx, sm, s>>>(a, k);
         return cudaGetLastError();
@@ -1051,7 +1064,7 @@ cudaError_t launch_init_equilibrium(void *f, void *h, const double *const fields
     const int bs = 128;
     const long long nb = (c.n + bs - 1) / bs;
     init_equilibrium_kernel<T><<<(unsigned)nb, bs, 0, s>>>(
-        (T *)f, (T *)h, fields[0], fields[1], fields[2], fields[3], fields[4], fields[6],
+        (typename PopT<T>::F *)f, (typename PopT<T>::G *)h, fields[0], fields[1], fields[2], fields[3], fields[4], fields[6],
         fields[7], fields[8], ref, c);
     return cudaGetLastError();
 }
@@ -1079,6 +1092,7 @@ EHD_INST_LBM(double, double)
 EHD_INST_LBM(float, float)
 EHD_INST_LBM(__half, float)
 EHD_INST_LBM(__nv_bfloat16, float)
+EHD_INST_LBM(Mix16, float)
 template cudaError_t launch_init_equilibrium<double>(void *, void *, const double *const[9],
                                                     const double *, const StepConst &, cudaStream_t);
 template cudaError_t launch_init_equilibrium<float>(void *, void *, const double *const[9],
@@ -1089,6 +1103,8 @@ template cudaError_t launch_init_equilibrium<__nv_bfloat16>(void *, void *,
                                                            const double *const[9],
                                                            const double *, const StepConst &,
                                                            cudaStream_t);
+template cudaError_t launch_init_equilibrium<Mix16>(void *, void *, const double *const[9],
+                                                   const double *, const StepConst &, cudaStream_t);
 template cudaError_t launch_materialize<double>(const void *, const void *, const void *,
                                                const void *, const void *, const void *,
                                                const double *, double *const[9], int,
@@ -1349,7 +1365,8 @@ __device__ __forceinline__ void eq_pair(int d, double rho, double ux, double uy,
 // reference ref.  out[1..3] hold du on entry and u0 + du on exit.  The
 // potential's non-mean part phi' is the column's, phi - phi00 per plane.
 template <typename T, typename R>
-__global__ void column_state_kernel(T *__restrict__ f, T *__restrict__ h, double *const *out,
+__global__ void column_state_kernel(typename PopT<T>::F *__restrict__ f,
+                                    typename PopT<T>::G *__restrict__ h, double *const *out,
                                     const double *__restrict__ prof,
                                     const double *__restrict__ colv,
                                     const double *__restrict__ ref, R *__restrict__ phip,
@@ -1374,8 +1391,8 @@ __global__ void column_state_kernel(T *__restrict__ f, T *__restrict__ h, double
         eq_pair(d, rho, u1, v1, w1, ch, u1 + kex, v1 + key, w1 + kez, c, fe1, he1);
         const double fv = colv[(size_t)d * nz + z] + (fe1 - fe0);
         const double hv = colv[(size_t)(Q + d) * nz + z] + (he1 - he0);
-        Store<T>::st(f + d * c.n + i, (decltype(Store<T>::ld(f)))(fv - w_of(d) * rref));
-        Store<T>::st(h + d * c.n + i, (decltype(Store<T>::ld(h)))(hv - w_of(d) * qref));
+        pst(f + d * c.n + i, (decltype(pld(f)))(fv - w_of(d) * rref));
+        pst(h + d * c.n + i, (decltype(pld(h)))(hv - w_of(d) * qref));
     }
 }
 
@@ -1385,7 +1402,8 @@ cudaError_t launch_column_state(void *f, void *h, double *const *out_dev, const 
                                 const double *phi00, const StepConst &c, cudaStream_t s) {
     const int bs = 128;
     column_state_kernel<T, R><<<(unsigned)((c.n + bs - 1) / bs), bs, 0, s>>>(
-        (T *)f, (T *)h, out_dev, prof_dev, colv_dev, ref, (R *)phip, phi00, c);
+        (typename PopT<T>::F *)f, (typename PopT<T>::G *)h, out_dev, prof_dev, colv_dev, ref,
+        (R *)phip, phi00, c);
     return cudaGetLastError();
 }
 #define EHD_INST_COLUMN(T, R)                                                                  \
@@ -1397,6 +1415,7 @@ EHD_INST_COLUMN(double, double)
 EHD_INST_COLUMN(float, float)
 EHD_INST_COLUMN(__half, float)
 EHD_INST_COLUMN(__nv_bfloat16, float)
+EHD_INST_COLUMN(Mix16, float)
 
 cudaError_t launch_seeded_state(double *const *out_dev, const double *prof_dev,
                                 unsigned long long seed, double amp, const StepConst &c,

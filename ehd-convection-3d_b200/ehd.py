@@ -18,7 +18,7 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libehd.so"
 
 FIELDS = ("rho", "u", "v", "w", "q", "phi", "ex", "ey", "ez")
-PRECISIONS = {"fp64": 0, "fp32": 1, "fp16": 2, "bf16": 3}
+PRECISIONS = {"fp64": 0, "fp32": 1, "fp16": 2, "bf16": 3, "mixed": 4}
 FLAG_NO_GRAPH = 0x1
 FLAG_NODE_KERNEL = 0x2
 

@@ -121,8 +121,8 @@ def main(argv=None):
     ap.add_argument("--lambda-f", type=float, default=0.25)
     ap.add_argument("--lambda-g", type=float, default=0.25)
     ap.add_argument("--steps", type=int, nargs="+", default=(100, 1000, 5000))
-    ap.add_argument("--precisions", nargs="+", default=("fp32", "fp16", "bf16"),
-                    choices=("fp32", "fp16", "bf16"))
+    ap.add_argument("--precisions", nargs="+", default=("fp32", "mixed", "fp16", "bf16"),
+                    choices=("fp32", "mixed", "fp16", "bf16"))
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--amp", type=float, default=1e-3)
     ap.add_argument("--transits", type=float, default=16.0)

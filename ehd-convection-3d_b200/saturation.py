@@ -121,7 +121,7 @@ def run(ehd, p, precision="fp32", sample_every=1000, tol=1e-3, hold=3, guard=0.0
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32", "fp16", "bf16"])
+    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32", "mixed", "fp16", "bf16"])
     ap.add_argument("--sample-every", type=int, default=1000)
     ap.add_argument("--tol", type=float, default=1e-3)
     ap.add_argument("--hold", type=int, default=3)

@@ -198,7 +198,7 @@ def main(argv=None, runner=run_share):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--instances", type=int, default=64)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--precision", default="fp16", choices=["fp64", "fp32", "fp16", "bf16"])
+    ap.add_argument("--precision", default="fp16", choices=["fp64", "fp32", "mixed", "fp16", "bf16"])
     ap.add_argument("--sample-every", type=int, default=1000)
     ap.add_argument("--tol", type=float, default=1e-3)
     ap.add_argument("--hold", type=int, default=3)

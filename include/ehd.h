@@ -62,7 +62,10 @@ typedef enum ehd_precision {
     EHD_PREC_FP64 = 0,       /* FP64 compute, FP64 populations                 */
     EHD_PREC_FP32 = 1,       /* FP32 compute, FP32 populations                 */
     EHD_PREC_FP16 = 2,       /* FP32 compute, FP16 population deviations       */
-    EHD_PREC_BF16 = 3        /* FP32 compute, BF16 population deviations       */
+    EHD_PREC_BF16 = 3,       /* FP32 compute, BF16 population deviations       */
+    EHD_PREC_MIXED = 4       /* FP32 compute, FP16 deviations of the flow
+                                populations f, FP32 deviations of the charge
+                                populations g (no reference counterpart)     */
 } ehd_precision;
 
 typedef struct ehd_config {

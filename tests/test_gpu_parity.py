@@ -100,6 +100,23 @@ def test_config0_matches_reference(prec):
             assert sim.current() == pytest.approx(float(g[f"current{n}"]), rel=tol)
 
 
+def test_config0_mixed_storage_matches_reference():
+    """Mixed storage (FP16 deviations of the flow populations, FP32 of the
+    charge populations) on config 0 against the reference's own build after
+    1000 steps.  The charge keeps FP32 storage, so q and phi stay near FP32
+    accuracy; the velocity carries the FP16 rounding of f.  Tolerances: q 5e-4,
+    phi 1e-5, E 1e-4, velocity 5e-3 (per component of the vector)."""
+    M, p, g, f = config0_inputs()
+    with ehd.Simulation(to_ehd(p), "mixed") as sim:
+        sim.set_fields(f)
+        sim.step(1000)
+        mine = O.data_end_view(sim.get_fields())
+    ref = {k: g[f"out1000_{k}"] for k in O.FIELDS}
+    err = config0_errors(mine, ref, p.rho0)
+    for k, tol in (("q", 5e-4), ("phi", 1e-5), ("E", 1e-4), ("velocity", 5e-3), ("rho", 1e-6)):
+        assert err[k] < tol, (k, err)
+
+
 def random_fields(p, seed):
     import make_golden as M
     return M.random_fields(p, seed)

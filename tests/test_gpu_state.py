@@ -52,7 +52,7 @@ def test_seeded_state_matches_oracle_generator(seed):
         assert np.array_equal(got[k], ref[k]), k
 
 
-@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+@pytest.mark.parametrize("prec", ["fp32", "fp16", "mixed"])
 def test_checkpoint_resume_is_bitexact(prec, tmp_path):
     M, p, g = config0()
     prof = {k: g[f"prof_{k}"] for k in O.FIELDS}
