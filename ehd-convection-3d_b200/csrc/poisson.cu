@@ -207,7 +207,8 @@ __device__ typename Cplx<R>::T *fft_smem(typename Cplx<R>::T *a, typename Cplx<R
 // ---------------------------------------------------------------------------
 
 // K1: s' = -(q - q_m)/eps on the planes z = 1..NZ-2 (odd_extension's interior
-// rows, poisson.cu:96-106), FFT along x, half spectrum out; FP64 row sums.
+// rows, poisson.cu:96-106), FFT along x of two real rows per complex
+// transform, half spectrum out; FP64 row sums.
 template <typename R>
 __global__ void __launch_bounds__(256)
 poisson_rows_fwd(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec,
@@ -228,20 +229,21 @@ poisson_rows_fwd(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec
     R2 *b = a + (size_t)rows * nx;
     R2 *tws = b + (size_t)rows * nx;
     const int zi = blockIdx.y;  // plane z = zi + 1
-    const int y0 = blockIdx.x * rows;
+    const int y0 = blockIdx.x * 2 * rows;  // transform r holds rows y0 + 2r, + 1
     const int tid = threadIdx.x;
     for (int i = tid; i < nx; i += blockDim.x) tws[i] = tw[i];
     const R *qp = q + (size_t)nx * ny * (zi + 1);
     const R qm = (R)qmean[2 * (zi + 1) + 1];
     for (int t = tid; t < rows * nx; t += blockDim.x) {
         const int r = t / nx, x = t - r * nx;
-        const int y = y0 + r;
-        R val = 0;
-        if (y < ny) val = -(qp[(size_t)nx * y + x] - qm) / (R)eps;
-        a[t] = R2{val, (R)0};
+        const int ya = y0 + 2 * r, yb = ya + 1;
+        R va = 0, vb = 0;
+        if (ya < ny) va = -(qp[(size_t)nx * ya + x] - qm) / (R)eps;
+        if (yb < ny) vb = -(qp[(size_t)nx * yb + x] - qm) / (R)eps;
+        a[t] = R2{va, vb};
     }
     const int warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
-    for (int r = warp; r < rows; r += nwarps) {
+    for (int r = warp; r < 2 * rows; r += nwarps) {
         const int y = y0 + r;
         if (y >= ny) continue;
         double sum = 0.0;
@@ -252,11 +254,16 @@ poisson_rows_fwd(const R *__restrict__ q, typename Cplx<R>::T *__restrict__ spec
     }
     __syncthreads();
     R2 *res = fft_smem<R>(a, b, pl, tws, (R)-1, rows);
+    // two real rows per transform: A[k] = (Z[k] + conj Z[N-k]) / 2,
+    // B[k] = (Z[k] - conj Z[N-k]) / (2i)
     R2 *sp = spec + (size_t)zi * ny * pitch;
     for (int t = tid; t < rows * nxh; t += blockDim.x) {
         const int r = t / nxh, k = t - r * nxh;
-        const int y = y0 + r;
-        if (y < ny) sp[(size_t)pitch * y + k] = res[(size_t)r * nx + k];
+        const int ya = y0 + 2 * r, yb = ya + 1;
+        const R2 zk = res[(size_t)r * nx + k];
+        const R2 zn = res[(size_t)r * nx + (k == 0 ? 0 : nx - k)];
+        if (ya < ny) sp[(size_t)pitch * ya + k] = R2{(R)0.5 * (zk.x + zn.x), (R)0.5 * (zk.y - zn.y)};
+        if (yb < ny) sp[(size_t)pitch * yb + k] = R2{(R)0.5 * (zk.y + zn.y), (R)0.5 * (zn.x - zk.x)};
     }
 }
 
@@ -331,23 +338,28 @@ poisson_rows_inv(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ p
     R2 *b = a + (size_t)rows * nx;
     R2 *tws = b + (size_t)rows * nx;
     const int zi = blockIdx.y;
-    const int y0 = blockIdx.x * rows;
+    const int y0 = blockIdx.x * 2 * rows;  // transform r holds rows y0 + 2r, + 1
     const int tid = threadIdx.x;
     for (int i = tid; i < nx; i += blockDim.x) tws[i] = tw[i];
     const R2 *sp = spec + (size_t)zi * ny * pitch;
+    // Z = A + i B over the full length, A and B the Hermitian-completed rows;
+    // the imaginary parts of the bins 0 and N/2, which a real row ignores,
+    // are dropped so that they do not leak into the other row
     for (int t = tid; t < rows * nx; t += blockDim.x) {
         const int r = t / nx, k = t - r * nx;
-        const int y = y0 + r;
-        R2 v = R2{(R)0, (R)0};
-        if (y < ny) {
-            if (k < nxh) {
-                v = sp[(size_t)pitch * y + k];
-            } else {
-                v = sp[(size_t)pitch * y + (nx - k)];
-                v.y = -v.y;
-            }
+        const int ya = y0 + 2 * r, yb = ya + 1;
+        const int kk = k < nxh ? k : nx - k;
+        R2 A = ya < ny ? sp[(size_t)pitch * ya + kk] : R2{(R)0, (R)0};
+        R2 B = yb < ny ? sp[(size_t)pitch * yb + kk] : R2{(R)0, (R)0};
+        if (kk == 0 || 2 * kk == nx) {
+            A.y = 0;
+            B.y = 0;
         }
-        a[t] = v;
+        if (k >= nxh) {
+            A.y = -A.y;
+            B.y = -B.y;
+        }
+        a[t] = R2{A.x - B.y, A.y + B.x};
     }
     __syncthreads();
     R2 *res = fft_smem<R>(a, b, pl, tws, (R)1, rows);
@@ -355,8 +367,9 @@ poisson_rows_inv(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ p
     R *pp = phip + (size_t)nx * ny * (zi + 1);
     for (int t = tid; t < rows * nx; t += blockDim.x) {
         const int r = t / nx, x = t - r * nx;
-        const int y = y0 + r;
-        if (y < ny) pp[(size_t)nx * y + x] = res[t].x * norm;
+        const int ya = y0 + 2 * r, yb = ya + 1;
+        if (ya < ny) pp[(size_t)nx * ya + x] = res[t].x * norm;
+        if (yb < ny) pp[(size_t)nx * yb + x] = res[t].y * norm;
     }
 }
 
@@ -1429,7 +1442,7 @@ static cudaError_t rows_fwd(const PoissonArgs &a, cudaStream_t s) {
     const size_t sm = (size_t)(2 * rows + 1) * a.nx * sizeof(R2);
     cudaError_t e = set_smem(poisson_rows_fwd<R>, sm, s);
     if (e != cudaSuccess) return e;
-    dim3 grid((a.ny + rows - 1) / rows, a.nz - 2, a.ngrp);
+    dim3 grid((a.ny + 2 * rows - 1) / (2 * rows), a.nz - 2, a.ngrp);
     poisson_rows_fwd<R><<<grid, 256, sm, s>>>((const R *)a.q, (R2 *)a.spec, a.rowsum,
                                                (const R2 *)a.twx, a.qmean, a.px,
                                                a.nx, a.ny, a.nxh, a.pitch, rows, a.eps, a.grp);
@@ -1449,7 +1462,7 @@ static cudaError_t rows_inv(const PoissonArgs &a, cudaStream_t s) {
     const size_t sm = (size_t)(2 * rows + 1) * a.nx * sizeof(R2);
     cudaError_t e = set_smem(poisson_rows_inv<R>, sm, s);
     if (e != cudaSuccess) return e;
-    dim3 grid((a.ny + rows - 1) / rows, a.nz - 2, a.ngrp);
+    dim3 grid((a.ny + 2 * rows - 1) / (2 * rows), a.nz - 2, a.ngrp);
     poisson_rows_inv<R><<<grid, 256, sm, s>>>((const R2 *)a.spec, (R *)a.phip,
                                                (const R2 *)a.twx, a.px, a.nx, a.ny, a.nxh,
                                                a.pitch, rows, a.grp);

@@ -130,7 +130,9 @@ def predict(ehd, net, mean, std, group: dict, coarse_grid, transits=4.0, device=
     for cb in cbs:
         cb.close()
     x = torch.tensor(W.channels(f0, p, group)[None], device=torch.device("cuda", device))
-    u = net.forward(x).cpu().numpy()[0].astype(np.float64) * std + mean
+    # the network predicts the change over the horizon (warmstart.py)
+    u = (W.channels(f0, p, group)[..., :W.COUT].astype(np.float64) +
+         net.forward(x).cpu().numpy()[0].astype(np.float64) * std + mean)
     pred = {"u": u[..., 0], "v": u[..., 1], "w": u[..., 2], "q": u[..., 3] * p.charge0,
             "phi": u[..., 4] * p.voltage}
     return p, pred
@@ -274,15 +276,16 @@ def main(argv=None):
     else:
         groups = W.sample_groups(a.train, seed=1)
         xtr, ytr, itr = W.trajectories(ehd, groups, a.horizon, grid=coarse)
-        mean = ytr.reshape(-1, W.COUT).mean(0)
-        std = ytr.reshape(-1, W.COUT).std(0) + 1e-12
+        dtr = ytr - xtr[..., :W.COUT]  # the change over the horizon, as warmstart.py
+        mean = dtr.reshape(-1, W.COUT).mean(0)
+        std = dtr.reshape(-1, W.COUT).std(0) + 1e-12
         dev = torch.device("cuda", 0)
         nz, ny, nx = xtr.shape[1:4]
         net = fno.FNO(nx, ny, nz, W.CIN, W.COUT, width=a.width, layers=a.layers,
                       modes=(a.modes, a.modes, min(a.modes, nz // 2)), hidden=a.hidden,
                       max_batch=a.batch, seed=7)
         hist = W.train(net, torch.tensor(xtr, device=dev),
-                       torch.tensor((ytr - mean) / std, device=dev, dtype=torch.float32),
+                       torch.tensor((dtr - mean) / std, device=dev, dtype=torch.float32),
                        a.epochs, a.lr, a.batch, log=log)
         res.update(train=len(itr), loss_first=hist[0], loss_last=hist[-1])
         if a.save:

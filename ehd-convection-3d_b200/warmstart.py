@@ -7,16 +7,18 @@ Pipeline, all on one GPU:
   1. trajectories: instances with T, M, C drawn uniformly, each from its
      hydrostatic column's state plus seeded noise, run `horizon` steps as batches
      (one graph launch per step for a whole batch);
-  2. training: Adam on the mean-square error of standardised fields;
+  2. training: Adam on the mean-square error of the standardised change of
+     the fields over the horizon (the prediction is the initial state plus
+     the predicted change);
   3. evaluation on held-out instances: the prediction against the plain
      run's state at the horizon, beside the same error of the initial state
      (what the plain method has without the network), and the Nu_e of a
      short run from the warm start against the plain run's.
 
 Input channels per node: u, v, w, q / q0, phi / V, then T / 400, M / 20,
-C / 20 and z / Lz as constant or coordinate channels.  Output channels: u, v,
-w, q / q0, phi / V at the horizon, standardised per channel with the training
-set's mean and spread.
+C / 20 and z / Lz as constant or coordinate channels.  Output channels: the
+change of u, v, w, q / q0, phi / V over the horizon, standardised per channel
+with the training set's mean and spread.
 
     python ehd-convection-3d_b200/warmstart.py --train 448 --test 64 --horizon 40000
 """
@@ -167,11 +169,16 @@ def main(argv=None):
     xte, yte, ite = trajectories(ehd, gte, a.horizon, extra=a.relax, grid=grid)
     t_data = time.perf_counter() - t0
     log(f"trajectories: {len(itr)} train, {len(ite)} test, {t_data:.1f} s")
-    mean = ytr.reshape(-1, COUT).mean(0)
-    std = ytr.reshape(-1, COUT).std(0) + 1e-12
+    # the network learns the change over the horizon (target minus the
+    # initial state of the same channels), standardised per channel; the
+    # prediction is the initial state plus that change, so a channel that
+    # hardly moves is carried over instead of being re-predicted
+    dtr = ytr - xtr[..., :COUT]
+    mean = dtr.reshape(-1, COUT).mean(0)
+    std = dtr.reshape(-1, COUT).std(0) + 1e-12
     dev = torch.device("cuda", 0)
     Xtr = torch.tensor(xtr, device=dev)
-    Ytr = torch.tensor((ytr - mean) / std, device=dev, dtype=torch.float32)
+    Ytr = torch.tensor((dtr - mean) / std, device=dev, dtype=torch.float32)
     nz, ny, nx = xtr.shape[1:4]
     net = fno.FNO(nx, ny, nz, CIN, COUT, width=a.width, layers=a.layers,
                   modes=(a.modes, a.modes, min(a.modes, nz // 2)),
@@ -186,7 +193,8 @@ def main(argv=None):
     base_c = [[] for _ in range(COUT)]
     preds = []
     for k in range(len(ite)):
-        u = net.forward(torch.tensor(xte[k:k + 1], device=dev)).cpu().numpy()[0] * std + mean
+        u = (xte[k][..., :COUT] +
+             net.forward(torch.tensor(xte[k:k + 1], device=dev)).cpu().numpy()[0] * std + mean)
         preds.append(u)
         errs.append(rel_l2(u, yte[k]))
         base.append(rel_l2(xte[k][..., :COUT], yte[k]))

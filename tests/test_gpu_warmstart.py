@@ -1,6 +1,15 @@
 """The learned warm start end to end on a small grid (warmstart.py): LBM
 trajectories, FNO training on the GPU, and the held-out prediction of the
-state after the horizon against the plain run's."""
+state after the horizon against the plain run's.
+
+The case is chosen so that the fields move over the horizon: T in [600, 1000]
+on 16 x 16 x 17 nodes, 4000 steps, from each instance's hydrostatic column
+plus its own seeded noise.  Over that horizon the seeded velocity noise
+relaxes by a factor of several in u and v while q and phi change little; the
+initial state is the plain method's estimate of the state at the horizon
+without the network, so the gain is the initial state's relative L2 error
+against the plain run's state over the prediction's.
+"""
 import importlib.util
 import math
 
@@ -11,20 +20,21 @@ from conftest import ROOT
 pytestmark = pytest.mark.gpu
 
 
-def test_warm_start_pipeline_trains_and_predicts_the_horizon_state():
+def test_warm_start_prediction_beats_the_initial_state():
     spec = importlib.util.spec_from_file_location(
         "ehd_warmstart", ROOT / "ehd-convection-3d_b200" / "warmstart.py")
     W = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(W)
-    res = W.main(["--train", "24", "--test", "4", "--horizon", "3000", "--epochs", "20",
-                  "--relax", "200", "--grid", "16", "16", "9", "--width", "8", "--modes", "4",
-                  "--layers", "2", "--hidden", "16", "--lr", "3e-3"])
-    assert res["train"] == 24 and res["test"] == 4
-    # the network fits its trajectories and predicts the held-out states at
-    # the horizon to a tenth; from the column's own hydrostatic state the
-    # fields move little over 3000 steps on this grid, so the initial state is
-    # closer still (the gains are reported, not asserted)
-    assert res["loss_last"] < 0.5 * res["loss_first"], res
-    assert res["pred_rel_l2_mean"] < 0.2, res
-    assert math.isfinite(res["gain"]) and math.isfinite(res["gain_velocity"])
+    res = W.main(["--train", "64", "--test", "8", "--horizon", "4000", "--epochs", "60",
+                  "--relax", "200", "--grid", "16", "16", "17", "--width", "8", "--modes", "4",
+                  "--layers", "2", "--hidden", "16", "--lr", "3e-3", "--t-range", "600", "1000"])
+    assert res["train"] == 64 and res["test"] == 8
+    assert res["loss_last"] < 0.7 * res["loss_first"], res
+    g = res["gain_channels"]
+    # the moving channels are predicted better than carried over ...
+    assert res["gain_velocity"] > 1.5, res
+    assert g["u"] > 1.5 and g["v"] > 1.5, g
+    # ... the quiet ones are carried over, not spoilt, and the whole state gains
+    assert g["q"] > 0.9 and g["phi"] > 0.9, g
+    assert res["gain"] > 1.0, res
     assert all(math.isfinite(x) for x in res["nu_e_warm_after_relax"])
