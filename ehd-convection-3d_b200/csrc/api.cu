@@ -594,11 +594,15 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
             pa.pz = make_plan(lz2);
         }
     }
+    // where 2 (nz - 1) is not a compile-time size, the Thomas solve stays
+    // available beside the run-time sine transform (ehd_tuning.z_solve)
+    const bool thomas = !poisson_fast_size(lz2);
     double *cpt = nullptr;
     void *twz = nullptr;
     if (zdst) {
         if ((r = dalloc(c, &twz, c->rsize * (size_t)(2 * lz2 + lz2 / 2 + 1)))) return bail(r);
-    } else {
+    }
+    if (thomas) {
         if ((r = dalloc(c, (void **)&cpt, sizeof(double) * nmodes * (size_t)(nz - 2)))) return bail(r);
         if ((r = dalloc(c, (void **)&pa.dpw, sizeof(double2) * nmodes * (size_t)(nz - 2)))) return bail(r);
     }
@@ -653,7 +657,8 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
                 std::vector<float> tf(t.begin(), t.end());
                 EHD_CK(cudaMemcpy(twz, tf.data(), sizeof(float) * tf.size(), cudaMemcpyHostToDevice));
             }
-        } else {
+        }
+        if (thomas) {
             // Thomas pivots per mode (kx, ky): beta = 2 + (kx^2 + ky^2) dz^2 with
             // the wavenumbers of main.cu:110-129, cp_0 = -1/beta,
             // cp_i = 1/(-beta - cp_{i-1}); layout [i][ky*nxh + kx].
@@ -729,6 +734,7 @@ int ehd_set_tuning(ehd_ctx *c, const ehd_tuning *t) {
     if (t->lbm_kernel != 0 && t->lbm_kernel != 1) return fail(EHD_ERR_INVALID, "lbm_kernel must be 0 or 1");
     if (t->poisson_path != 0 && t->poisson_path != 1)
         return fail(EHD_ERR_INVALID, "poisson_path must be 0 or 1");
+    if (t->z_solve != 0 && t->z_solve != 1) return fail(EHD_ERR_INVALID, "z_solve must be 0 or 1");
     const int bx = t->node_block_x;
     if (bx != 16 && bx != 32 && bx != 64 && bx != 128)
         return fail(EHD_ERR_INVALID, "node_block_x must be 16, 32, 64 or 128 (got %d)", bx);
@@ -748,6 +754,7 @@ int ehd_set_tuning(ehd_ctx *c, const ehd_tuning *t) {
     c->pa.rows_per_block = t->fft_rows;
     c->pa.cols_per_block = t->fft_cols;
     c->pa.split = t->poisson_path == 0 ? 1 : 0;
+    c->pa.thomas = t->z_solve == 1 && c->pa.cpt ? 1 : 0;
     return EHD_OK;
 }
 

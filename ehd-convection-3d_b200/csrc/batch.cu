@@ -83,7 +83,7 @@ int upload(const X *host, size_t n, std::vector<void *> &bufs, X **dev) {
 // One group of instances with the same grid and launch shapes, and the
 // device descriptors of its launches.
 struct Group {
-    int nx = 0, ny = 0, nz = 0, n = 0;
+    int nx = 0, ny = 0, nz = 0, n = 0, bx = 0;
     void *lbm = nullptr;
     ReduceDesc *red = nullptr;
     PoissonArgs pa{};
@@ -119,6 +119,7 @@ int build_group(ehd_batch *b, const std::vector<size_t> &members, bool macros,
     g->ny = p->ny;
     g->nz = p->nz;
     g->n = n;
+    g->bx = la[0].node_bx;
     g->lbm = ld;
     g->pa = pa0;
     g->pa.grp = pd;
@@ -136,7 +137,8 @@ int capture_groups(ehd_batch *b, const std::vector<char> &act, bool macros,
         const ehd_params *p = ctx_params(b->inst[i]);
         ehd_tuning t{};
         ctx_tuning(b->inst[i], &t);
-        groups[{p->nx, p->ny, p->nz, t.node_block_x, t.fft_rows, t.fft_cols, t.poisson_path}]
+        groups[{p->nx, p->ny, p->nz, t.node_block_x, t.fft_rows, t.fft_cols, t.poisson_path,
+                t.z_solve}]
             .push_back(i);
     }
     std::vector<Group> gl;
@@ -149,7 +151,8 @@ int capture_groups(ehd_batch *b, const std::vector<char> &act, bool macros,
     cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_fail("batch capture", e);
     for (const Group &g : gl)
-        if (e == cudaSuccess) e = launch_lbm_group<T, R>(g.lbm, g.n, g.nx, g.ny, g.nz, macros, b->stream);
+        if (e == cudaSuccess)
+            e = launch_lbm_group<T, R>(g.lbm, g.n, g.nx, g.ny, g.nz, g.bx, macros, b->stream);
     for (const Group &g : gl)
         if (e == cudaSuccess) e = launch_reduce_tables_group<R>(g.red, g.n, g.nz, b->stream);
     for (const Group &g : gl)
@@ -536,6 +539,11 @@ int ehd_batch_autotune(ehd_batch *b, int trial_steps) {
         if (r == EHD_OK) {  // the split-y or the five-kernel Poisson solve
             ehd_tuning t = best;
             t.poisson_path = 1 - best.poisson_path;
+            r = trial(t);
+        }
+        if (r == EHD_OK && !poisson_fast_size(2 * (p.nz - 1))) {  // sine transform or Thomas
+            ehd_tuning t = best;
+            t.z_solve = 1 - best.z_solve;
             r = trial(t);
         }
         if (!poisson_fast_size(p.nx))

@@ -66,9 +66,10 @@ size_t lbm_group_desc_bytes(int n);
 // host memory of lbm_group_desc_bytes(n) bytes, to be copied to the device
 template <typename T, typename R>
 void build_lbm_group_desc(const LbmArgs *la, const StepConst *c, int n, void *host);
+// bx: the per-node block width (16, 32, 64 or 128) of every instance of the group
 template <typename T, typename R>
-cudaError_t launch_lbm_group(const void *desc_dev, int n, int nx, int ny, int nz, bool macros,
-                             cudaStream_t s);
+cudaError_t launch_lbm_group(const void *desc_dev, int n, int nx, int ny, int nz, int bx,
+                             bool macros, cudaStream_t s);
 // one instance's arguments of launch_reduce_tables
 struct ReduceDesc {
     const float2 *psum;
@@ -139,6 +140,7 @@ struct PoissonPtrs {
 struct PoissonArgs {
     int nx, ny, nz, nxh, pitch;
     int split;           // 1: the split-y three-kernel path where it applies
+    int thomas;          // 1: the Thomas z solve where the sine transform is run-time
     int rows_per_block;  // x-row FFT batch per block (run-time radix path)
     int cols_per_block;  // y-column FFT batch per block (run-time radix path)
     FftPlan px, py;

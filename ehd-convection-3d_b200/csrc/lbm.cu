@@ -1011,9 +1011,8 @@ void build_lbm_group_desc(const LbmArgs *la, const StepConst *c, int n, void *ho
     }
 }
 template <typename T, typename R>
-cudaError_t launch_lbm_group(const void *desc_dev, int n, int nx, int ny, int nz, bool macros,
-                             cudaStream_t s) {
-    const int bx = lbm_default_block_x(nx);
+cudaError_t launch_lbm_group(const void *desc_dev, int n, int nx, int ny, int nz, int bx,
+                             bool macros, cudaStream_t s) {
     const dim3 block(bx, 128 / bx, 1);
     const dim3 grid((nx + bx - 1) / bx, (ny + block.y - 1) / block.y, nz * n);
     const auto *d = reinterpret_cast<const LbmGroupDesc<T, R> *>(desc_dev);
@@ -1087,7 +1086,8 @@ cudaError_t launch_materialize(const void *rho, const void *u, const void *v, co
     const StepConst &, int, int, bool, cudaStream_t); \
     template size_t lbm_group_desc_bytes<T, R>(int); \
     template void build_lbm_group_desc<T, R>(const LbmArgs *, const StepConst *, int, void *); \
-    template cudaError_t launch_lbm_group<T, R>(const void *, int, int, int, int, bool, cudaStream_t);
+    template cudaError_t launch_lbm_group<T, R>(const void *, int, int, int, int, int, bool, \
+                                                cudaStream_t);
 EHD_INST_LBM(double, double)
 EHD_INST_LBM(float, float)
 EHD_INST_LBM(__half, float)
@@ -1298,7 +1298,19 @@ template cudaError_t launch_build_tables<double>(const double *, double *, const
                                                  void *, const StepConst &, cudaStream_t);
 
 // number of per-warp partial sums per plane written by the step kernel
-int lbm_default_block_x(int nx) { return nx >= 64 ? 64 : 32; }
+// the widest of 64, 32, 16 that leaves the fewest idle lanes at the row end
+// (96 -> 32, 80 and 48 -> 16, 256 and 122 -> 64)
+int lbm_default_block_x(int nx) {
+    int best = 64, waste = 1 << 30;
+    for (int bx : {64, 32, 16}) {
+        const int w = (nx + bx - 1) / bx * bx - nx;
+        if (w < waste) {
+            waste = w;
+            best = bx;
+        }
+    }
+    return best;
+}
 
 int lbm_blocks_per_plane(int nx, int ny, int bx) {
     const int by = 128 / bx;

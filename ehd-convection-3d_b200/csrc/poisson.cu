@@ -1673,7 +1673,7 @@ cudaError_t launch_poisson(const PoissonArgs &a, cudaStream_t s) {
             default: e = zdst<R, 512>(a, s); break;
         }
         if (e != cudaSuccess) return e;
-    } else if (a.twz) {
+    } else if (a.twz && !(a.thomas && a.cpt)) {
         const int modes = a.nxh * a.ny;
         const int L = 2 * (a.nz - 1);
         const size_t sm = zdst_rt_smem(L, a.ztb, sizeof(R));

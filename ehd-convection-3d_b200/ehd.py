@@ -77,7 +77,8 @@ class Diag(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("lbm_kernel", ctypes.c_int32), ("node_block_x", ctypes.c_int32),
                 ("fft_rows", ctypes.c_int32), ("fft_cols", ctypes.c_int32),
-                ("poisson_path", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
+                ("poisson_path", ctypes.c_int32), ("z_solve", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 2)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -221,6 +221,33 @@ def test_poisson_split_path_matches_oracle_and_five_kernel_path(shape, prec, tol
         assert relerr(out[0][k], out[1][k]) < tol, (k, "five-kernel", relerr(out[0][k], out[1][k]))
 
 
+@pytest.mark.parametrize("shape", [(48, 40, 25), (122, 122, 101), (30, 25, 7)])
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("fp32", 2e-6)])
+def test_z_solve_choices_match_oracle(shape, prec, tol):
+    """Where 2 (NZ - 1) is not a compile-time FFT size, the z solve is the sine
+    transform with run-time FFT passes (ehd_tuning.z_solve = 0) or the FP64
+    Thomas sweep (z_solve = 1); both against the oracle's odd-extension DFT
+    solve (poisson.cu:78-167) on random charge."""
+    nx, ny, nz = shape
+    dz = 1.0 / (nz - 1)
+    p = O.params_from_groups(nx, ny, nz, nx * dz, ny * dz, T=200, M=10, C=10, Fe=4000)
+    f = random_fields(p, 6)
+    o = O.Oracle(p)
+    o.set_fields(f)
+    o.poisson()
+    o.efield()
+    b = o.get_fields()
+    o.close()
+    for zs in (0, 1):
+        with ehd.Simulation(to_ehd(p), prec) as sim:
+            sim.set_tuning(z_solve=zs)
+            sim.set_fields(f)
+            sim.poisson()
+            a = sim.get_fields()
+        for k in ("phi", "ex", "ey", "ez"):
+            assert relerr(a[k], b[k]) < tol, (zs, k, relerr(a[k], b[k]))
+
+
 @pytest.mark.parametrize("shape", [(64, 48, 33), (96, 64, 65), (32, 20, 129), (16, 12, 257)])
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("fp32", 2e-6)])
 def test_poisson_sine_transform_z_solve_matches_oracle(shape, prec, tol):
