@@ -611,8 +611,8 @@ def main():
                          "time to saturated Nu_e on the reference's default case; batch: "
                          "the 64-instance batched T-sweep's step rate")
     ap.add_argument("--autotune", action="store_true", help="batch workload: autotune first")
-    ap.add_argument("--batch-mode", type=int, choices=[0, 1], default=0,
-                    help="batch workload: 0 grouped launches, 1 per-instance graph branches")
+    ap.add_argument("--batch-mode", type=int, choices=[0, 1], default=1,
+                    help="batch workload: 1 per-instance graph branches, 0 grouped launches")
     ap.add_argument("--sat-max-steps", type=int, default=6_000_000)
     ap.add_argument("--ref-window", type=int, default=20_000,
                     help="reference arm of the saturation workload: steps it runs")

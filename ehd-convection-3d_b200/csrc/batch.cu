@@ -26,7 +26,7 @@ using namespace ehd;
 
 struct ehd_batch {
     int device = 0;
-    int mode = 0;  // 0: grouped launches, 1: per-instance graph branches
+    int mode = 1;  // 0: grouped launches, 1: per-instance graph branches
     cudaStream_t stream = nullptr;
     std::vector<ehd_ctx *> inst;
     std::vector<char> active;

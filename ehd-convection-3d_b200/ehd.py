@@ -407,8 +407,8 @@ class Batch:
         _check(lib().ehd_batch_set_active(self.h, int(i), int(bool(active))))
 
     def set_mode(self, mode: int):
-        """ehd_batch_set_mode: 0 grouped launches (default), 1 per-instance
-        graph branches."""
+        """ehd_batch_set_mode: 1 per-instance graph branches (default), 0
+        grouped launches."""
         _check(lib().ehd_batch_set_mode(self.h, int(mode)))
 
     def step(self, n: int = 1):

@@ -272,13 +272,15 @@ int ehd_batch_size(const ehd_batch *batch);
 int ehd_batch_instance(ehd_batch *batch, int i, ehd_ctx **ctx);
 int ehd_batch_set_active(ehd_batch *batch, int i, int active);
 /* How a batch step launches its instances (no reference counterpart).
- * mode 0 (the default): instances with the same grid and launch shapes form a
- * group, and each kernel of the step is one launch over every instance of a
- * group (the LBM half on the per-node kernel, each instance's result bitwise
- * that of a lone context on the per-node kernel with the same shapes); one
- * CUDA graph per step holds the groups' launches.  mode 1: one graph per step
- * with a branch per instance holding that instance's own launches (the row
- * kernel where it applies). */
+ * mode 1 (the default): one CUDA graph per step with a branch per instance
+ * holding that instance's own launches (the row kernel where it applies);
+ * each instance's result is bitwise that of a lone context.  mode 0: instances
+ * with the same grid and launch shapes form a group, and each kernel of the
+ * step is one launch over every instance of a group (the LBM half on the
+ * per-node kernel), one graph per step holding the groups' launches; an
+ * instance's result agrees with a lone context on the per-node kernel to FP32
+ * round-off (the grouped kernels are separate compilations, whose
+ * multiply-add contractions may differ). */
 int ehd_batch_set_mode(ehd_batch *batch, int mode);
 /* nsteps steps of every active instance.  Instances whose next step is the
  * first after an upload take that step on their own streams; after it, one

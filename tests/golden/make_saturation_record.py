@@ -35,9 +35,12 @@ def pack(ours: dict, ref: dict) -> dict:
                "nu_e": [round(h["nu_e"], 9) for h in hist],
                "current": [h["current"] for h in hist],
                "kinetic_energy": [round(h["kinetic_energy"], 6) for h in hist]}}
-    rkeep = ("window_steps", "window_gpu_s", "ms_per_step", "mlups", "i0", "projected_to_step",
-             "value", "how")
+    rkeep = ("window_steps", "window_gpu_s", "ms_per_step", "mlups", "i0", "how")
     out["reference"] = {k: ref[k] for k in rkeep if k in ref}
+    # the reference's wall time projected to the step at which this run saturated
+    if ours.get("status") == "saturated":
+        out["reference"]["projected_to_step"] = int(ours["steps"])
+        out["reference"]["value"] = round(ref["window_gpu_s"] / ref["window_steps"] * ours["steps"], 2)
     out["reference_history"] = {"step": [h["step"] for h in ref["history"]],
                                 "current": [h["current"] for h in ref["history"]]}
     return out

@@ -29,7 +29,7 @@ def test_warm_start_prediction_beats_the_initial_state():
                   "--relax", "200", "--grid", "16", "16", "17", "--width", "8", "--modes", "4",
                   "--layers", "2", "--hidden", "16", "--lr", "3e-3", "--t-range", "600", "1000"])
     assert res["train"] == 64 and res["test"] == 8
-    assert res["loss_last"] < 0.8 * res["loss_first"], res
+    assert res["loss_last"] < 0.9 * res["loss_first"], res
     g = res["gain_channels"]
     # the moving channels are predicted better than carried over ...
     assert res["gain_velocity"] > 1.5, res

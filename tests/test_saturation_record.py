@@ -9,7 +9,8 @@ Checked here, without a GPU:
     the recorded end and at no earlier sample;
   * over the reference's window (its collector current printed every 1000
     steps, main.cu:227-231, "%g") this build's currents at the same steps agree
-    with the reference's to 1e-3 (FP32 against FP64, six printed digits);
+    with the reference's to 2e-5 in FP64 (six printed digits) and 1e-3 in
+    FP32;
   * the projected reference wall time is its time per step times the step at
     which this build's run saturated.
 """
@@ -47,8 +48,10 @@ def test_saturation_record(path):
     ref, rhist = rec["reference"], rec["reference_history"]
     mine = dict(zip(hist["step"], hist["current"]))
     assert len(rhist["step"]) >= 10
+    # FP64 against FP64 is limited by the reference's six printed digits
+    tol = 2e-5 if ours["precision"] == "fp64" else 1e-3
     for s, c in zip(rhist["step"], rhist["current"]):
-        assert abs(mine[s] - c) <= 1e-3 * abs(c), (s, mine[s], c)
+        assert abs(mine[s] - c) <= tol * abs(c), (s, mine[s], c)
     if ref.get("projected_to_step"):
         assert ref["projected_to_step"] == ours["steps"]
         assert ref["value"] == pytest.approx(ref["window_gpu_s"] / ref["window_steps"]
