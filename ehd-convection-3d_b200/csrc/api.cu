@@ -406,11 +406,14 @@ int ctx_step_args(ehd_ctx *c, bool macros, LbmArgs *la, StepConst *sc, ReduceDes
     a.zref = c->ktab[p];
     a.psum = c->psum;
     a.err = c->err;
-    a.rows_grid = 0;
+    // the steady-state step's kernel, as in lbm(): the row kernel where it is
+    // available and chosen, else the per-node kernel
+    const bool rows = c->rows_grid > 0 && c->tune.lbm_kernel == 0;
+    a.rows_grid = rows ? c->rows_grid : 0;
     a.node_bx = c->tune.node_block_x;
     *la = a;
     *sc = c->sc;
-    // the reduction of lbm() for the per-node kernel's plane-sum slots
+    // the reduction of lbm() for that kernel's plane-sum slots
     rd->psum = c->psum;
     rd->m = c->mean[p ^ 1];
     rd->msrc = c->mean[p];
@@ -418,7 +421,8 @@ int ctx_step_args(ehd_ctx *c, bool macros, LbmArgs *la, StepConst *sc, ReduceDes
     rd->wread = c->wref[p ^ 1];
     rd->ktab = c->ktab[p ^ 1];
     rd->nxy = c->sc.nxy;
-    rd->nblk = lbm_blocks_per_plane(c->p.nx, c->p.ny, c->tune.node_block_x);
+    rd->nblk = rows ? lbm_rows_slots_per_plane(c->p.nx, c->p.ny)
+                    : lbm_blocks_per_plane(c->p.nx, c->p.ny, c->tune.node_block_x);
     rd->nz = c->p.nz;
     // poisson() after lbm() reads the plane means of the new state
     *pa = c->pa;
@@ -857,10 +861,7 @@ int ehd_set_reference_current(ehd_ctx *c, double i0) {
     return EHD_OK;
 }
 
-int ehd_diagnostics(ehd_ctx *c, ehd_diag *o) {
-    if (!c || !o) return fail(EHD_ERR_INVALID, "NULL argument");
-    if (!c->have_state) return fail(EHD_ERR_STATE, "no state: call ehd_set_fields first");
-    DeviceGuard dg(c->device);
+static DiagArgs diag_args(ehd_ctx *c) {
     DiagArgs a{};
     a.nx = c->p.nx;
     a.ny = c->p.ny;
@@ -877,6 +878,14 @@ int ehd_diagnostics(ehd_ctx *c, ehd_diag *o) {
     a.partial = c->diag_partial;
     a.result = c->diag_result;
     a.nblocks = c->diag_blocks;
+    return a;
+}
+
+int ehd_diagnostics(ehd_ctx *c, ehd_diag *o) {
+    if (!c || !o) return fail(EHD_ERR_INVALID, "NULL argument");
+    if (!c->have_state) return fail(EHD_ERR_STATE, "no state: call ehd_set_fields first");
+    DeviceGuard dg(c->device);
+    const DiagArgs a = diag_args(c);
     cudaError_t e = c->rsize == 8 ? launch_diag<double>(a, c->stream) : launch_diag<float>(a, c->stream);
     if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "diagnostics: %s", cudaGetErrorString(e));
     EHD_CK(cudaMemcpyAsync(c->host_diag, c->diag_result, sizeof(double) * 5,
@@ -898,11 +907,17 @@ int ehd_diagnostics(ehd_ctx *c, ehd_diag *o) {
 }
 
 int ehd_current(ehd_ctx *c, double *current) {
-    if (!current) return fail(EHD_ERR_INVALID, "NULL argument");
-    ehd_diag d;
-    int r = ehd_diagnostics(c, &d);
-    if (r != EHD_OK) return r;
-    *current = d.current;
+    if (!c || !current) return fail(EHD_ERR_INVALID, "NULL argument");
+    if (!c->have_state) return fail(EHD_ERR_STATE, "no state: call ehd_set_fields first");
+    DeviceGuard dg(c->device);
+    const DiagArgs a = diag_args(c);
+    cudaError_t e = c->rsize == 8 ? launch_current<double>(a, c->stream) : launch_current<float>(a, c->stream);
+    if (e != cudaSuccess) return fail(EHD_ERR_CUDA, "current: %s", cudaGetErrorString(e));
+    EHD_CK(cudaMemcpyAsync(c->host_diag, c->diag_result, sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream));
+    EHD_CK(cudaStreamSynchronize(c->stream));
+    if (int rc = check_device_error(c)) return rc;
+    *current = c->host_diag[0] * c->p.K * c->p.dy * c->p.dy;  // LBM.cu:1669
     return EHD_OK;
 }
 

@@ -84,6 +84,7 @@ int upload(const X *host, size_t n, std::vector<void *> &bufs, X **dev) {
 // device descriptors of its launches.
 struct Group {
     int nx = 0, ny = 0, nz = 0, n = 0, bx = 0;
+    int rows = 0;  // > 0: the row kernel on this many CTAs per instance
     void *lbm = nullptr;
     ReduceDesc *red = nullptr;
     PoissonArgs pa{};
@@ -120,6 +121,8 @@ int build_group(ehd_batch *b, const std::vector<size_t> &members, bool macros,
     g->nz = p->nz;
     g->n = n;
     g->bx = la[0].node_bx;
+    // the instances' persistent row-kernel CTAs shared among the group
+    g->rows = la[0].rows_grid > 0 ? std::max(1, la[0].rows_grid / n) : 0;
     g->lbm = ld;
     g->pa = pa0;
     g->pa.grp = pd;
@@ -137,8 +140,8 @@ int capture_groups(ehd_batch *b, const std::vector<char> &act, bool macros,
         const ehd_params *p = ctx_params(b->inst[i]);
         ehd_tuning t{};
         ctx_tuning(b->inst[i], &t);
-        groups[{p->nx, p->ny, p->nz, t.node_block_x, t.fft_rows, t.fft_cols, t.poisson_path,
-                t.z_solve}]
+        groups[{p->nx, p->ny, p->nz, t.lbm_kernel, t.node_block_x, t.fft_rows, t.fft_cols,
+                t.poisson_path, t.z_solve}]
             .push_back(i);
     }
     std::vector<Group> gl;
@@ -152,7 +155,10 @@ int capture_groups(ehd_batch *b, const std::vector<char> &act, bool macros,
     if (e != cudaSuccess) return cuda_fail("batch capture", e);
     for (const Group &g : gl)
         if (e == cudaSuccess)
-            e = launch_lbm_group<T, R>(g.lbm, g.n, g.nx, g.ny, g.nz, g.bx, macros, b->stream);
+            e = g.rows > 0 ? launch_lbm_rows_group<T, R>(g.lbm, g.n, g.nx, g.ny, g.rows, macros,
+                                                         b->stream)
+                           : launch_lbm_group<T, R>(g.lbm, g.n, g.nx, g.ny, g.nz, g.bx, macros,
+                                                    b->stream);
     for (const Group &g : gl)
         if (e == cudaSuccess) e = launch_reduce_tables_group<R>(g.red, g.n, g.nz, b->stream);
     for (const Group &g : gl)
@@ -528,8 +534,7 @@ int ehd_batch_autotune(ehd_batch *b, int trial_steps) {
             return EHD_OK;
         };
         const ehd_params &p = ps[g.second.front()];
-        // grouped launches run the per-node kernel: no row-kernel trials
-        for (int kern = 0; r == EHD_OK && kern <= (b->mode == 0 ? 0 : 1); ++kern)
+        for (int kern = 0; r == EHD_OK && kern <= 1; ++kern)
             for (int bx = 16; r == EHD_OK && bx <= 128; bx *= 2) {
                 ehd_tuning t = best;
                 t.lbm_kernel = kern;

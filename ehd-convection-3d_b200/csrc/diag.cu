@@ -120,4 +120,68 @@ cudaError_t launch_diag(const DiagArgs &a, cudaStream_t s) {
 template cudaError_t launch_diag<float>(const DiagArgs &, cudaStream_t);
 template cudaError_t launch_diag<double>(const DiagArgs &, cudaStream_t);
 
+// The current alone ([0] above) from the collector plane: q(NZ-2), q(NZ-3)
+// and phi'(NZ-3) of one plane instead of the whole field, the same per-node
+// term, a fixed partition of the plane into blocks and a fixed tree order.
+namespace {
+__device__ __forceinline__ double block_sum(double v, double *sm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) sm[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = lane < kDiagThreads / 32 ? sm[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+}  // namespace
+
+template <typename R>
+__global__ void __launch_bounds__(kDiagThreads)
+current_stage1(const R *__restrict__ q, const R *__restrict__ phip,
+               const double *__restrict__ ez00, const double *__restrict__ ez, double inv2dz,
+               int nxy, int nz, double *__restrict__ partial) {
+    __shared__ double sm[kDiagThreads / 32];
+    const int chunk = (nxy + gridDim.x - 1) / gridDim.x;
+    const int beg = chunk * blockIdx.x;
+    const int end = beg + chunk < nxy ? beg + chunk : nxy;
+    const size_t top = (size_t)(nz - 1) * nxy;
+    double acc = 0.0;
+    for (int p = beg + threadIdx.x; p < end; p += kDiagThreads) {
+        const double qt = 2.0 * (double)q[(size_t)(nz - 2) * nxy + p] - (double)q[(size_t)(nz - 3) * nxy + p];
+        const double e = ez != nullptr ? ez[top + p]
+                                       : ez00[nz - 2] + (double)phip[(size_t)(nz - 3) * nxy + p] * inv2dz;
+        acc += qt * e;
+    }
+    acc = block_sum(acc, sm);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+__global__ void __launch_bounds__(kDiagThreads)
+current_stage2(const double *__restrict__ partial, int nblocks, double *__restrict__ result) {
+    __shared__ double sm[kDiagThreads / 32];
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += kDiagThreads) acc += partial[b];
+    acc = block_sum(acc, sm);
+    if (threadIdx.x == 0) result[0] = acc;
+}
+
+template <typename R>
+cudaError_t launch_current(const DiagArgs &a, cudaStream_t s) {
+    const int nxy = a.nx * a.ny;
+    int nb = (nxy + 4 * kDiagThreads - 1) / (4 * kDiagThreads);
+    nb = nb < 1 ? 1 : (nb > a.nblocks ? a.nblocks : nb);
+    current_stage1<R><<<nb, kDiagThreads, 0, s>>>((const R *)a.q, (const R *)a.phip, a.ez00, a.ez,
+                                                  a.inv2dz, nxy, a.nz, a.partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    current_stage2<<<1, kDiagThreads, 0, s>>>(a.partial, nb, a.result);
+    return cudaGetLastError();
+}
+template cudaError_t launch_current<float>(const DiagArgs &, cudaStream_t);
+template cudaError_t launch_current<double>(const DiagArgs &, cudaStream_t);
+
 }  // namespace ehd

@@ -157,7 +157,8 @@ __device__ __forceinline__ void pass(R2 *buf, const R2 *tw, int j) {
     __syncthreads();
 }
 
-// Pass schedules for the power-of-two sizes; G = threads per transform.
+// Pass schedules of the compile-time sizes; G = threads per transform, a
+// divisor of 256 and at least the butterflies of every pass.
 template <int N> struct Plan;
 template <> struct Plan<64> {
     static constexpr int G = 8;
@@ -180,12 +181,157 @@ template <> struct Plan<256> {
         pass<256, 16, 16, S>(b, tw, j);
     }
 };
+// mixed radix (the grids of the T sweeps: 48, 80, 96 nodes, and their odd
+// extensions 2 (NZ - 1) = 48, 80, 96)
+template <> struct Plan<48> {
+    static constexpr int G = 16;
+    template <int S, typename R2> __device__ static void run(R2 *b, const R2 *tw, int j) {
+        pass<48, 16, 1, S>(b, tw, j);
+        pass<48, 3, 16, S>(b, tw, j);
+    }
+};
+template <> struct Plan<80> {
+    static constexpr int G = 16;
+    template <int S, typename R2> __device__ static void run(R2 *b, const R2 *tw, int j) {
+        pass<80, 16, 1, S>(b, tw, j);
+        pass<80, 5, 16, S>(b, tw, j);
+    }
+};
+template <> struct Plan<96> {
+    static constexpr int G = 32;
+    template <int S, typename R2> __device__ static void run(R2 *b, const R2 *tw, int j) {
+        pass<96, 8, 1, S>(b, tw, j);
+        pass<96, 4, 8, S>(b, tw, j);
+        pass<96, 3, 32, S>(b, tw, j);
+    }
+};
 template <> struct Plan<512> {
     static constexpr int G = 64;
     template <int S, typename R2> __device__ static void run(R2 *b, const R2 *tw, int j) {
         pass<512, 8, 1, S>(b, tw, j);
         pass<512, 8, 8, S>(b, tw, j);
         pass<512, 8, 64, S>(b, tw, j);
+    }
+};
+
+// ---- warp-synchronous transforms ----
+// The G <= 32 threads of a transform lie in one warp (t = lane % G) and
+// handle the butterflies j = t, t + G, ... of every pass; the warp
+// synchronises between a pass's loads and its stores, so every pass may work
+// in place.  The first pass takes its inputs from ld(m) and the last hands
+// each output m to st(m, value), so a caller gathers, scatters and scales on
+// the way in and out; the passes in between go through buf (padded, as
+// pass()).  The caller synchronises the warp before it reads what st wrote.
+template <int N, int R, int G, int S, typename R2, typename Ld>
+__device__ __forceinline__ void wpass_first(R2 *buf, const R2 *tw, int t, Ld ld) {
+    constexpr int NB = N / R, BPT = (NB + G - 1) / G;
+    R2 v[BPT][R];
+#pragma unroll
+    for (int b = 0; b < BPT; ++b) {
+        const int j = t + G * b;
+        if (j < NB) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[b][r] = ld(j + r * NB);
+            Dft<R, S, R2>::run(v[b], tw, NB);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int b = 0; b < BPT; ++b)
+        if (t + G * b < NB) pass_store<N, R, 1>(buf, t + G * b, v[b]);
+    __syncwarp();
+}
+template <int N, int R, int NS, int G, int S, typename R2>
+__device__ __forceinline__ void wpass(R2 *buf, const R2 *tw, int t) {
+    constexpr int NB = N / R, BPT = (NB + G - 1) / G;
+    R2 v[BPT][R];
+#pragma unroll
+    for (int b = 0; b < BPT; ++b)
+        if (t + G * b < NB) pass_compute<N, R, NS, S>(buf, tw, t + G * b, v[b]);
+    __syncwarp();
+#pragma unroll
+    for (int b = 0; b < BPT; ++b)
+        if (t + G * b < NB) pass_store<N, R, NS>(buf, t + G * b, v[b]);
+    __syncwarp();
+}
+template <int N, int R, int NS, int G, int S, typename R2, typename St>
+__device__ __forceinline__ void wpass_last(const R2 *buf, const R2 *tw, int t, St st) {
+    constexpr int NB = N / R, BPT = (NB + G - 1) / G;
+    R2 v[BPT][R];
+#pragma unroll
+    for (int b = 0; b < BPT; ++b)
+        if (t + G * b < NB) pass_compute<N, R, NS, S>(buf, tw, t + G * b, v[b]);
+    __syncwarp();
+#pragma unroll
+    for (int b = 0; b < BPT; ++b) {
+        const int j = t + G * b;
+        if (j < NB) {
+            const int base = (j / NS) * NS * R + j % NS;
+#pragma unroll
+            for (int r = 0; r < R; ++r) st(base + r * NS, v[b][r]);
+        }
+    }
+}
+
+// A transform of sign S1, a pointwise map mid(k, X[k]) of its output, a
+// transform of sign S2, for N = R * R by G = R threads.  The first
+// transform's last pass leaves the outputs k = t + R r in the registers that
+// the second's first pass reads as its inputs t + R r, so the spectrum never
+// goes through buf.
+template <int N, int R, int S1, int S2, typename R2, typename Ld, typename Mid, typename St>
+__device__ __forceinline__ void wfilter_sq(R2 *buf, const R2 *tw, int t, Ld ld, Mid mid, St st) {
+    static_assert(R * R == N, "square sizes only");
+    R2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = ld(t + R * r);
+    Dft<R, S1, R2>::run(v, tw, R);
+    pass_store<N, R, 1>(buf, t, v);
+    __syncwarp();
+    pass_compute<N, R, R, S1>(buf, tw, t, v);
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = mid(t + R * r, v[r]);
+    Dft<R, S2, R2>::run(v, tw, R);
+    __syncwarp();
+    pass_store<N, R, 1>(buf, t, v);
+    __syncwarp();
+    pass_compute<N, R, R, S2>(buf, tw, t, v);
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < R; ++r) st(t + R * r, v[r]);
+}
+
+template <int N> struct WPlan;
+template <> struct WPlan<64> {
+    static constexpr int G = 8;
+    template <int S, typename R2, typename Ld, typename St>
+    __device__ static void run(R2 *b, const R2 *tw, int t, Ld ld, St st) {
+        wpass_first<64, 8, G, S>(b, tw, t, ld);
+        wpass_last<64, 8, 8, G, S>(b, tw, t, st);
+    }
+};
+template <> struct WPlan<128> {
+    static constexpr int G = 16;
+    template <int S, typename R2, typename Ld, typename St>
+    __device__ static void run(R2 *b, const R2 *tw, int t, Ld ld, St st) {
+        wpass_first<128, 8, G, S>(b, tw, t, ld);
+        wpass_last<128, 16, 8, G, S>(b, tw, t, st);
+    }
+};
+template <> struct WPlan<256> {
+    static constexpr int G = 16;
+    template <int S, typename R2, typename Ld, typename St>
+    __device__ static void run(R2 *b, const R2 *tw, int t, Ld ld, St st) {
+        wpass_first<256, 16, G, S>(b, tw, t, ld);
+        wpass_last<256, 16, 16, G, S>(b, tw, t, st);
+    }
+};
+template <> struct WPlan<512> {
+    static constexpr int G = 32;
+    template <int S, typename R2, typename Ld, typename St>
+    __device__ static void run(R2 *b, const R2 *tw, int t, Ld ld, St st) {
+        wpass_first<512, 8, G, S>(b, tw, t, ld);
+        wpass<512, 8, 8, G, S>(b, tw, t);
+        wpass_last<512, 8, 64, G, S>(b, tw, t, st);
     }
 };
 

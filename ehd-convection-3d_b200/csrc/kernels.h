@@ -70,6 +70,11 @@ void build_lbm_group_desc(const LbmArgs *la, const StepConst *c, int n, void *ho
 template <typename T, typename R>
 cudaError_t launch_lbm_group(const void *desc_dev, int n, int nx, int ny, int nz, int bx,
                              bool macros, cudaStream_t s);
+// the same step on the bulk-copy row kernel (lbm_rows_usable grids), per_inst
+// CTAs per instance
+template <typename T, typename R>
+cudaError_t launch_lbm_rows_group(const void *desc_dev, int n, int nx, int ny, int per_inst,
+                                  bool macros, cudaStream_t s);
 // one instance's arguments of launch_reduce_tables
 struct ReduceDesc {
     const float2 *psum;
@@ -193,6 +198,9 @@ struct DiagArgs {
 };
 template <typename R>
 cudaError_t launch_diag(const DiagArgs &a, cudaStream_t s);
+// the current alone into result[0] (partial: at least a.nblocks doubles)
+template <typename R>
+cudaError_t launch_current(const DiagArgs &a, cudaStream_t s);
 
 // sets the calling thread's ehd_last_error message; returns code
 int set_error(int code, const char *msg);

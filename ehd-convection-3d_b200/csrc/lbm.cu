@@ -660,9 +660,13 @@ __device__ __forceinline__ int ez_rt(int d) { return (int)((kEzPack >> (2 * d)) 
 // kernel, launched for that plane alone.  A wait that does not complete within
 // kWaitLimit polls sets *err, waits (bounded) for the copies that may still
 // be landing, and ends the warp.
+//
+// rows_run is the loop of CTA blk of nblk; lbm_rows_kernel runs one instance,
+// lbm_rows_group_kernel several instances of the same NX (blockIdx.y) with
+// their arguments from a device table.
 template <typename T, typename R, bool MACROS>
-__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 1 : 2)
-lbm_rows_kernel(const StepArgs<T, R> a, const KConst<R> c) {
+__device__ __forceinline__ void rows_run(const StepArgs<T, R> &a, const KConst<R> &c, int blk,
+                                         int nblk) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ unsigned long long bar[2];
     __shared__ unsigned cnt[2];
@@ -711,9 +715,9 @@ lbm_rows_kernel(const StepArgs<T, R> a, const KConst<R> c) {
         }
         return n < kWaitLimit;
     };
-    // rows r = NY + blockIdx.x + k gridDim.x, r < NY NZ, as (y, z); a step of
-    // gridDim.x rows advances y by gy and z by gz (plus the carry)
-    const int g = (int)gridDim.x, gy = g % NY, gz = g / NY;
+    // rows r = NY + blk + k nblk, r < NY NZ, as (y, z); a step of nblk rows
+    // advances y by gy and z by gz (plus the carry)
+    const int g = nblk, gy = g % NY, gz = g / NY;
     auto advance = [&](int &yy, int &zz) {
         yy += gy;
         zz += gz;
@@ -724,7 +728,7 @@ lbm_rows_kernel(const StepArgs<T, R> a, const KConst<R> c) {
     };
 
     unsigned phases = 0u;  // bit s: parity of the next phase of bar[s]
-    int y = (int)(blockIdx.x % NY), z = 1 + (int)(blockIdx.x / NY);
+    int y = blk % NY, z = 1 + blk / NY;
     if (warp == 0) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         int y1 = y, z1 = z;
@@ -787,6 +791,40 @@ lbm_rows_kernel(const StepArgs<T, R> a, const KConst<R> c) {
             }
         }
     }
+}
+
+template <typename T, typename R, bool MACROS>
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 1 : 2)
+lbm_rows_kernel(const StepArgs<T, R> a, const KConst<R> c) {
+    rows_run<T, R, MACROS>(a, c, (int)blockIdx.x, (int)gridDim.x);
+}
+
+template <typename T, typename R>
+struct LbmGroupDesc {
+    StepArgs<T, R> a;
+    KConst<R> k;
+};
+
+// A copy of the instance's descriptor in shared memory, as 8-byte words.
+template <typename T, typename R>
+__device__ __forceinline__ void load_group_desc(LbmGroupDesc<T, R> &sd,
+                                                const LbmGroupDesc<T, R> *__restrict__ desc,
+                                                int inst) {
+    static_assert(sizeof(LbmGroupDesc<T, R>) % 8 == 0, "copied as 8-byte words");
+    constexpr int W = sizeof(LbmGroupDesc<T, R>) / 8;
+    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(desc + inst);
+    unsigned long long *dst = reinterpret_cast<unsigned long long *>(&sd);
+    const int nt = blockDim.x * blockDim.y;
+    for (int i = threadIdx.x + blockDim.x * threadIdx.y; i < W; i += nt) dst[i] = src[i];
+}
+
+template <typename T, typename R, bool MACROS>
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 1 : 2)
+lbm_rows_group_kernel(const LbmGroupDesc<T, R> *__restrict__ desc) {
+    __shared__ LbmGroupDesc<T, R> sd;
+    load_group_desc(sd, desc, (int)blockIdx.y);
+    __syncthreads();
+    rows_run<T, R, MACROS>(sd.a, sd.k, (int)blockIdx.x, (int)gridDim.x);
 }
 
 // Equilibrium populations from the FP64 fields (gpu_init_equilibrium,
@@ -921,7 +959,9 @@ cudaError_t prepare_lbm_rows(int nx, int ny, int nz, int *grid) {
     const int sm = (int)lbm_rows_smem(nx, sizeof(F), sizeof(G));
     cudaError_t e;
     if ((e = allow_max_dynamic_smem(lbm_rows_kernel<T, R, true>)) != cudaSuccess ||
-        (e = allow_max_dynamic_smem(lbm_rows_kernel<T, R, false>)) != cudaSuccess)
+        (e = allow_max_dynamic_smem(lbm_rows_kernel<T, R, false>)) != cudaSuccess ||
+        (e = allow_max_dynamic_smem(lbm_rows_group_kernel<T, R, true>)) != cudaSuccess ||
+        (e = allow_max_dynamic_smem(lbm_rows_group_kernel<T, R, false>)) != cudaSuccess)
         return e;
     int dev = 0, nsm = 0, occ_a = 0, occ_b = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
@@ -974,25 +1014,12 @@ static StepArgs<T, R> make_step_args(const LbmArgs &la, const StepConst &c) {
 // constants (about 1.3 KB) into shared memory and runs the same node_block as
 // lbm_step_kernel, so an instance's result is bitwise that of a lone context
 // on the per-node kernel with the default block shape.
-template <typename T, typename R>
-struct LbmGroupDesc {
-    StepArgs<T, R> a;
-    KConst<R> k;
-};
-
 template <typename T, typename R, bool MACROS>
 __global__ void __launch_bounds__(128, sizeof(R) == 8 ? 2 : 4)
 lbm_group_kernel(const LbmGroupDesc<T, R> *__restrict__ desc, int nz) {
     __shared__ LbmGroupDesc<T, R> sd;
     const int inst = blockIdx.z / nz, z = blockIdx.z - inst * nz;
-    {
-        static_assert(sizeof(LbmGroupDesc<T, R>) % 8 == 0, "copied as 8-byte words");
-        constexpr int W = sizeof(LbmGroupDesc<T, R>) / 8;
-        const unsigned long long *src = reinterpret_cast<const unsigned long long *>(desc + inst);
-        unsigned long long *dst = reinterpret_cast<unsigned long long *>(&sd);
-        for (int i = threadIdx.x + blockDim.x * threadIdx.y; i < W; i += blockDim.x * blockDim.y)
-            dst[i] = src[i];
-    }
+    load_group_desc(sd, desc, inst);
     __syncthreads();
     node_block<T, R, false, MACROS>(sd.a, sd.k, blockIdx.x, blockIdx.y, z, gridDim.x, gridDim.y,
                                     0, 0);
@@ -1018,6 +1045,26 @@ cudaError_t launch_lbm_group(const void *desc_dev, int n, int nx, int ny, int nz
     const auto *d = reinterpret_cast<const LbmGroupDesc<T, R> *>(desc_dev);
     if (macros) lbm_group_kernel<T, R, true><<<grid, block, 0, s>>>(d, nz);
     else lbm_group_kernel<T, R, false><<<grid, block, 0, s>>>(d, nz);
+    return cudaGetLastError();
+}
+
+// The steady-state step of a group on the row kernel: plane z = 0 of every
+// instance on the per-node kernel in blocks of whole warps along x (its plane
+// sums land in the row kernel's slots [y][x / 32]), then the planes z >= 1 on
+// per_inst CTAs of the row kernel per instance.
+template <typename T, typename R>
+cudaError_t launch_lbm_rows_group(const void *desc_dev, int n, int nx, int ny, int per_inst,
+                                  bool macros, cudaStream_t s) {
+    const auto *d = reinterpret_cast<const LbmGroupDesc<T, R> *>(desc_dev);
+    int bx = 128;
+    while (nx % bx != 0) bx -= 32;
+    const dim3 g0(nx / bx, ny, n);
+    if (macros) lbm_group_kernel<T, R, true><<<g0, bx, 0, s>>>(d, 1);
+    else lbm_group_kernel<T, R, false><<<g0, bx, 0, s>>>(d, 1);
+    const size_t sm = lbm_rows_smem(nx, sizeof(typename PopT<T>::F), sizeof(typename PopT<T>::G));
+    const dim3 g1(per_inst, n, 1);
+    if (macros) lbm_rows_group_kernel<T, R, true><<<g1, nx, sm, s>>>(d);
+    else lbm_rows_group_kernel<T, R, false><<<g1, nx, sm, s>>>(d);
     return cudaGetLastError();
 }
 
@@ -1087,7 +1134,9 @@ cudaError_t launch_materialize(const void *rho, const void *u, const void *v, co
     template size_t lbm_group_desc_bytes<T, R>(int); \
     template void build_lbm_group_desc<T, R>(const LbmArgs *, const StepConst *, int, void *); \
     template cudaError_t launch_lbm_group<T, R>(const void *, int, int, int, int, int, bool, \
-                                                cudaStream_t);
+                                                cudaStream_t); \
+    template cudaError_t launch_lbm_rows_group<T, R>(const void *, int, int, int, int, bool, \
+                                                     cudaStream_t);
 EHD_INST_LBM(double, double)
 EHD_INST_LBM(float, float)
 EHD_INST_LBM(__half, float)

@@ -381,6 +381,9 @@ poisson_rows_inv(const typename Cplx<R>::T *__restrict__ spec, R *__restrict__ p
 // the transposed (column-major) accesses do not collide on one bank
 template <int N> __host__ __device__ constexpr int tstride() { return fft::padded(N) + 1; }
 template <int N> constexpr int per_block() { return 256 / fft::Plan<N>::G; }
+// rows of a split-path slab: the n = L/2 - 1 interior planes rounded up to
+// whole rounds of 32 rows (8 warps of 4 FFT64s)
+template <int L> constexpr int slab_rows() { return (L / 2 - 1 + 31) / 32 * 32; }
 
 template <typename R, int N>
 __device__ __forceinline__ void load_twiddles(typename Cplx<R>::T *tws,
@@ -454,7 +457,7 @@ poisson_rows_fwd_fast(const R *__restrict__ q, typename Cplx<R>::T *__restrict__
         const int t2 = i / nxh, k = i - t2 * nxh;
         const int ya = y0 + 2 * t2, yb = ya + 1;
         const R2 zk = buf[t2 * P + fft::pad(k)];
-        const R2 zn = buf[t2 * P + fft::pad((N - k) & (N - 1))];
+        const R2 zn = buf[t2 * P + fft::pad(k == 0 ? 0 : N - k)];
         const R2 A = R2{(R)0.5 * (zk.x + zn.x), (R)0.5 * (zk.y - zn.y)};
         const R2 B = R2{(R)0.5 * (zk.y + zn.y), (R)0.5 * (zn.x - zk.x)};
         if (ya < ny) sp[(size_t)pitch * ya + k] = A;
@@ -970,6 +973,15 @@ poisson_zdst_rt(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::
 // contiguous block.
 namespace {
 
+// x, hidden from the optimiser: the values derived from it inside a loop are
+// recomputed in each iteration instead of being hoisted into registers that
+// stay live over the whole loop
+__device__ __forceinline__ int opaque(int x) {
+    int y;
+    asm volatile("mov.b32 %0, %1;" : "=r"(y) : "r"(x));
+    return y;
+}
+
 // rows (ya, yb) of transform tr of a split-row block (two real rows per
 // complex transform): S = 1 pairs consecutive rows; S >= 2 pairs
 // n + 64 a and n + 64 (a + S/2) of group n = block * GB + tr / (S/2)
@@ -1118,16 +1130,36 @@ poisson_rows_fwd_split(const R *__restrict__ q, typename Cplx<R>::T *__restrict_
     }
 }
 
+// dynamic shared memory of the slab kernel: the FFT64 and z twiddles, the
+// output twiddles, the slab and the z-transform buffers of the 8 warps
+template <typename R, int L>
+constexpr size_t slab_smem() {
+    constexpr int TPW = 32 / fft::WPlan<L>::G;
+    return sizeof(typename Cplx<R>::T) * ((size_t)128 + L + (size_t)slab_rows<L>() * tstride<64>() +
+                                          (size_t)8 * TPW * tstride<L>());
+}
+// two resident blocks per SM where their shared memory allows, which caps
+// the registers at 128 a thread; one block (and up to 255 registers) otherwise
+// and for the FP64 transforms longer than 64, which spill under that cap
+template <typename R, int L>
+constexpr int slab_min_blocks() {
+    return 2 * slab_smem<R, L>() + 4096 <= 227 * 1024 && (sizeof(R) == 4 || L == 64) ? 2 : 1;
+}
+
 // K2 of the split path, one block per (kx, j): the slab a_j[z - 1][n] of all
 // interior planes in shared memory; FFT64 along n (ky = S k' + j), the
 // sine-transform z solve of each of the 64 modes (as poisson_zdst: odd
-// extension of length L = 2 (NZ - 1), FFT, division by lambda_k + h dz^2,
-// FFT), inverse FFT64, the twiddle W_NY^(-j n), written back in place as b_j.
-// The block (kx, j) = (0, 0) also forms the FP64 plane sums of the source and
-// solves the (0,0) mode in closed form (as poisson_zdst), writing phi00 and
-// its Ez.
+// extension of length L = 2 (NZ - 1), forward FFT, division by
+// lambda_k + h dz^2, forward FFT), inverse FFT64, the twiddle W_NY^(-j n),
+// written back in place as b_j.  Every transform is warp-synchronous (fft::WPlan): the rows n of a plane are
+// transformed on their way in from global memory and on their way out, the
+// odd extension is gathered from the slab's column by the first pass and the
+// division applied by the last, so the block synchronises only between the
+// three phases.  The block (kx, j) = (0, 0) also forms the FP64 plane sums of
+// the source and solves the (0,0) mode in closed form (as poisson_zdst),
+// writing phi00 and its Ez.
 template <typename R, int L, int S>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, slab_min_blocks<R, L>())
 poisson_slab(typename Cplx<R>::T *__restrict__ spl, const typename Cplx<R>::T *__restrict__ twy,
              const typename Cplx<R>::T *__restrict__ twz, const R *__restrict__ lamz,
              const double *__restrict__ rowsum, double *__restrict__ planesum,
@@ -1147,35 +1179,32 @@ poisson_slab(typename Cplx<R>::T *__restrict__ spl, const typename Cplx<R>::T *_
     using R2 = typename Cplx<R>::T;
     constexpr int NY = 64 * S;
     constexpr int n = L / 2 - 1, nz = n + 2;
-    constexpr int G64 = fft::Plan<64>::G, T64 = 256 / G64, P64 = tstride<64>();
-    constexpr int NR = (n + T64 - 1) / T64 * T64;  // slab rows, whole FFT rounds
-    constexpr int GL = fft::Plan<L>::G, TBZ = 256 / GL, PL = tstride<L>();
+    constexpr int P64 = tstride<64>(), PL = tstride<L>();
+    constexpr int NR = slab_rows<L>();     // slab rows, whole rounds of 32
+    constexpr int GZ = fft::WPlan<L>::G;   // threads per z transform
+    constexpr int TPW = 32 / GZ;           // z transforms per warp
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R2 *tw64 = reinterpret_cast<R2 *>(smem_raw);
-    R2 *twl = tw64 + 64;
+    R2 *twj = tw64 + 64;  // conj W_NY^(j n), n < 64
+    R2 *twl = twj + 64;
     R2 *slab = twl + L;
     R2 *zb = slab + NR * P64;
     __shared__ double mrhs[n], mphi[nz];
-    __shared__ R hdz2[TBZ];
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int kx = blockIdx.x, j = blockIdx.y;
     const bool mean_block = kx == 0 && j == 0;
     const double dz2 = dz * dz;
     R2 *base = spl + ((size_t)j * nxh + kx) * n * 64;
-    for (int i = tid; i < 64; i += 256) tw64[i] = twy[S * i];
+    for (int i = tid; i < 64; i += 256) {
+        tw64[i] = twy[S * i];
+        R2 w = twy[(j * i) % NY];
+        w.y = -w.y;
+        twj[i] = w;
+    }
     for (int i = tid; i < L; i += 256) twl[i] = twz[i];
-    for (int i = tid; i < n * 64; i += 256) {
-        const int zi = i >> 6, nn = i & 63;
-        slab[zi * P64 + fft::pad(nn)] = base[i];
-    }
-    for (int i = n * 64 + tid; i < NR * 64; i += 256) {
-        const int zi = i >> 6, nn = i & 63;
-        slab[zi * P64 + fft::pad(nn)] = R2{(R)0, (R)0};
-    }
     if (mean_block) {
         // FP64 plane sums of the source (fixed order), then the right-hand
         // side of the mean mode (poisson.cu:97 for the voltage on z = 1)
-        const int warp = tid >> 5, lane = tid & 31;
         const double nxy = (double)nx * (double)NY;
         for (int zi = warp; zi < n; zi += 8) {
             double sum = 0.0;
@@ -1191,76 +1220,70 @@ poisson_slab(typename Cplx<R>::T *__restrict__ spl, const typename Cplx<R>::T *_
         }
     }
     __syncthreads();
-    {
-        const int tr = tid / G64, jj = tid - tr * G64;
-        for (int r0 = 0; r0 < NR; r0 += T64)
-            fft::Plan<64>::template run<-1>(slab + (r0 + tr) * P64, tw64, jj);
+    // phase 1: forward FFT64 of each plane's row on its way in, 4 rows a warp
+    const int g8 = lane >> 3, t8 = lane & 7;
+#pragma unroll 1
+    for (int zi = warp * 4 + g8; zi < NR; zi += 32) {
+        const bool act = zi < n;
+        const R2 *src = base + (size_t)zi * 64;
+        R2 *row = slab + zi * P64;
+        fft::WPlan<64>::template run<-1>(
+            row, tw64, opaque(t8), [&](int m) { return act ? src[m] : R2{(R)0, (R)0}; },
+            [&](int m, R2 v) { row[fft::pad(m)] = v; });
     }
-    // z solve of the modes k' = b0 .. b0 + TBZ - 1
-    constexpr int YS = 256 / TBZ, IT = (n + YS - 1) / YS;
-    const R sc = (R)(dz2 / (double)L);
-    for (int b0 = 0; b0 < 64; b0 += TBZ) {
-        const int t = tid % TBZ, zt = tid / TBZ;
-        const int kp = b0 + t;
-        if (zt == 0) {
+    __syncthreads();
+    // phase 2: z solve of the modes k', TPW per warp
+    {
+        const R sc = (R)(dz2 / (double)L);
+        const int g = lane / GZ, t0 = lane - g * GZ;
+        R2 *zw = zb + (warp * TPW + g) * PL;
+#pragma unroll 1
+        for (int kp = warp * TPW + g; kp < 64; kp += 8 * TPW) {
+            const int t = opaque(t0);
             const int ky = S * kp + j;
             const double wx = kx * kx0, wy = (ky <= NY / 2 ? ky : ky - NY) * ky0;
-            hdz2[t] = (kx == 0 && ky == 0) ? (R)-1 : (R)((wx * wx + wy * wy) * dz2);
-        }
-#pragma unroll
-        for (int r = 0; r < IT; ++r) {
-            const int zi = zt + YS * r;
-            if (zi < n) {
-                const R2 v = slab[zi * P64 + fft::pad(kp)];
-                zb[t * PL + fft::pad(zi + 1)] = v;
-                zb[t * PL + fft::pad(L - 1 - zi)] = R2{-v.x, -v.y};
-            }
-        }
-        if (tid < TBZ) {
-            zb[tid * PL + fft::pad(0)] = R2{(R)0, (R)0};
-            zb[tid * PL + fft::pad(L / 2)] = R2{(R)0, (R)0};
-        }
-        __syncthreads();
-        const int tr = tid / GL, jj = tid - tr * GL;
-        fft::Plan<L>::template run<-1>(zb + tr * PL, twl, jj);
-#pragma unroll
-        for (int u = 0; u < L / GL; ++u) {
-            const int k = jj + GL * u;
-            R2 &yv = zb[tr * PL + fft::pad(k)];
-            const R h = hdz2[tr];
-            if (k == 0 || k == L / 2 || h < (R)0) {
-                yv = R2{(R)0, (R)0};
-            } else {
+            const R h = (kx == 0 && ky == 0) ? (R)-1 : (R)((wx * wx + wy * wy) * dz2);
+            R2 *col = slab + fft::pad(kp);
+            // odd extension x[m] = s[m], x[L - m] = -s[m] (m = 1..n), x[0] = x[L/2] = 0
+            auto ld = [&](int m) {
+                const bool up = m < L / 2;
+                const R2 v = col[(up ? (m > 0 ? m - 1 : 0) : L - 1 - m) * P64];
+                return (m == 0 || m == L / 2) ? R2{(R)0, (R)0} : (up ? v : R2{-v.x, -v.y});
+            };
+            auto div = [&](int k, R2 v) {
+                if (k == 0 || k == L / 2 || h < (R)0) return R2{(R)0, (R)0};
                 const R f = rcp(lamz[k < L / 2 ? k : L - k] + h);
-                yv = R2{yv.x * f, yv.y * f};
+                return R2{v.x * f, v.y * f};
+            };
+            auto st = [&](int m, R2 v) {
+                if (m >= 1 && m <= n) col[(m - 1) * P64] = R2{v.x * sc, v.y * sc};
+            };
+            // both transforms forward, as poisson_zdst: the sign of the
+            // solution follows from the two factors -2i of the odd extension
+            if constexpr (L == 64 || L == 256) {
+                fft::wfilter_sq<L, GZ, -1, -1>(zw, twl, t, ld, div, st);
+            } else {
+                fft::WPlan<L>::template run<-1>(zw, twl, t, ld,
+                                                [&](int k, R2 v) { zw[fft::pad(k)] = div(k, v); });
+                __syncwarp();
+                fft::WPlan<L>::template run<-1>(zw, twl, opaque(t0),
+                                                [&](int m) { return zw[fft::pad(m)]; }, st);
+                __syncwarp();
             }
         }
-        __syncthreads();
-        fft::Plan<L>::template run<-1>(zb + tr * PL, twl, jj);
-#pragma unroll
-        for (int r = 0; r < IT; ++r) {
-            const int zi = zt + YS * r;
-            if (zi < n) {
-                const R2 w = zb[t * PL + fft::pad(zi + 1)];
-                slab[zi * P64 + fft::pad(kp)] = R2{w.x * sc, w.y * sc};
-            }
-        }
-        __syncthreads();
     }
-    {
-        const int tr = tid / G64, jj = tid - tr * G64;
-        for (int r0 = 0; r0 < NR; r0 += T64)
-            fft::Plan<64>::template run<1>(slab + (r0 + tr) * P64, tw64, jj);
-    }
-    for (int i = tid; i < n * 64; i += 256) {
-        const int zi = i >> 6, nn = i & 63;
-        R2 v = slab[zi * P64 + fft::pad(nn)];
-        if (j * nn != 0) {
-            R2 w = __ldg(twy + (j * nn) % NY);
-            w.y = -w.y;
-            v = cmul(v, w);
-        }
-        base[i] = v;
+    __syncthreads();
+    // phase 3: inverse FFT64 of each row and the twiddle on the way out
+#pragma unroll 1
+    for (int zi = warp * 4 + g8; zi < NR; zi += 32) {
+        const bool act = zi < n;
+        R2 *dst = base + (size_t)zi * 64;
+        R2 *row = slab + zi * P64;
+        fft::WPlan<64>::template run<1>(
+            row, tw64, opaque(t8), [&](int m) { return row[fft::pad(m)]; },
+            [&](int m, R2 v) {
+                if (act) dst[m] = j * m != 0 ? cmul(v, twj[m]) : v;
+            });
     }
     if (mean_block) {
         const double nxy = (double)nx * (double)NY;
@@ -1382,7 +1405,11 @@ static cudaError_t set_smem(K kern, size_t bytes, cudaStream_t s) {
     return allow_max_dynamic_smem(kern);
 }
 
-bool poisson_fast_size(int n) { return n == 64 || n == 128 || n == 256 || n == 512; }
+bool poisson_fast_size(int n) {
+    return n == 48 || n == 64 || n == 80 || n == 96 || n == 128 || n == 256 || n == 512;
+}
+// the sizes of the split-y path's x rows and z transforms
+static bool split_size(int n) { return n == 64 || n == 128 || n == 256 || n == 512; }
 
 size_t zdst_rt_smem(int L, int tb, size_t rsize) {
     const int n = L / 2 - 1, nz = n + 2;
@@ -1432,7 +1459,10 @@ template <typename R>
 static cudaError_t rows_fwd(const PoissonArgs &a, cudaStream_t s) {
     using R2 = typename Cplx<R>::T;
     switch (a.nx) {
+        case 48: return rows_fwd_fast<R, 48>(a, s);
         case 64: return rows_fwd_fast<R, 64>(a, s);
+        case 80: return rows_fwd_fast<R, 80>(a, s);
+        case 96: return rows_fwd_fast<R, 96>(a, s);
         case 128: return rows_fwd_fast<R, 128>(a, s);
         case 256: return rows_fwd_fast<R, 256>(a, s);
         case 512: return rows_fwd_fast<R, 512>(a, s);
@@ -1452,7 +1482,10 @@ template <typename R>
 static cudaError_t rows_inv(const PoissonArgs &a, cudaStream_t s) {
     using R2 = typename Cplx<R>::T;
     switch (a.nx) {
+        case 48: return rows_inv_fast<R, 48>(a, s);
         case 64: return rows_inv_fast<R, 64>(a, s);
+        case 80: return rows_inv_fast<R, 80>(a, s);
+        case 96: return rows_inv_fast<R, 96>(a, s);
         case 128: return rows_inv_fast<R, 128>(a, s);
         case 256: return rows_inv_fast<R, 256>(a, s);
         case 512: return rows_inv_fast<R, 512>(a, s);
@@ -1472,7 +1505,10 @@ template <typename R, int S>
 static cudaError_t cols(const PoissonArgs &a, cudaStream_t s) {
     using R2 = typename Cplx<R>::T;
     switch (a.ny) {
+        case 48: return cols_fast<R, 48, S>(a, s);
         case 64: return cols_fast<R, 64, S>(a, s);
+        case 80: return cols_fast<R, 80, S>(a, s);
+        case 96: return cols_fast<R, 96, S>(a, s);
         case 128: return cols_fast<R, 128, S>(a, s);
         case 256: return cols_fast<R, 256, S>(a, s);
         case 512: return cols_fast<R, 512, S>(a, s);
@@ -1506,15 +1542,6 @@ static cudaError_t zdst(const PoissonArgs &a, cudaStream_t s) {
 
 // ---- split-y path ----
 
-template <typename R, int L, int S>
-constexpr size_t slab_smem() {
-    constexpr int n = L / 2 - 1;
-    constexpr int T64 = 256 / fft::Plan<64>::G;
-    constexpr int NR = (n + T64 - 1) / T64 * T64;
-    constexpr int TBZ = 256 / fft::Plan<L>::G;
-    return sizeof(typename Cplx<R>::T) *
-           ((size_t)64 + L + (size_t)NR * tstride<64>() + (size_t)TBZ * tstride<L>());
-}
 template <typename R, int N, int S>
 constexpr size_t rows_inv_split_smem() {
     constexpr int TB = per_block<N>();
@@ -1547,7 +1574,7 @@ static cudaError_t split_rows_inv(const PoissonArgs &a, cudaStream_t s) {
 template <typename R, int L, int S>
 static cudaError_t split_slab(const PoissonArgs &a, cudaStream_t s) {
     using R2 = typename Cplx<R>::T;
-    constexpr size_t sm = slab_smem<R, L, S>();
+    constexpr size_t sm = slab_smem<R, L>();
     cudaError_t e = set_smem(poisson_slab<R, L, S>, sm, s);
     if (e != cudaSuccess) return e;
     const R2 *tw = (const R2 *)a.twz;
@@ -1584,10 +1611,10 @@ static cudaError_t split_all(const PoissonArgs &a, cudaStream_t s) {
 template <typename R, int S>
 static size_t split_slab_smem(int L) {
     switch (L) {
-        case 64: return slab_smem<R, 64, S>();
-        case 128: return slab_smem<R, 128, S>();
-        case 256: return slab_smem<R, 256, S>();
-        default: return slab_smem<R, 512, S>();
+        case 64: return slab_smem<R, 64>();
+        case 128: return slab_smem<R, 128>();
+        case 256: return slab_smem<R, 256>();
+        default: return slab_smem<R, 512>();
     }
 }
 
@@ -1596,7 +1623,7 @@ static size_t split_slab_smem(int L) {
 // shared memory
 template <typename R>
 bool poisson_split_usable(const PoissonArgs &a) {
-    if (!poisson_fast_size(a.nx) || !a.twz || !poisson_fast_size(2 * (a.nz - 1))) return false;
+    if (!split_size(a.nx) || !a.twz || !split_size(2 * (a.nz - 1))) return false;
     const int S = a.ny / 64;
     if (a.ny % 64 != 0 || (S != 1 && S != 2 && S != 4 && S != 8)) return false;
     const int L = 2 * (a.nz - 1);
@@ -1637,9 +1664,42 @@ static cudaError_t prepare_split_s(int nx, int L) {
         default: return prepare_split_ns<R, 512, S>(L);
     }
 }
+template <typename R, int N>
+static cudaError_t prepare_fast_n() {
+    cudaError_t e = allow_max_dynamic_smem(poisson_rows_fwd_fast<R, N>);
+    if (e == cudaSuccess) e = allow_max_dynamic_smem(poisson_rows_inv_fast<R, N>);
+    if (e == cudaSuccess) e = allow_max_dynamic_smem(poisson_cols_fast<R, N, -1>);
+    if (e == cudaSuccess) e = allow_max_dynamic_smem(poisson_cols_fast<R, N, 1>);
+    if (e == cudaSuccess) e = allow_max_dynamic_smem(poisson_zdst<R, N>);
+    return e;
+}
+template <typename R>
+static cudaError_t prepare_fast(int n) {
+    switch (n) {
+        case 48: return prepare_fast_n<R, 48>();
+        case 64: return prepare_fast_n<R, 64>();
+        case 80: return prepare_fast_n<R, 80>();
+        case 96: return prepare_fast_n<R, 96>();
+        case 128: return prepare_fast_n<R, 128>();
+        case 256: return prepare_fast_n<R, 256>();
+        case 512: return prepare_fast_n<R, 512>();
+        default: return cudaSuccess;
+    }
+}
+// Every Poisson kernel that a context of this grid can launch, under any
+// tuning, may use the device's whole opt-in shared memory: the attribute
+// cannot be set by a launch inside a stream capture (set_smem), and the
+// batch graphs capture every launch.
 template <typename R>
 cudaError_t prepare_poisson(const PoissonArgs &a) {
-    if (!poisson_split_usable<R>(a)) return cudaSuccess;
+    cudaError_t e = allow_max_dynamic_smem(poisson_rows_fwd<R>);
+    if (e == cudaSuccess) e = allow_max_dynamic_smem(poisson_rows_inv<R>);
+    if (e == cudaSuccess) e = allow_max_dynamic_smem(poisson_cols<R>);
+    if (e == cudaSuccess) e = allow_max_dynamic_smem(poisson_zdst_rt<R>);
+    if (e == cudaSuccess) e = prepare_fast<R>(a.nx);
+    if (e == cudaSuccess) e = prepare_fast<R>(a.ny);
+    if (e == cudaSuccess) e = prepare_fast<R>(2 * (a.nz - 1));
+    if (e != cudaSuccess || !poisson_split_usable<R>(a)) return e;
     const int L = 2 * (a.nz - 1);
     switch (a.ny / 64) {
         case 1: return prepare_split_s<R, 1>(a.nx, L);
@@ -1667,7 +1727,10 @@ cudaError_t launch_poisson(const PoissonArgs &a, cudaStream_t s) {
     if ((e = cols<R, -1>(a, s)) != cudaSuccess) return e;
     if (a.twz && poisson_fast_size(2 * (a.nz - 1))) {
         switch (2 * (a.nz - 1)) {
+            case 48: e = zdst<R, 48>(a, s); break;
             case 64: e = zdst<R, 64>(a, s); break;
+            case 80: e = zdst<R, 80>(a, s); break;
+            case 96: e = zdst<R, 96>(a, s); break;
             case 128: e = zdst<R, 128>(a, s); break;
             case 256: e = zdst<R, 256>(a, s); break;
             default: e = zdst<R, 512>(a, s); break;

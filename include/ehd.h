@@ -277,10 +277,10 @@ int ehd_batch_set_active(ehd_batch *batch, int i, int active);
  * each instance's result is bitwise that of a lone context.  mode 0: instances
  * with the same grid and launch shapes form a group, and each kernel of the
  * step is one launch over every instance of a group (the LBM half on the
- * per-node kernel), one graph per step holding the groups' launches; an
- * instance's result agrees with a lone context on the per-node kernel to FP32
- * round-off (the grouped kernels are separate compilations, whose
- * multiply-add contractions may differ). */
+ * persistent row kernel or the per-node kernel, as the instances' tuning
+ * says), one graph per step holding the groups' launches; an instance's
+ * result agrees with a lone context to FP32 round-off (the grouped kernels
+ * are separate compilations, whose multiply-add contractions may differ). */
 int ehd_batch_set_mode(ehd_batch *batch, int mode);
 /* nsteps steps of every active instance.  Instances whose next step is the
  * first after an upload take that step on their own streams; after it, one

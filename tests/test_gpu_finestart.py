@@ -25,8 +25,9 @@ def test_fine_grid_warm_start_runs_and_stays_close_to_fp32(tmp_path):
     import torch
     net = fno.FNO(16, 16, 9, 9, 5, width=8, layers=2, modes=(4, 4, 4), hidden=16, max_batch=1,
                   seed=3)
-    # outputs near a mid-gap charge and potential: a smooth, finite start
-    mean = np.array([0.0, 0.0, 0.0, 0.5, 0.5])
+    # outputs near zero velocity and near zero change of q and phi: the start's
+    # column carried over, a smooth, finite start
+    mean = np.array([0.0, 0.0, 0.0, 0.0, 0.0])
     std = np.array([1e-4, 1e-4, 1e-4, 1e-3, 1e-3])
     path = tmp_path / "net.npz"
     F.save_net(path, net, mean, std)
@@ -41,7 +42,11 @@ def test_fine_grid_warm_start_runs_and_stays_close_to_fp32(tmp_path):
     cp, pred = F.predict(ehd, net2, m2, s2, group, (16, 16, 9))
     net2.close()
     assert pred["q"].shape == (9, 16, 16)
-    assert np.allclose(pred["q"], 0.5 * cp.charge0, rtol=2e-2)
+    q = pred["q"]
+    assert np.all(np.isfinite(q)) and q.min() > -1e-2 * cp.charge0
+    # each plane is the column's value plus a change of order std
+    assert np.all(np.abs(q - q.mean(axis=(1, 2), keepdims=True)) < 1e-2 * cp.charge0)
+    assert np.ptp(q.mean(axis=(1, 2))) > 0.1 * cp.charge0
     res = F.compare(ehd, cp, pred, group, tiles=2, factor=2, steps=40, sample=20,
                     warm_precision="fp16")
     assert res["fine_grid"] == [64, 64, 17] and res["fine_lx"] == pytest.approx(2 * cp.lx)

@@ -164,11 +164,12 @@ def test_step_halves_match_oracle(shape):
 
 @pytest.mark.parametrize("shape", [(256, 128, 9), (128, 256, 7), (512, 64, 5), (64, 512, 5),
                                    (256, 96, 6), (122, 122, 7), (14, 77, 5), (61, 26, 6),
-                                   (127, 13, 5)])
+                                   (127, 13, 5), (96, 96, 49), (80, 48, 41), (48, 80, 25)])
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-11), ("fp32", 2e-6)])
 def test_poisson_fft_sizes_match_oracle(shape, prec, tol):
-    """The compile-time-radix FFT paths (N = 64..512, two real rows per
-    transform) and the run-time radix path (radix 2/3/4/5 and the direct
+    """The compile-time-radix FFT paths (N = 48, 64, 80, 96, 128, 256, 512, two
+    real rows per transform; the z sine transforms of length 48, 80, 96 on the
+    T-sweep grids) and the run-time radix path (radix 2/3/4/5 and the direct
     radix-p passes for other primes: 122 = 2 x 61, the reference's own grid
     width, LBM.h:34-35; 77 = 7 x 11; prime and odd widths), against the
     oracle's odd-extension DFT solve (poisson.cu:78-167) on random charge."""
@@ -221,7 +222,7 @@ def test_poisson_split_path_matches_oracle_and_five_kernel_path(shape, prec, tol
         assert relerr(out[0][k], out[1][k]) < tol, (k, "five-kernel", relerr(out[0][k], out[1][k]))
 
 
-@pytest.mark.parametrize("shape", [(48, 40, 25), (122, 122, 101), (30, 25, 7)])
+@pytest.mark.parametrize("shape", [(48, 40, 27), (122, 122, 101), (30, 25, 7)])
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("fp32", 2e-6)])
 def test_z_solve_choices_match_oracle(shape, prec, tol):
     """Where 2 (NZ - 1) is not a compile-time FFT size, the z solve is the sine
@@ -326,10 +327,12 @@ def test_diagnostics_match_host_reductions(prec):
         sim.set_fields(f)
         sim.step(30)
         d = sim.diagnostics()
+        cur = sim.current()  # the collector plane alone, another summation order
         fl = sim.get_fields()
     dv = p.dx * p.dy * p.dz
     rtol = 1e-12 if prec == "fp64" else 1e-6
     assert d["current"] == pytest.approx(O.current_of(p, fl["q"], fl["ez"]), rel=rtol)
+    assert cur == pytest.approx(d["current"], rel=1e-13)
     ke = 0.5 * np.sum(fl["rho"] * (fl["u"] ** 2 + fl["v"] ** 2 + fl["w"] ** 2)) * dv
     assert d["kinetic_energy"] == pytest.approx(ke, rel=rtol)
     assert d["total_charge"] == pytest.approx(np.sum(fl["q"]) * dv, rel=rtol)
