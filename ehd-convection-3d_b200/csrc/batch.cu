@@ -6,8 +6,10 @@
 // grid and launch shape, nThreads in LBM.h).  Each instance is a complete
 // context (csrc/api.cu) with its own stream; a batch step is captured once per
 // (active set, buffer parities, macro output) as a fork on the batch stream,
-// one branch per instance with that instance's step launches on its own
-// stream, and a join, so the instances' kernels run side by side.
+// parallel branches and a join, so that independent kernels run side by side.
+// Mode 1 has one branch per instance with that instance's own step launches
+// on its stream; mode 0 one branch per group of instances with the same grid
+// and launch shapes, each kernel of the step one launch over the group.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -84,6 +86,7 @@ int upload(const X *host, size_t n, std::vector<void *> &bufs, X **dev) {
 // device descriptors of its launches.
 struct Group {
     int nx = 0, ny = 0, nz = 0, n = 0, bx = 0;
+    size_t first = 0;  // the member whose stream carries the group's branch
     int rows = 0;  // > 0: the row kernel on this many CTAs per instance
     void *lbm = nullptr;
     ReduceDesc *red = nullptr;
@@ -120,6 +123,7 @@ int build_group(ehd_batch *b, const std::vector<size_t> &members, bool macros,
     g->ny = p->ny;
     g->nz = p->nz;
     g->n = n;
+    g->first = members[0];
     g->bx = la[0].node_bx;
     // the instances' persistent row-kernel CTAs shared among the group
     g->rows = la[0].rows_grid > 0 ? std::max(1, la[0].rows_grid / n) : 0;
@@ -151,18 +155,24 @@ int capture_groups(ehd_batch *b, const std::vector<char> &act, bool macros,
         if (r != EHD_OK) return r;
         gl.push_back(g);
     }
+    // one branch per group (on the stream of its first member), so that the
+    // groups' kernels overlap: a fork on the batch stream, each group's LBM
+    // half, reduction and Poisson solve in order on its branch, a join
     cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_fail("batch capture", e);
-    for (const Group &g : gl)
+    e = cudaEventRecord(b->fork, b->stream);
+    for (const Group &g : gl) {
+        if (e != cudaSuccess) break;
+        cudaStream_t gs = ctx_stream(b->inst[g.first]);
+        e = cudaStreamWaitEvent(gs, b->fork, 0);
         if (e == cudaSuccess)
-            e = g.rows > 0 ? launch_lbm_rows_group<T, R>(g.lbm, g.n, g.nx, g.ny, g.rows, macros,
-                                                         b->stream)
-                           : launch_lbm_group<T, R>(g.lbm, g.n, g.nx, g.ny, g.nz, g.bx, macros,
-                                                    b->stream);
-    for (const Group &g : gl)
-        if (e == cudaSuccess) e = launch_reduce_tables_group<R>(g.red, g.n, g.nz, b->stream);
-    for (const Group &g : gl)
-        if (e == cudaSuccess) e = launch_poisson<R>(g.pa, b->stream);
+            e = g.rows > 0 ? launch_lbm_rows_group<T, R>(g.lbm, g.n, g.nx, g.ny, g.rows, macros, gs)
+                           : launch_lbm_group<T, R>(g.lbm, g.n, g.nx, g.ny, g.nz, g.bx, macros, gs);
+        if (e == cudaSuccess) e = launch_reduce_tables_group<R>(g.red, g.n, g.nz, gs);
+        if (e == cudaSuccess) e = launch_poisson<R>(g.pa, gs);
+        if (e == cudaSuccess) e = cudaEventRecord(b->join[g.first], gs);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->join[g.first], 0);
+    }
     cudaGraph_t gr = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(b->stream, &gr);
     if (e != cudaSuccess || e2 != cudaSuccess) {

@@ -284,6 +284,7 @@ __device__ __forceinline__ void wfilter_sq(R2 *buf, const R2 *tw, int t, Ld ld, 
     R2 v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = ld(t + R * r);
+    __syncwarp();  // ld may read buf
     Dft<R, S1, R2>::run(v, tw, R);
     pass_store<N, R, 1>(buf, t, v);
     __syncwarp();
@@ -325,6 +326,31 @@ template <> struct WPlan<256> {
         wpass_last<256, 16, 16, G, S>(b, tw, t, st);
     }
 };
+template <> struct WPlan<48> {
+    static constexpr int G = 16;
+    template <int S, typename R2, typename Ld, typename St>
+    __device__ static void run(R2 *b, const R2 *tw, int t, Ld ld, St st) {
+        wpass_first<48, 16, G, S>(b, tw, t, ld);
+        wpass_last<48, 3, 16, G, S>(b, tw, t, st);
+    }
+};
+template <> struct WPlan<80> {
+    static constexpr int G = 16;
+    template <int S, typename R2, typename Ld, typename St>
+    __device__ static void run(R2 *b, const R2 *tw, int t, Ld ld, St st) {
+        wpass_first<80, 16, G, S>(b, tw, t, ld);
+        wpass_last<80, 5, 16, G, S>(b, tw, t, st);
+    }
+};
+template <> struct WPlan<96> {
+    static constexpr int G = 32;
+    template <int S, typename R2, typename Ld, typename St>
+    __device__ static void run(R2 *b, const R2 *tw, int t, Ld ld, St st) {
+        wpass_first<96, 8, G, S>(b, tw, t, ld);
+        wpass<96, 4, 8, G, S>(b, tw, t);
+        wpass_last<96, 3, 32, G, S>(b, tw, t, st);
+    }
+};
 template <> struct WPlan<512> {
     static constexpr int G = 32;
     template <int S, typename R2, typename Ld, typename St>
@@ -334,6 +360,20 @@ template <> struct WPlan<512> {
         wpass_last<512, 8, 64, G, S>(b, tw, t, st);
     }
 };
+
+// In-place transform of one row of a tile (padded, length N) by its G
+// threads, ending with a block barrier as Plan<N>::run does: warp-synchronous
+// where the warp plan has the block plan's G, block-wide otherwise (N = 512).
+template <int N, int S, typename R2>
+__device__ __forceinline__ void run_tile(R2 *b, const R2 *tw, int j) {
+    if constexpr (WPlan<N>::G == Plan<N>::G) {
+        WPlan<N>::template run<S>(
+            b, tw, j, [&](int m) { return b[pad(m)]; }, [&](int m, R2 v) { b[pad(m)] = v; });
+        __syncthreads();
+    } else {
+        Plan<N>::template run<S>(b, tw, j);
+    }
+}
 
 }  // namespace fft
 }  // namespace ehd

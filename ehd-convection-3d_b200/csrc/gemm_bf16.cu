@@ -414,17 +414,29 @@ __global__ void __launch_bounds__(256) leftmul_kernel(const GemmArgs a, int pair
     const float *B = reinterpret_cast<const float *>(a.B);
     const int chunks = (a.N + NC - 1) / NC;
     const long long units = (long long)a.batch * chunks;
-    for (long long u = (long long)blockIdx.x * 8 + warp; u < units; u += (long long)gridDim.x * 8) {
+    const long long ustep = (long long)gridDim.x * 8;
+    // the B offsets of unit u's columns
+    auto unit_cols = [&](long long u, int (&bno)[NT], unsigned &nmask) {
         const int bidx = (int)(u / chunks), n0 = (int)(u - (long long)bidx * chunks) * NC;
         const int boff = at_off<int>(a.bbat, bidx);
-        int bno[NT];
-        unsigned nmask = 0;
+        nmask = 0;
 #pragma unroll
         for (int j = 0; j < NT; ++j) {
             const int n = n0 + 8 * j + gq;
             bno[j] = boff + (n < a.N ? at_off<int>(a.bn, n) : 0);
             nmask |= (n < a.N ? 1u : 0u) << j;
         }
+    };
+    int bno[NT];
+    unsigned nmask = 0;
+    float rb[NT][4];
+    long long u = (long long)blockIdx.x * 8 + warp;
+    if (u < units) {
+        unit_cols(u, bno, nmask);
+        lm_load<NT>(rb, B, bno, nmask, a.bk, a.K, 0, tq);
+    }
+    for (; u < units; u += ustep) {
+        const int bidx = (int)(u / chunks), n0 = (int)(u - (long long)bidx * chunks) * NC;
         float acc[MT][NT][4];
 #pragma unroll
         for (int i = 0; i < MT; ++i)
@@ -432,8 +444,6 @@ __global__ void __launch_bounds__(256) leftmul_kernel(const GemmArgs a, int pair
             for (int j = 0; j < NT; ++j)
 #pragma unroll
                 for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
-        float rb[NT][4];
-        lm_load<NT>(rb, B, bno, nmask, a.bk, a.K, 0, tq);
         for (int s = 0; s < kt; ++s) {
             uint32_t bf[NT][2];
 #pragma unroll
@@ -441,7 +451,14 @@ __global__ void __launch_bounds__(256) leftmul_kernel(const GemmArgs a, int pair
                 bf[j][0] = pack_bf16(make_float2(rb[j][0], rb[j][1]));
                 bf[j][1] = pack_bf16(make_float2(rb[j][2], rb[j][3]));
             }
-            if (s + 1 < kt) lm_load<NT>(rb, B, bno, nmask, a.bk, a.K, s + 1, tq);
+            // the next K step's fragments in flight during this step's
+            // products; after the last step, the next unit's first
+            if (s + 1 < kt) {
+                lm_load<NT>(rb, B, bno, nmask, a.bk, a.K, s + 1, tq);
+            } else if (u + ustep < units) {
+                unit_cols(u + ustep, bno, nmask);
+                lm_load<NT>(rb, B, bno, nmask, a.bk, a.K, 0, tq);
+            }
 #pragma unroll
             for (int i = 0; i < MT; ++i) {
                 const __nv_bfloat16 *ap = As + (16 * i + gq) * KP + 16 * s + 2 * tq;

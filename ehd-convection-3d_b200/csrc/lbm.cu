@@ -664,7 +664,7 @@ __device__ __forceinline__ int ez_rt(int d) { return (int)((kEzPack >> (2 * d)) 
 // rows_run is the loop of CTA blk of nblk; lbm_rows_kernel runs one instance,
 // lbm_rows_group_kernel several instances of the same NX (blockIdx.y) with
 // their arguments from a device table.
-template <typename T, typename R, bool MACROS>
+template <typename T, typename R, bool MACROS, bool PART>
 __device__ __forceinline__ void rows_run(const StepArgs<T, R> &a, const KConst<R> &c, int blk,
                                          int nblk) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -680,9 +680,13 @@ __device__ __forceinline__ void rows_run(const StepArgs<T, R> &a, const KConst<R
         return reinterpret_cast<G *>(smem_raw + (size_t)st * stage_bytes + (size_t)Q * NX * sizeof(F));
     };
     const unsigned row_bytes_f = (unsigned)(NX * sizeof(F)), row_bytes_g = (unsigned)(NX * sizeof(G));
-    const int x = threadIdx.x;
+    // blockDim.x = NX rounded up to whole warps: with PART (NX not a multiple
+    // of 32), lanes past the row work on its last node (so that the whole warp
+    // takes part in the plane sums) and store nothing
+    const bool inside = !PART || (int)threadIdx.x < NX;
+    const int x = inside ? (int)threadIdx.x : NX - 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned nw = (unsigned)(NX / 32);
+    const unsigned nw = blockDim.x / 32u;
 
     if (threadIdx.x == 0) {
         mbar_init(&bar[0], 1);
@@ -769,9 +773,9 @@ __device__ __forceinline__ void rows_run(const StepArgs<T, R> &a, const KConst<R
             }
         }
         const Moments<R> mo = moments(f, h, zr);
-        warp_plane_sum((float)mo.rho, (float)mo.charge, a.psum,
+        warp_plane_sum(inside ? (float)mo.rho : 0.f, inside ? (float)mo.charge : 0.f, a.psum,
                        ((size_t)z * NY + y) * nw + warp);
-        finish_node<T, R, MACROS>(f, h, mo, x, y, z, node, zr, a, c, false, false);
+        if (inside) finish_node<T, R, MACROS>(f, h, mo, x, y, z, node, zr, a, c, false, false);
         // this warp is done with the stage; the last of the nw warps refills it
         __syncwarp();
         unsigned last = 0u;
@@ -793,10 +797,10 @@ __device__ __forceinline__ void rows_run(const StepArgs<T, R> &a, const KConst<R
     }
 }
 
-template <typename T, typename R, bool MACROS>
+template <typename T, typename R, bool MACROS, bool PART>
 __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 1 : 2)
 lbm_rows_kernel(const StepArgs<T, R> a, const KConst<R> c) {
-    rows_run<T, R, MACROS>(a, c, (int)blockIdx.x, (int)gridDim.x);
+    rows_run<T, R, MACROS, PART>(a, c, (int)blockIdx.x, (int)gridDim.x);
 }
 
 template <typename T, typename R>
@@ -818,13 +822,31 @@ __device__ __forceinline__ void load_group_desc(LbmGroupDesc<T, R> &sd,
     for (int i = threadIdx.x + blockDim.x * threadIdx.y; i < W; i += nt) dst[i] = src[i];
 }
 
-template <typename T, typename R, bool MACROS>
+template <typename T, typename R, bool MACROS, bool PART>
 __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 1 : 2)
 lbm_rows_group_kernel(const LbmGroupDesc<T, R> *__restrict__ desc) {
     __shared__ LbmGroupDesc<T, R> sd;
     load_group_desc(sd, desc, (int)blockIdx.y);
     __syncthreads();
-    rows_run<T, R, MACROS>(sd.a, sd.k, (int)blockIdx.x, (int)gridDim.x);
+    rows_run<T, R, MACROS, PART>(sd.a, sd.k, (int)blockIdx.x, (int)gridDim.x);
+}
+
+// the row kernels for (macro output, row ending inside a warp)
+template <typename T, typename R>
+using RowsKern = void (*)(const StepArgs<T, R>, const KConst<R>);
+template <typename T, typename R>
+RowsKern<T, R> rows_kernel(bool macros, bool part) {
+    return macros ? (part ? lbm_rows_kernel<T, R, true, true> : lbm_rows_kernel<T, R, true, false>)
+                  : (part ? lbm_rows_kernel<T, R, false, true> : lbm_rows_kernel<T, R, false, false>);
+}
+template <typename T, typename R>
+using RowsGroupKern = void (*)(const LbmGroupDesc<T, R> *);
+template <typename T, typename R>
+RowsGroupKern<T, R> rows_group_kernel(bool macros, bool part) {
+    return macros ? (part ? lbm_rows_group_kernel<T, R, true, true>
+                          : lbm_rows_group_kernel<T, R, true, false>)
+                  : (part ? lbm_rows_group_kernel<T, R, false, true>
+                          : lbm_rows_group_kernel<T, R, false, false>);
 }
 
 // Equilibrium populations from the FP64 fields (gpu_init_equilibrium,
@@ -937,6 +959,18 @@ __global__ void fields_to_compute_kernel(const double *const *out, R *rho, R *u,
 
 // ---- launchers ---------------------------------------------------------------
 
+// Block width of the per-node launch of the injector plane beside the row
+// kernel: whole warps along x, so that its plane sums land in the row
+// kernel's slots [y][x / 32] (the widest of 128, 96, 64 that divides NX, else
+// 32 with a partial last block).
+static int z0_block_x(int nx) {
+    for (int bx = 128; bx > 32; bx -= 32)
+        if (nx % bx == 0) return bx;
+    return 32;
+}
+// CTA width of the row kernel: NX rounded up to whole warps
+static int rows_block_x(int nx) { return (nx + 31) / 32 * 32; }
+
 size_t lbm_rows_smem(int nx, size_t fsize, size_t gsize) {
     return (size_t)2 * Q * nx * (fsize + gsize);
 }
@@ -946,7 +980,7 @@ size_t lbm_rows_smem(int nx, size_t fsize, size_t gsize) {
 // the mixed storage (2-byte f, 4-byte g) runs on it.  Rows are whole bulk
 // copies, so their bytes are multiples of 16.
 bool lbm_rows_usable(int nx, size_t fsize, size_t gsize) {
-    return gsize >= 4 && nx >= 32 && nx <= 256 && nx % 32 == 0 && (nx * fsize) % 16 == 0 &&
+    return gsize >= 4 && nx >= 32 && nx <= 256 && (nx * fsize) % 16 == 0 &&
            (nx * gsize) % 16 == 0 && lbm_rows_smem(nx, fsize, gsize) <= 220 * 1024;
 }
 
@@ -958,18 +992,19 @@ cudaError_t prepare_lbm_rows(int nx, int ny, int nz, int *grid) {
     if (!lbm_rows_usable(nx, sizeof(F), sizeof(G))) return cudaSuccess;
     const int sm = (int)lbm_rows_smem(nx, sizeof(F), sizeof(G));
     cudaError_t e;
-    if ((e = allow_max_dynamic_smem(lbm_rows_kernel<T, R, true>)) != cudaSuccess ||
-        (e = allow_max_dynamic_smem(lbm_rows_kernel<T, R, false>)) != cudaSuccess ||
-        (e = allow_max_dynamic_smem(lbm_rows_group_kernel<T, R, true>)) != cudaSuccess ||
-        (e = allow_max_dynamic_smem(lbm_rows_group_kernel<T, R, false>)) != cudaSuccess)
-        return e;
+    for (int v = 0; v < 4; ++v)
+        if ((e = allow_max_dynamic_smem(rows_kernel<T, R>(v & 1, v & 2))) != cudaSuccess ||
+            (e = allow_max_dynamic_smem(rows_group_kernel<T, R>(v & 1, v & 2))) != cudaSuccess)
+            return e;
+    const bool part = nx % 32 != 0;
     int dev = 0, nsm = 0, occ_a = 0, occ_b = 0;
+    const int tx = rows_block_x(nx);
     if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
         (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
-        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, lbm_rows_kernel<T, R, true>, nx,
-                                                           sm)) != cudaSuccess ||
-        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, lbm_rows_kernel<T, R, false>, nx,
-                                                           sm)) != cudaSuccess)
+        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, rows_kernel<T, R>(true, part),
+                                                           tx, sm)) != cudaSuccess ||
+        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, rows_kernel<T, R>(false, part),
+                                                           tx, sm)) != cudaSuccess)
         return e;
     const long long rows = (long long)ny * (nz - 1);
     *grid = (int)std::min<long long>(rows, (long long)nsm * std::min(occ_a, occ_b));
@@ -1049,22 +1084,19 @@ cudaError_t launch_lbm_group(const void *desc_dev, int n, int nx, int ny, int nz
 }
 
 // The steady-state step of a group on the row kernel: plane z = 0 of every
-// instance on the per-node kernel in blocks of whole warps along x (its plane
-// sums land in the row kernel's slots [y][x / 32]), then the planes z >= 1 on
+// instance on the per-node kernel (z0_block_x), then the planes z >= 1 on
 // per_inst CTAs of the row kernel per instance.
 template <typename T, typename R>
 cudaError_t launch_lbm_rows_group(const void *desc_dev, int n, int nx, int ny, int per_inst,
                                   bool macros, cudaStream_t s) {
     const auto *d = reinterpret_cast<const LbmGroupDesc<T, R> *>(desc_dev);
-    int bx = 128;
-    while (nx % bx != 0) bx -= 32;
-    const dim3 g0(nx / bx, ny, n);
+    const int bx = z0_block_x(nx);
+    const dim3 g0((nx + bx - 1) / bx, ny, n);
     if (macros) lbm_group_kernel<T, R, true><<<g0, bx, 0, s>>>(d, 1);
     else lbm_group_kernel<T, R, false><<<g0, bx, 0, s>>>(d, 1);
     const size_t sm = lbm_rows_smem(nx, sizeof(typename PopT<T>::F), sizeof(typename PopT<T>::G));
     const dim3 g1(per_inst, n, 1);
-    if (macros) lbm_rows_group_kernel<T, R, true><<<g1, nx, sm, s>>>(d);
-    else lbm_rows_group_kernel<T, R, false><<<g1, nx, sm, s>>>(d);
+    rows_group_kernel<T, R>(macros, nx % 32 != 0)<<<g1, rows_block_x(nx), sm, s>>>(d);
     return cudaGetLastError();
 }
 
@@ -1079,14 +1111,13 @@ cudaError_t launch_lbm_step(const LbmArgs &la, const StepConst &c, int local_pop
         // x so that its plane sums land in the row kernel's slots
         // [y][x / 32]; then the planes z >= 1 on the row kernel (its
         // shared-memory attribute was set by prepare_lbm_rows)
-        int bx = 128;
-        while (c.nx % bx != 0) bx -= 32;
-        const dim3 g0(c.nx / bx, c.ny, 1);
+        const int bx = z0_block_x(c.nx);
+        const dim3 g0((c.nx + bx - 1) / bx, c.ny, 1);
         if (macros) lbm_step_kernel<T, R, false, true><<<g0, bx, 0, s>>>(a, k, 0, 0);
         else lbm_step_kernel<T, R, false, false><<<g0, bx, 0, s>>>(a, k, 0, 0);
         const size_t sm = lbm_rows_smem(c.nx, sizeof(typename PopT<T>::F), sizeof(typename PopT<T>::G));
-        if (macros) lbm_rows_kernel<T, R, true><<<la.rows_grid, c.nx, sm, s>>>(a, k);
-        else lbm_rows_kernel<T, R, false><<<la.rows_grid, c.nx, sm, s>>>(a, k);
+        const int tx = rows_block_x(c.nx);
+        rows_kernel<T, R>(macros, c.nx % 32 != 0)<<<la.rows_grid, tx, sm, s>>>(a, k);
         return cudaGetLastError();
     }
     const int bx = la.node_bx > 0 ? la.node_bx : lbm_default_block_x(c.nx);
@@ -1366,7 +1397,7 @@ int lbm_blocks_per_plane(int nx, int ny, int bx) {
     return ((nx + bx - 1) / bx) * ((ny + by - 1) / by) * 4;
 }
 
-int lbm_rows_slots_per_plane(int nx, int ny) { return ny * (nx / 32); }
+int lbm_rows_slots_per_plane(int nx, int ny) { return ny * ((nx + 31) / 32); }
 
 // ---- seeded initial state ------------------------------------------------------
 

@@ -451,7 +451,7 @@ poisson_rows_fwd_fast(const R *__restrict__ q, typename Cplx<R>::T *__restrict__
     }
     __syncthreads();
     const int tr = tid / G, j = tid - tr * G;
-    fft::Plan<N>::template run<-1>(buf + tr * P, tws, j);
+    fft::run_tile<N, -1>(buf + tr * P, tws, j);
     R2 *sp = spec + (size_t)zi * ny * pitch;
     for (int i = tid; i < TB * nxh; i += 256) {
         const int t2 = i / nxh, k = i - t2 * nxh;
@@ -504,7 +504,7 @@ poisson_cols_fast(typename Cplx<R>::T *__restrict__ spec,
     if (S < 0 && blockIdx.x == 0 && tid < 32) plane_sum_warp(rowsum, planesum, zi, N);
     __syncthreads();
     const int tr = tid / G, j = tid - tr * G;
-    fft::Plan<N>::template run<S>(buf + tr * P, tws, j);
+    fft::run_tile<N, S>(buf + tr * P, tws, j);
     if (valid) {
 #pragma unroll
         for (int r = 0; r < IT; ++r)
@@ -567,7 +567,7 @@ poisson_rows_inv_fast(const typename Cplx<R>::T *__restrict__ spec, R *__restric
     }
     __syncthreads();
     const int tr = tid / G, j = tid - tr * G;
-    fft::Plan<N>::template run<1>(buf + tr * P, tws, j);
+    fft::run_tile<N, 1>(buf + tr * P, tws, j);
     const R norm = (R)(1.0 / ((double)N * (double)ny));
     R *pp = phip + (size_t)N * ny * (zi + 1);
     for (int i = tid; i < TB * N; i += 256) {
@@ -685,6 +685,15 @@ poisson_zsolve(typename Cplx<R>::T *__restrict__ spec, const double *__restrict_
     }
 }
 
+// x, hidden from the optimiser: the values derived from it inside a loop are
+// recomputed in each iteration instead of being hoisted into registers that
+// stay live over the whole loop
+__device__ __forceinline__ int opaque(int x) {
+    int y;
+    asm volatile("mov.b32 %0, %1;" : "=r"(y) : "r"(x));
+    return y;
+}
+
 // correctly rounded reciprocal
 __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
@@ -725,7 +734,7 @@ poisson_zdst(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::T *
         ez00 = (double *)gp.ez00;
     }
     using R2 = typename Cplx<R>::T;
-    constexpr int G = fft::Plan<L>::G, TB = 256 / G, P = tstride<L>();
+    constexpr int G = fft::WPlan<L>::G, TB = 256 / G, P = tstride<L>();
     constexpr int n = L / 2 - 1, nz = n + 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R2 *tws = reinterpret_cast<R2 *>(smem_raw);
@@ -783,23 +792,30 @@ poisson_zdst(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::T *
         }
     }
     __syncthreads();
-    const int tr = tid / G, j = tid - tr * G;
-    fft::Plan<L>::template run<-1>(buf + tr * P, tws, j);
-    // transform tr, bins k = j + G u
-#pragma unroll
-    for (int u = 0; u < L / G; ++u) {
-        const int k = j + G * u;
-        R2 &y = buf[tr * P + fft::pad(k)];
+    {
+        // the two transforms of each mode warp-synchronous (G threads of one
+        // warp), the division applied by the first one's last pass
+        const int tr = tid / G, j = tid - tr * G;
+        R2 *tb = buf + tr * P;
         const R h = hdz2[tr];
-        if (k == 0 || k == L / 2 || h < (R)0) {
-            y = R2{(R)0, (R)0};
-        } else {
+        auto ld = [&](int m) { return tb[fft::pad(m)]; };
+        auto div = [&](int k, R2 v) {
+            if (k == 0 || k == L / 2 || h < (R)0) return R2{(R)0, (R)0};
             const R f = rcp(lamz[k < L / 2 ? k : L - k] + h);
-            y = R2{y.x * f, y.y * f};
+            return R2{v.x * f, v.y * f};
+        };
+        if constexpr (L == 64 || L == 256) {
+            fft::wfilter_sq<L, G, -1, -1>(tb, tws, j, ld, div,
+                                         [&](int m, R2 v) { tb[fft::pad(m)] = v; });
+        } else {
+            fft::WPlan<L>::template run<-1>(tb, tws, j, ld,
+                                            [&](int k, R2 v) { tb[fft::pad(k)] = div(k, v); });
+            __syncwarp();
+            fft::WPlan<L>::template run<-1>(tb, tws, j, ld,
+                                            [&](int m, R2 v) { tb[fft::pad(m)] = v; });
         }
     }
     __syncthreads();
-    fft::Plan<L>::template run<-1>(buf + tr * P, tws, j);
     const R sc = (R)(dz2 / (double)L);
     if (m < modes) {
 #pragma unroll
@@ -973,15 +989,6 @@ poisson_zdst_rt(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::
 // contiguous block.
 namespace {
 
-// x, hidden from the optimiser: the values derived from it inside a loop are
-// recomputed in each iteration instead of being hoisted into registers that
-// stay live over the whole loop
-__device__ __forceinline__ int opaque(int x) {
-    int y;
-    asm volatile("mov.b32 %0, %1;" : "=r"(y) : "r"(x));
-    return y;
-}
-
 // rows (ya, yb) of transform tr of a split-row block (two real rows per
 // complex transform): S = 1 pairs consecutive rows; S >= 2 pairs
 // n + 64 a and n + 64 (a + S/2) of group n = block * GB + tr / (S/2)
@@ -1100,7 +1107,7 @@ poisson_rows_fwd_split(const R *__restrict__ q, typename Cplx<R>::T *__restrict_
     __syncthreads();
     {
         const int tr = tid / G, jj = tid - tr * G;
-        fft::Plan<N>::template run<-1>(buf + tr * P, tws, jj);
+        fft::run_tile<N, -1>(buf + tr * P, tws, jj);
     }
     // items (g, kx), g fastest: the S rows n + 64 m of group g at bin kx, a
     // radix-S DFT over m, the twiddle W_NY^(j n), S outputs of GB consecutive
@@ -1204,18 +1211,32 @@ poisson_slab(typename Cplx<R>::T *__restrict__ spl, const typename Cplx<R>::T *_
     for (int i = tid; i < L; i += 256) twl[i] = twz[i];
     if (mean_block) {
         // FP64 plane sums of the source (fixed order), then the right-hand
-        // side of the mean mode (poisson.cu:97 for the voltage on z = 1)
+        // side of the mean mode (poisson.cu:97 for the voltage on z = 1); the
+        // row sums of four planes in flight at a time (this block is the
+        // longest of the launch otherwise)
         const double nxy = (double)nx * (double)NY;
-        for (int zi = warp; zi < n; zi += 8) {
-            double sum = 0.0;
-            for (int y = lane; y < NY; y += 32) sum += rowsum[(size_t)zi * NY + y];
+        constexpr int PW = 4, YL = NY / 32;
+        for (int z0 = warp * PW; z0 < n; z0 += 8 * PW) {
+            double v[PW][YL];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-            if (lane == 0) {
-                planesum[zi + 1] = sum;
-                double d = sum + nxy * (-(double)(R)qmean[2 * (zi + 1) + 1] / eps);
-                if (zi == 0) d += -voltage / dz2 * nxy;
-                mrhs[zi] = d * dz2;
+            for (int u = 0; u < PW; ++u)
+#pragma unroll
+                for (int t = 0; t < YL; ++t)
+                    v[u][t] = z0 + u < n ? rowsum[(size_t)(z0 + u) * NY + lane + 32 * t] : 0.0;
+#pragma unroll
+            for (int u = 0; u < PW; ++u) {
+                const int zi = z0 + u;
+                double sum = 0.0;
+#pragma unroll
+                for (int t = 0; t < YL; ++t) sum += v[u][t];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+                if (lane == 0 && zi < n) {
+                    planesum[zi + 1] = sum;
+                    double d = sum + nxy * (-(double)(R)qmean[2 * (zi + 1) + 1] / eps);
+                    if (zi == 0) d += -voltage / dz2 * nxy;
+                    mrhs[zi] = d * dz2;
+                }
             }
         }
     }
@@ -1373,7 +1394,7 @@ poisson_rows_inv_split(const typename Cplx<R>::T *__restrict__ spl, R *__restric
     __syncthreads();
     {
         const int tr = tid / G, jj = tid - tr * G;
-        fft::Plan<N>::template run<1>(buf + tr * P, tws, jj);
+        fft::run_tile<N, 1>(buf + tr * P, tws, jj);
     }
     const R norm = (R)(1.0 / ((double)N * (double)NY));
     R *pp = phip + (size_t)N * NY * (zi + 1);
@@ -1528,7 +1549,7 @@ static cudaError_t cols(const PoissonArgs &a, cudaStream_t s) {
 template <typename R, int L>
 static cudaError_t zdst(const PoissonArgs &a, cudaStream_t s) {
     using R2 = typename Cplx<R>::T;
-    constexpr int TB = per_block<L>();
+    constexpr int TB = 256 / fft::WPlan<L>::G;  // modes per block, as poisson_zdst
     const size_t sm = sizeof(R2) * ((size_t)L + (size_t)TB * tstride<L>());
     cudaError_t e = set_smem(poisson_zdst<R, L>, sm, s);
     if (e != cudaSuccess) return e;

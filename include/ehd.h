@@ -97,9 +97,10 @@ typedef struct ehd_tuning {
                                 where it applies (NX a power of two 64..512,
                                 NY = 64, 128, 256 or 512, 2 (NZ-1) likewise),
                                 else the five-kernel one; 1: five-kernel     */
-    int32_t z_solve;         /* where 2 (NZ-1) is not 64, 128, 256 or 512: 0
-                                the sine transform with run-time FFT passes,
-                                1 the FP64 Thomas sweep                       */
+    int32_t z_solve;         /* where 2 (NZ-1) is not a compile-time FFT
+                                size (48, 64, 80, 96, 128, 256, 512): 0 the
+                                sine transform with run-time FFT passes, 1 the
+                                FP64 Thomas sweep                             */
     int32_t reserved[2];     /* must be 0                                     */
 } ehd_tuning;
 

@@ -1,6 +1,7 @@
 """The bulk-copy row kernel (steady-state steps with FP32 or FP64 populations
-on grids with nx a multiple of 32 up to 256) against the oracle and against
-the one-thread-per-node kernel.
+on grids with 32 <= nx <= 256 and rows of a multiple of 16 bytes; CTAs of nx
+rounded up to whole warps, the lanes past the row idle) against the oracle and
+against the one-thread-per-node kernel.
 
 The first step after set_fields always runs on the per-node kernel (it reads
 the uploaded state in place); the steps after it run on the row kernel
@@ -23,9 +24,11 @@ def random_fields(p, seed):
     return M.random_fields(p, seed)
 
 
-# x-rows of 1 to 8 warps; ny = 1 and nz = 4 are the smallest planes and stacks
+# x-rows of 1 to 8 warps, and rows that end inside a warp (48, 80, 100, 250
+# nodes); ny = 1 and nz = 4 are the smallest planes and stacks
 @pytest.mark.parametrize("shape", [(32, 12, 9), (64, 20, 11), (96, 10, 6), (256, 4, 5),
-                                   (128, 1, 17), (64, 64, 4)])
+                                   (128, 1, 17), (64, 64, 4), (48, 12, 9), (80, 10, 7),
+                                   (100, 6, 5), (250, 3, 5)])
 def test_row_kernel_steps_match_oracle(shape):
     nx, ny, nz = shape
     dz = 1.0 / (nz - 1)
@@ -44,13 +47,16 @@ def test_row_kernel_steps_match_oracle(shape):
         assert relerr(a[k], b[k]) < 1e-10, (k, relerr(a[k], b[k]))
 
 
+@pytest.mark.parametrize("shape", [(64, 64, 33), (80, 48, 25)])
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-11), ("fp32", 1e-5)])
-def test_row_kernel_agrees_with_node_kernel(prec, tol):
-    """Same run on both kernels.  The plane sums behind the per-plane
-    references are taken in a different order, so the two agree to the
-    rounding of the storage type, not bitwise."""
-    dz = 1.0 / 32
-    p = O.params_from_groups(64, 64, 33, 64 * dz, 64 * dz, T=200, M=10, C=10, Fe=4000)
+def test_row_kernel_agrees_with_node_kernel(shape, prec, tol):
+    """Same run on both kernels (80 nodes: the third warp of a row half
+    idle).  The plane sums behind the per-plane references are taken in a
+    different order, so the two agree to the rounding of the storage type,
+    not bitwise."""
+    nx, ny, nz = shape
+    dz = 1.0 / (nz - 1)
+    p = O.params_from_groups(nx, ny, nz, nx * dz, ny * dz, T=200, M=10, C=10, Fe=4000)
     f = random_fields(p, 5)
     out = []
     for rows in (True, False):
