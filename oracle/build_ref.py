@@ -64,6 +64,13 @@ CASES = {
     # magic parameters: the developed-convection run to non-finite fields
     "config0_t400": dict(nx=64, ny=64, nz=33, threads=64, flag=1, nu=0.0625, K=2.5e-5,
                          charge0=10.0, diffu=6.25e-5, V=1.0 / 12.0, VC=1.0e-6),
+    # the same two starts run on towards non-finite fields, printing the
+    # collector current every 1000 steps (main.cu:227-231), no whole-field output
+    "config0_long": dict(nx=64, ny=64, nz=33, threads=64, flag=1, no_output=True,
+                         print_current=1000, **_GROUPS),
+    "config0_t400_long": dict(nx=64, ny=64, nz=33, threads=64, flag=1, no_output=True,
+                              print_current=1000, nu=0.0625, K=2.5e-5, charge0=10.0,
+                              diffu=6.25e-5, V=1.0 / 12.0, VC=1.0e-6),
     # timing only: 256 x 256 x 129, reference initialisation, no text output
     "bench": dict(nx=256, ny=256, nz=129, threads=128, flag=0, no_output=True, **_GROUPS),
     # the reference's own default case (LBM.h:31-86: 122 x 122 x 101, dx = 1/100,
