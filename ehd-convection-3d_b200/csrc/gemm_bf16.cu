@@ -392,6 +392,62 @@ __device__ __forceinline__ void lm_load(float (&rb)[NT][4], const float *B, cons
             rb[j][e] = (kin[e] && (nmask >> j & 1u)) ? __ldg(B + bno[j] + ko[e]) : 0.f;
 }
 
+// C fragments of one warp unit (rows 16 i + gq + 8 h, columns n0 + 8 j + 2 tq
+// and + 1) with alpha, beta, bias and the optional GELU output
+template <int MT, int NT>
+__device__ __forceinline__ void lm_epilogue(const GemmArgs &a, const float (&acc)[MT][NT][4],
+                                            int bidx, int n0, int gq, int tq, int pair_store) {
+    const int coff = at_off<int>(a.cbat, bidx);
+    int cno[NT];
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+        const int n = n0 + 8 * j + 2 * tq;
+        cno[j] = n < a.N ? at_off<int>(a.cn, n) : 0;
+    }
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int m = 16 * i + gq + 8 * h;
+            if (m >= a.M) continue;
+            const int mo = coff + at_off<int>(a.cm, m);
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+                const int n = n0 + 8 * j + 2 * tq;
+                if (n >= a.N) continue;
+                float v0 = a.alpha * acc[i][j][2 * h], v1 = a.alpha * acc[i][j][2 * h + 1];
+                float *c = a.C + mo + cno[j];
+                if (pair_store && n + 1 < a.N) {
+                    if (a.beta != 0.f) {
+                        const float2 o = *reinterpret_cast<const float2 *>(c);
+                        v0 += a.beta * o.x;
+                        v1 += a.beta * o.y;
+                    }
+                    if (a.bias) {
+                        v0 += __ldg(a.bias + n);
+                        v1 += __ldg(a.bias + n + 1);
+                    }
+                    *reinterpret_cast<float2 *>(c) = make_float2(v0, v1);
+                    if (a.C2)
+                        *reinterpret_cast<float2 *>(a.C2 + mo + cno[j]) =
+                            make_float2(gelu(v0), gelu(v1));
+                } else {
+                    if (a.beta != 0.f) v0 += a.beta * *c;
+                    if (a.bias) v0 += __ldg(a.bias + n);
+                    *c = v0;
+                    if (a.C2) a.C2[mo + cno[j]] = gelu(v0);
+                    if (n + 1 < a.N) {
+                        const int o1 = mo + at_off<int>(a.cn, n + 1);
+                        if (a.beta != 0.f) v1 += a.beta * a.C[o1];
+                        if (a.bias) v1 += __ldg(a.bias + n + 1);
+                        a.C[o1] = v1;
+                        if (a.C2) a.C2[o1] = gelu(v1);
+                    }
+                }
+            }
+        }
+}
+
 template <int MT, int NT>
 __global__ void __launch_bounds__(256) leftmul_kernel(const GemmArgs a, int pair_store) {
     constexpr int NC = 8 * NT;
@@ -470,57 +526,136 @@ __global__ void __launch_bounds__(256) leftmul_kernel(const GemmArgs a, int pair
                 for (int j = 0; j < NT; ++j) mma16816(acc[i][j], a0, a1, a2, a3, bf[j][0], bf[j][1]);
             }
         }
-        // epilogue: rows 16 i + gq + 8 h, columns n0 + 8 j + 2 tq (+1)
-        const int coff = at_off<int>(a.cbat, bidx);
-        int cno[NT];
-#pragma unroll
-        for (int j = 0; j < NT; ++j) {
-            const int n = n0 + 8 * j + 2 * tq;
-            cno[j] = n < a.N ? at_off<int>(a.cn, n) : 0;
+        lm_epilogue<MT, NT>(a, acc, bidx, n0, gq, tq, pair_store);
+    }
+}
+
+
+// ---- the same products with B staged by asynchronous copies ---------------
+//
+// Where every row of a warp unit's B block (NC = 8 NT consecutive columns at
+// one k) starts on a 16-byte boundary, each warp streams its units' K steps
+// into a ring of LM_STAGES shared-memory buffers of its own by cp.async (16
+// bytes a lane per copy, no registers held while the copies fly), LM_STAGES - 1
+// steps ahead of the products and across unit boundaries, and reads its
+// fragments from shared memory (rows padded by 4 floats, so that the 32 lanes
+// of a fragment load hit 32 distinct banks).  Columns past N and k past K are
+// zero-filled by the copies.
+constexpr int LM_STAGES = 3;
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, int bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int NT>
+constexpr int lm_stage_floats() { return 16 * (8 * NT + 4); }
+
+template <int MT, int NT>
+__global__ void __launch_bounds__(256) leftmul_cp_kernel(const GemmArgs a, int pair_store) {
+    constexpr int NC = 8 * NT, RS = NC + 4, STAGE = lm_stage_floats<NT>();
+    constexpr int C4 = NC / 4, CH = 16 * C4, CPL = (CH + 31) / 32;
+    extern __shared__ __align__(16) unsigned char lm_smem[];
+    const int kt = (a.K + 15) / 16, KP = 16 * kt + 8;
+    __nv_bfloat16 *As = reinterpret_cast<__nv_bfloat16 *>(lm_smem);  // [16 MT][KP]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int gq = lane >> 2, tq = lane & 3;
+    float *ring = reinterpret_cast<float *>(lm_smem + ((size_t)16 * MT * KP * 2 + 15) / 16 * 16) +
+                  (size_t)warp * LM_STAGES * STAGE;
+    for (int i = tid; i < 16 * MT * 16 * kt; i += blockDim.x) {
+        const int m = i / (16 * kt), k = i - m * (16 * kt);
+        float v = 0.f;
+        if (m < a.M && k < a.K) {
+            const long long o = at(a.am, m) + at(a.ak, k);
+            v = a.a_bf16 ? __bfloat162float(reinterpret_cast<const __nv_bfloat16 *>(a.A)[o])
+                         : reinterpret_cast<const float *>(a.A)[o];
         }
+        As[m * KP + k] = __float2bfloat16_rn(v);
+    }
+    __syncthreads();
+    const float *B = reinterpret_cast<const float *>(a.B);
+    const int chunks = (a.N + NC - 1) / NC;
+    const long long units = (long long)a.batch * chunks;
+    const long long ustep = (long long)gridDim.x * 8;
+    // copy cursor: unit lu, K step ls
+    long long lu = (long long)blockIdx.x * 8 + warp;
+    int ls = 0, lbase = 0, lcols = 0;
+    auto set_unit = [&](long long u) {
+        const int bidx = (int)(u / chunks), n0 = (int)(u - (long long)bidx * chunks) * NC;
+        lbase = at_off<int>(a.bbat, bidx) + at_off<int>(a.bn, n0);
+        lcols = a.N - n0 < NC ? a.N - n0 : NC;
+    };
+    if (lu < units) set_unit(lu);
+    auto issue = [&](int slot) {
+        if (lu < units) {
+            float *dst = ring + slot * STAGE;
+#pragma unroll
+            for (int t = 0; t < CPL; ++t) {
+                const int c = lane + 32 * t;
+                if (CH % 32 == 0 || c < CH) {
+                    const int r = c / C4, col = 4 * (c - r * C4), k = 16 * ls + r;
+                    int nv = lcols - col;
+                    nv = k < a.K ? (nv < 0 ? 0 : (nv > 4 ? 4 : nv)) : 0;
+                    const float *src = nv > 0 ? B + lbase + at_off<int>(a.bk, k) + col : B;
+                    cp_async16(dst + r * RS + col, src, 4 * nv);
+                }
+            }
+            if (++ls == kt) {
+                ls = 0;
+                lu += ustep;
+                if (lu < units) set_unit(lu);
+            }
+        }
+        cp_commit();  // one group per call, empty or not: the waits count groups
+    };
+#pragma unroll
+    for (int t = 0; t < LM_STAGES - 1; ++t) issue(t);
+    int cslot = 0, islot = LM_STAGES - 1;
+    for (long long u = (long long)blockIdx.x * 8 + warp; u < units; u += ustep) {
+        const int bidx = (int)(u / chunks), n0 = (int)(u - (long long)bidx * chunks) * NC;
+        float acc[MT][NT][4];
 #pragma unroll
         for (int i = 0; i < MT; ++i)
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int m = 16 * i + gq + 8 * h;
-                if (m >= a.M) continue;
-                const int mo = coff + at_off<int>(a.cm, m);
+            for (int j = 0; j < NT; ++j)
 #pragma unroll
-                for (int j = 0; j < NT; ++j) {
-                    const int n = n0 + 8 * j + 2 * tq;
-                    if (n >= a.N) continue;
-                    float v0 = a.alpha * acc[i][j][2 * h], v1 = a.alpha * acc[i][j][2 * h + 1];
-                    float *c = a.C + mo + cno[j];
-                    if (pair_store && n + 1 < a.N) {
-                        if (a.beta != 0.f) {
-                            const float2 o = *reinterpret_cast<const float2 *>(c);
-                            v0 += a.beta * o.x;
-                            v1 += a.beta * o.y;
-                        }
-                        if (a.bias) {
-                            v0 += __ldg(a.bias + n);
-                            v1 += __ldg(a.bias + n + 1);
-                        }
-                        *reinterpret_cast<float2 *>(c) = make_float2(v0, v1);
-                        if (a.C2)
-                            *reinterpret_cast<float2 *>(a.C2 + mo + cno[j]) =
-                                make_float2(gelu(v0), gelu(v1));
-                    } else {
-                        if (a.beta != 0.f) v0 += a.beta * *c;
-                        if (a.bias) v0 += __ldg(a.bias + n);
-                        *c = v0;
-                        if (a.C2) a.C2[mo + cno[j]] = gelu(v0);
-                        if (n + 1 < a.N) {
-                            const int o1 = mo + at_off<int>(a.cn, n + 1);
-                            if (a.beta != 0.f) v1 += a.beta * a.C[o1];
-                            if (a.bias) v1 += __ldg(a.bias + n + 1);
-                            a.C[o1] = v1;
-                            if (a.C2) a.C2[o1] = gelu(v1);
-                        }
-                    }
-                }
+                for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+        for (int s = 0; s < kt; ++s) {
+            cp_wait<LM_STAGES - 2>();
+            __syncwarp();  // every lane's copies of this step landed; the slot
+                           // consumed last step is free for the next copies
+            const float *st = ring + cslot * STAGE + gq;
+            uint32_t bf[NT][2];
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+                const float *c0 = st + 8 * j;
+                bf[j][0] = pack_bf16(make_float2(c0[(2 * tq) * RS], c0[(2 * tq + 1) * RS]));
+                bf[j][1] = pack_bf16(make_float2(c0[(2 * tq + 8) * RS], c0[(2 * tq + 9) * RS]));
             }
+            issue(islot);
+            cslot = cslot + 1 == LM_STAGES ? 0 : cslot + 1;
+            islot = islot + 1 == LM_STAGES ? 0 : islot + 1;
+#pragma unroll
+            for (int i = 0; i < MT; ++i) {
+                const __nv_bfloat16 *ap = As + (16 * i + gq) * KP + 16 * s + 2 * tq;
+                const uint32_t a0 = *reinterpret_cast<const uint32_t *>(ap);
+                const uint32_t a1 = *reinterpret_cast<const uint32_t *>(ap + 8 * KP);
+                const uint32_t a2 = *reinterpret_cast<const uint32_t *>(ap + 8);
+                const uint32_t a3 = *reinterpret_cast<const uint32_t *>(ap + 8 * KP + 8);
+#pragma unroll
+                for (int j = 0; j < NT; ++j) mma16816(acc[i][j], a0, a1, a2, a3, bf[j][0], bf[j][1]);
+            }
+        }
+        lm_epilogue<MT, NT>(a, acc, bidx, n0, gq, tq, pair_store);
     }
+    cp_wait<0>();
 }
 
 // ---- parameter gradients of pointwise layers ------------------------------
@@ -762,6 +897,30 @@ LeftKern left_kernel(int mt, int nt) {
     return nt == 4 ? left_kernel_nt<4>(mt) : nt == 2 ? left_kernel_nt<2>(mt) : left_kernel_nt<1>(mt);
 }
 
+template <int NT>
+LeftKern left_cp_kernel_nt(int mt) {
+    switch (mt) {
+        case 1: return leftmul_cp_kernel<1, NT>;
+        case 2: return leftmul_cp_kernel<2, NT>;
+        case 3: return leftmul_cp_kernel<3, NT>;
+        case 4: return leftmul_cp_kernel<4, NT>;
+        case 5: return leftmul_cp_kernel<5, NT < 4 ? NT : 2>;
+        case 6: return leftmul_cp_kernel<6, NT < 4 ? NT : 2>;
+        case 7: return leftmul_cp_kernel<7, NT < 4 ? NT : 2>;
+        default: return leftmul_cp_kernel<8, NT < 4 ? NT : 2>;
+    }
+}
+LeftKern left_cp_kernel(int mt, int nt) {
+    return nt == 4 ? left_cp_kernel_nt<4>(mt)
+                   : nt == 2 ? left_cp_kernel_nt<2>(mt) : left_cp_kernel_nt<1>(mt);
+}
+// every row of every unit's B block on a 16-byte boundary (cp.async)
+bool left_cp_aligned(const GemmArgs &a) {
+    auto m4 = [](const Map &m) { return m.s0 % 4 == 0 && (one_level(m) || m.s1 % 4 == 0); };
+    return ((uintptr_t)a.B & 15u) == 0 && m4(a.bk) && (a.batch == 1 || m4(a.bbat)) &&
+           (one_level(a.bn) || a.bn.s1 % 4 == 0);
+}
+
 bool even_map(const Map &m) { return (m.s0 % 2 == 0) && (one_level(m) || m.s1 % 2 == 0); }
 
 // The small-left-matrix kernel when the product has its shape: one A for the
@@ -779,11 +938,20 @@ bool try_leftmul(const GemmArgs &a, cudaStream_t s, cudaError_t *err) {
     const bool pair = a.cn.s0 == 1 && (one_level(a.cn) || (a.cn.g % 2 == 0 && a.cn.s1 % 2 == 0)) &&
                       even_map(a.cm) && (a.batch == 1 || even_map(a.cbat)) && aligned8(a.C) &&
                       (!a.C2 || aligned8(a.C2));
-    LeftKern k = left_kernel(mt, nt);
-    const size_t smem = (size_t)16 * mt * (16 * kt + 8) * sizeof(__nv_bfloat16);
+    // B staged by asynchronous copies where its rows are 16-byte aligned
+    const bool staged = left_cp_aligned(a);
+    LeftKern k = staged ? left_cp_kernel(mt, nt) : left_kernel(mt, nt);
+    size_t smem = (size_t)16 * mt * (16 * kt + 8) * sizeof(__nv_bfloat16);
+    if (staged) {
+        const int stage = nt == 4 ? lm_stage_floats<4>() : nt == 2 ? lm_stage_floats<2>()
+                                                                   : lm_stage_floats<1>();
+        smem = (smem + 15) / 16 * 16 + (size_t)8 * LM_STAGES * stage * sizeof(float);
+    }
     int dev = 0, nsm = 0, occ = 0;
-    cudaError_t e;
-    if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+    cudaError_t e = cudaSuccess;
+    if (smem > 48 * 1024)
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess || (e = cudaGetDevice(&dev)) != cudaSuccess ||
         (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
         (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 256, smem)) != cudaSuccess) {
         *err = e;

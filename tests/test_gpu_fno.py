@@ -60,11 +60,15 @@ def test_gemm_matches_float64_products_of_bf16_operands(M, N, K, batch, ta, tb):
 
 
 @pytest.mark.parametrize("M,N,K,batch", [(24, 8192, 64, 16), (64, 8192, 48, 8),
-                                         (128, 4096, 40, 8)])
+                                         (128, 4096, 40, 8), (24, 1004, 64, 48),
+                                         (40, 1002, 33, 48)])
 def test_gemm_with_one_left_matrix_for_the_batch(M, N, K, batch):
     """The small-left-matrix kernel with 32-, 16- and 8-column warp units (it
     takes the widest that still leaves 4096 units): one A for every product
-    of the batch, as the truncated DFTs have it."""
+    of the batch, as the truncated DFTs have it.  B's rows are 16-byte
+    aligned (N a multiple of 4: B staged by asynchronous copies, partial last
+    units zero-filled) or not (N = 1002: fragments loaded from global
+    memory)."""
     import torch
     g = torch.Generator().manual_seed(M + N + K)
     A = torch.randn(1, M, K, generator=g).cuda().expand(batch, M, K)
