@@ -1,7 +1,7 @@
 // gemm_bf16.cu -- the batched BF16 tensor-core product of gemm_bf16.cuh, and
 // the weight and bias gradients of pointwise layers.
 //
-// gemm() sends a product to one of three kernels by its shape (all of them
+// gemm() sends a product to one of four kernels by its shape (the first three
 // mma.sync.m16n8k16, BF16 operands, FP32 accumulation):
 //  - rowwise_kernel: A FP32 with unit stride along k, 16 | K <= 128, N <= 128
 //    (pointwise layers and their input gradients): B resident in shared
@@ -14,7 +14,10 @@
 //    of 32, 128 threads, each warp a 32 x 32 quarter as 2 x 4 mma tiles;
 //    operands staged in shared memory as BF16, A as [m][k] and B as [n][k],
 //    so that every fragment register is one aligned 32-bit load of two
-//    consecutive k.
+//    consecutive k;
+//  - smallk_kernel, K <= 16 and N <= 128 with A and C row-major (the lift and
+//    the projection's input gradient): BF16-rounded operands, FP32 FMAs,
+//    bound by the bytes it writes.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -658,6 +661,65 @@ __global__ void __launch_bounds__(256) leftmul_cp_kernel(const GemmArgs a, int p
     cp_wait<0>();
 }
 
+
+// ---- products with a small K -------------------------------------------------
+//
+// C[m][n] = alpha sum_k A[m][k] B[k][n] (+ beta C, + bias[n], GELU output) for
+// K <= 16 and N <= 128 with A and C row-major: the FNO's lift (K = 9) and the
+// projection's input gradient (K = 5).  They are bound by the output bytes, so
+// they run on the FP32 pipes: B staged once per block in shared memory, each
+// warp taking 32 rows at a time (their A values staged in shared memory by
+// coalesced loads, read back as broadcasts), lane l computing the columns
+// l + 32 j.  Operands are rounded to BF16 as on the tensor-core paths, so
+// every product is the same exact FP32 value; only the order of the K-term
+// sum differs.
+constexpr int SK_MAXK = 16, SK_MAXN = 128;
+
+template <int BF>
+__global__ void __launch_bounds__(256) smallk_kernel(const GemmArgs a) {
+    __shared__ float Bs[SK_MAXK * SK_MAXN];
+    __shared__ float As[8][32 * SK_MAXK];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int K = a.K, N = a.N;
+    for (int i = tid; i < K * N; i += blockDim.x) {
+        const int k = i / N, n = i - k * N;
+        const uint32_t raw = a.b_bf16 ? ld_raw<1>(a.B, at(a.bk, k) + at(a.bn, n))
+                                      : ld_raw<0>(a.B, at(a.bk, k) + at(a.bn, n));
+        Bs[i] = __bfloat162float(a.b_bf16 ? to_bf16<1>(raw) : to_bf16<0>(raw));
+    }
+    __syncthreads();
+    const long long lda = a.am.s0, ldc = a.cm.s0;
+    float *as = As[warp];
+    const long long tiles = ((long long)a.M + 31) / 32;
+    for (long long t = (long long)blockIdx.x * 8 + warp; t < tiles; t += (long long)gridDim.x * 8) {
+        const long long m0 = t * 32;
+        const int rows = a.M - m0 < 32 ? (int)(a.M - m0) : 32;
+        __syncwarp();
+        for (int i = lane; i < rows * K; i += 32) {
+            const int r = i / K, k = i - r * K;
+            as[i] = __bfloat162float(to_bf16<BF>(ld_raw<BF>(a.A, (m0 + r) * lda + k)));
+        }
+        __syncwarp();
+        for (int r = 0; r < rows; ++r) {
+            const float *ar = as + r * K;
+            float *crow = a.C + (m0 + r) * ldc;
+            float *c2row = a.C2 ? a.C2 + (m0 + r) * ldc : nullptr;
+#pragma unroll
+            for (int j = 0; j < SK_MAXN / 32; ++j) {
+                const int n = lane + 32 * j;
+                if (n >= N) break;
+                float acc = 0.f;
+                for (int k = 0; k < K; ++k) acc = fmaf(ar[k], Bs[k * N + n], acc);
+                float v = a.alpha * acc;
+                if (a.beta != 0.f) v += a.beta * crow[n];
+                if (a.bias) v += __ldg(a.bias + n);
+                crow[n] = v;
+                if (c2row) c2row[n] = gelu(v);
+            }
+        }
+    }
+}
+
 // ---- parameter gradients of pointwise layers ------------------------------
 //
 // G[m][n] += sum_r X[r][m] D[r][n] and gb[n] += sum_r D[r][n] over all rows r
@@ -964,6 +1026,28 @@ bool try_leftmul(const GemmArgs &a, cudaStream_t s, cudaError_t *err) {
     return true;
 }
 
+// The small-K kernel when the product has its shape: K <= 16, N <= 128, one
+// product (no batch, no split K), A with unit stride along k and C along n.
+bool try_smallk(const GemmArgs &a, cudaStream_t s, cudaError_t *err) {
+    if (a.K > SK_MAXK || a.N > SK_MAXN || a.batch != 1 || a.ksplit != 1) return false;
+    if (!one_level(a.ak) || a.ak.s0 != 1 || !one_level(a.am) || !one_level(a.cn) ||
+        a.cn.s0 != 1 || !one_level(a.cm))
+        return false;
+    int dev = 0, nsm = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) {
+        *err = e;
+        return true;
+    }
+    const long long tiles = ((long long)a.M + 31) / 32;
+    const long long blocks = std::min((tiles + 7) / 8, (long long)nsm * 4);
+    if (a.a_bf16) smallk_kernel<1><<<(unsigned)blocks, 256, 0, s>>>(a);
+    else smallk_kernel<0><<<(unsigned)blocks, 256, 0, s>>>(a);
+    *err = cudaGetLastError();
+    return true;
+}
+
 using WgradKern = void (*)(const float *, int, int, const float *, int, int, long long, float *,
                            int, float *);
 
@@ -1025,7 +1109,8 @@ cudaError_t gemm(const GemmArgs &a, cudaStream_t s) {
     const long long gy = (a.M + BM - 1) / BM, gz = (long long)a.batch * a.ksplit;
     if (gy > 65535 || gz > 65535) return cudaErrorInvalidValue;
     cudaError_t rerr = cudaSuccess;
-    if (try_rowwise(a, s, &rerr) || try_leftmul(a, s, &rerr)) return rerr;
+    if (try_rowwise(a, s, &rerr) || try_leftmul(a, s, &rerr) || try_smallk(a, s, &rerr))
+        return rerr;
     dim3 grid((a.N + BN - 1) / BN, (unsigned)gy, (unsigned)gz);
     // lanes along the operand's unit-stride index: k where it has one, else
     // the row index (m of A, n of B)

@@ -27,8 +27,10 @@ def rel(a, b):
 # (16, 8, 16): partial 16-row tiles, odd C rows (single-element stores),
 # batches; the small-left-matrix one (one A, M, K <= 128, B with unit stride
 # along n) for (17, 9, 112) and the last four: M = 9..128, K = 5..128
-# (partial K steps), odd N; the tiled one for the rest (K = 200, a transposed
-# A per product, K = 1000)
+# (partial K steps), odd N; the small-K one (K <= 16, N <= 128, A and C
+# row-major) for the last three, shaped like the lift and the projection's
+# input gradient; the tiled one for the rest (K = 200, a transposed A per
+# product, K = 1000)
 @pytest.mark.parametrize("M,N,K,batch,ta,tb", [(64, 64, 32, 1, False, False),
                                                (37, 5, 128, 2, False, False),
                                                (300, 128, 32, 1, False, False),
@@ -43,7 +45,10 @@ def rel(a, b):
                                                (100, 300, 40, 1, True, False),
                                                (24, 1000, 64, 1, True, False),
                                                (128, 77, 128, 1, True, False),
-                                               (9, 33, 5, 1, True, False)])
+                                               (9, 33, 5, 1, True, False),
+                                               (5000, 32, 9, 1, False, False),
+                                               (3000, 128, 5, 1, False, True),
+                                               (77, 100, 3, 1, False, False)])
 def test_gemm_matches_float64_products_of_bf16_operands(M, N, K, batch, ta, tb):
     import torch
     g = torch.Generator().manual_seed(M * N + K)
