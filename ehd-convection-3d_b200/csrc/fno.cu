@@ -126,6 +126,83 @@ __global__ void mix_kernel(const float *__restrict__ re, const float *__restrict
     }
 }
 
+// The same for W a template parameter (W = 8, 16, 32) and at most 4 samples:
+// a lane holds its W^2/32 weights of each part and its share of the inputs in
+// registers, and loads the next mode's while the products of this one run,
+// so that one mode's loads are in flight at any time instead of one row
+// batch of them.
+template <int WT>
+__global__ void mix_kernel_w(const float *__restrict__ re, const float *__restrict__ im,
+                             const float *__restrict__ in, float *__restrict__ out, int modes,
+                             int B, int adj) {
+    constexpr int W = WT, WP = W + 1, V = (W * W + 31) / 32, XV = (8 * W + 31) / 32;
+    extern __shared__ float mix_smem[];
+    const int nw = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float *Rr = mix_smem + (size_t)warp * mix_warp_floats(W);
+    float *Ri = Rr + W * WP;
+    float *X = Ri + W * WP;  // [4 samples][re, im][W]
+    const size_t plane = (size_t)modes * W;
+    float vr[V], vi[V], xv[XV];
+    auto load = [&](int md) {
+        const float *pr = re + (size_t)md * W * W, *pi = im + (size_t)md * W * W;
+#pragma unroll
+        for (int u = 0; u < V; ++u) {
+            const int t = lane + 32 * u;
+            vr[u] = t < W * W ? __ldg(pr + t) : 0.f;
+            vi[u] = t < W * W ? __ldg(pi + t) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < XV; ++u) {
+            const int t = lane + 32 * u;
+            const int bb = t / (2 * W), rem = t - bb * 2 * W, ri = rem / W, c = rem - ri * W;
+            xv[u] = bb < B ? __ldg(in + (size_t)bb * 2 * plane + ri * plane + (size_t)md * W + c)
+                           : 0.f;
+        }
+    };
+    int md = blockIdx.x * nw + warp;
+    if (md < modes) load(md);
+    for (; md < modes; md += gridDim.x * nw) {
+        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < V; ++u) {
+            const int t = lane + 32 * u;
+            if (t < W * W) {
+                const int o = t / W, i = t - o * W;
+                const int r = adj ? i : o, c = adj ? o : i;
+                Rr[r * WP + c] = vr[u];
+                Ri[r * WP + c] = adj ? -vi[u] : vi[u];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < XV; ++u)
+            if (lane + 32 * u < 8 * W) X[lane + 32 * u] = xv[u];
+        __syncwarp();
+        const int next = md + gridDim.x * nw;
+        if (next < modes) load(next);
+        for (int o = lane; o < W; o += 32) {
+            float ar[4] = {0.f, 0.f, 0.f, 0.f}, ai[4] = {0.f, 0.f, 0.f, 0.f};
+            const float *rr = Rr + o * WP, *rm = Ri + o * WP;
+#pragma unroll 8
+            for (int i = 0; i < W; ++i) {
+                const float r = rr[i], m = rm[i];
+#pragma unroll
+                for (int bb = 0; bb < 4; ++bb) {
+                    const float xr = X[bb * 2 * W + i], xi = X[bb * 2 * W + W + i];
+                    ar[bb] = fmaf(r, xr, fmaf(-m, xi, ar[bb]));
+                    ai[bb] = fmaf(r, xi, fmaf(m, xr, ai[bb]));
+                }
+            }
+#pragma unroll
+            for (int bb = 0; bb < 4; ++bb) {
+                if (bb >= B) break;
+                float *po = out + (size_t)bb * 2 * plane + (size_t)md * W + o;
+                po[0] = ar[bb];
+                po[plane] = ai[bb];
+            }
+        }
+    }
+}
+
 // Gradient of R from the mixing's output gradient dout and its input x
 // (both Zh layout), added to gRe, gIm ([mode][out][in]):
 //   gRe[o][i] += sum_b dout_re[o] x_re[i] + dout_im[o] x_im[i]
@@ -180,12 +257,6 @@ __global__ void mix_wgrad_kernel(const float *__restrict__ dout, const float *__
             }
         }
     }
-}
-
-__device__ __forceinline__ float gelu_grad(float z) {
-    const float phi = 0.3989422804014327f * expf(-0.5f * z * z);
-    const float cdf = 0.5f * (1.f + erff(z * 0.70710678118654752f));
-    return cdf + z * phi;
 }
 
 // d *= gelu'(z)
@@ -622,8 +693,16 @@ int mix_warps(int W, size_t per_warp_floats) {
 cudaError_t mix(const ehd_fno *f, int l, const float *in, float *out, int B, bool adj) {
     const int nw = mix_warps(f->W, mix_warp_floats(f->W));
     const unsigned blocks = (unsigned)std::min<size_t>((f->modes + nw - 1) / nw, 148 * 16);
-    mix_kernel<<<blocks, 32 * nw, nw * mix_warp_floats(f->W) * sizeof(float), f->stream>>>(
-        f->param + f->lo[l].Rre, f->param + f->lo[l].Rim, in, out, f->modes, f->W, B, adj ? 1 : 0);
+    const size_t sm = nw * mix_warp_floats(f->W) * sizeof(float);
+    const float *re = f->param + f->lo[l].Rre, *im = f->param + f->lo[l].Rim;
+    const int a = adj ? 1 : 0;
+    if (B <= 4 && (f->W == 8 || f->W == 16 || f->W == 32)) {
+        if (f->W == 8) mix_kernel_w<8><<<blocks, 32 * nw, sm, f->stream>>>(re, im, in, out, f->modes, B, a);
+        else if (f->W == 16) mix_kernel_w<16><<<blocks, 32 * nw, sm, f->stream>>>(re, im, in, out, f->modes, B, a);
+        else mix_kernel_w<32><<<blocks, 32 * nw, sm, f->stream>>>(re, im, in, out, f->modes, B, a);
+    } else {
+        mix_kernel<<<blocks, 32 * nw, sm, f->stream>>>(re, im, in, out, f->modes, f->W, B, a);
+    }
     return cudaGetLastError();
 }
 

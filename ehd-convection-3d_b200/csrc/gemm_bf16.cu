@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cstdint>
 #include <utility>
 
@@ -41,10 +42,6 @@ __device__ __forceinline__ void mma16816(float (&c)[4], uint32_t a0, uint32_t a1
         "{%8,%9}, {%0,%1,%2,%3};"
         : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-
-__device__ __forceinline__ float gelu(float v) {
-    return 0.5f * v * (1.f + erff(v * 0.70710678118654752f));
 }
 
 // Raw bits of one operand element: the FP32 value, or the BF16 value in the
@@ -667,54 +664,75 @@ __global__ void __launch_bounds__(256) leftmul_cp_kernel(const GemmArgs a, int p
 // C[m][n] = alpha sum_k A[m][k] B[k][n] (+ beta C, + bias[n], GELU output) for
 // K <= 16 and N <= 128 with A and C row-major: the FNO's lift (K = 9) and the
 // projection's input gradient (K = 5).  They are bound by the output bytes, so
-// they run on the FP32 pipes: B staged once per block in shared memory, each
-// warp taking 32 rows at a time (their A values staged in shared memory by
-// coalesced loads, read back as broadcasts), lane l computing the columns
-// l + 32 j.  Operands are rounded to BF16 as on the tensor-core paths, so
+// they run on the FP32 pipes, K a template parameter: lane l holds B[k][n] of
+// its columns n = l + 32 j in registers, each warp takes 32 rows at a time
+// (their A values loaded one tile ahead into registers, staged in shared
+// memory, read back as broadcasts).  Operands are rounded to BF16 as on the tensor-core paths, so
 // every product is the same exact FP32 value; only the order of the K-term
 // sum differs.
-constexpr int SK_MAXK = 16, SK_MAXN = 128;
+constexpr int SK_MAXK = 16, SK_MAXN = 128, SK_NJ = SK_MAXN / 32;
 
-template <int BF>
+template <int BF, int KK>
 __global__ void __launch_bounds__(256) smallk_kernel(const GemmArgs a) {
-    __shared__ float Bs[SK_MAXK * SK_MAXN];
-    __shared__ float As[8][32 * SK_MAXK];
+    __shared__ float As[8][32 * KK];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int K = a.K, N = a.N;
-    for (int i = tid; i < K * N; i += blockDim.x) {
-        const int k = i / N, n = i - k * N;
-        const uint32_t raw = a.b_bf16 ? ld_raw<1>(a.B, at(a.bk, k) + at(a.bn, n))
-                                      : ld_raw<0>(a.B, at(a.bk, k) + at(a.bn, n));
-        Bs[i] = __bfloat162float(a.b_bf16 ? to_bf16<1>(raw) : to_bf16<0>(raw));
-    }
-    __syncthreads();
+    const int N = a.N;
+    float bv[KK][SK_NJ];
+#pragma unroll
+    for (int k = 0; k < KK; ++k)
+#pragma unroll
+        for (int j = 0; j < SK_NJ; ++j) {
+            const int n = lane + 32 * j;
+            float v = 0.f;
+            if (n < N) {
+                const long long o = at(a.bk, k) + at(a.bn, n);
+                v = a.b_bf16 ? __bfloat162float(to_bf16<1>(ld_raw<1>(a.B, o)))
+                             : __bfloat162float(to_bf16<0>(ld_raw<0>(a.B, o)));
+            }
+            bv[k][j] = v;
+        }
     const long long lda = a.am.s0, ldc = a.cm.s0;
     float *as = As[warp];
-    const long long tiles = ((long long)a.M + 31) / 32;
-    for (long long t = (long long)blockIdx.x * 8 + warp; t < tiles; t += (long long)gridDim.x * 8) {
+    const long long tiles = ((long long)a.M + 31) / 32, tstep = (long long)gridDim.x * 8;
+    // the next tile's A values in flight while this tile's rows are computed
+    uint32_t araw[KK];
+    auto load_tile = [&](long long t) {
+        const long long m0 = t * 32;
+        const int rows = a.M - m0 < 32 ? (int)(a.M - m0) : 32;
+#pragma unroll
+        for (int u = 0; u < KK; ++u) {
+            const int i = lane + 32 * u, r = i / KK, k = i - r * KK;
+            araw[u] = r < rows ? ld_raw<BF>(a.A, (m0 + r) * lda + k) : 0u;
+        }
+    };
+    long long t = (long long)blockIdx.x * 8 + warp;
+    if (t < tiles) load_tile(t);
+    for (; t < tiles; t += tstep) {
         const long long m0 = t * 32;
         const int rows = a.M - m0 < 32 ? (int)(a.M - m0) : 32;
         __syncwarp();
-        for (int i = lane; i < rows * K; i += 32) {
-            const int r = i / K, k = i - r * K;
-            as[i] = __bfloat162float(to_bf16<BF>(ld_raw<BF>(a.A, (m0 + r) * lda + k)));
-        }
-        __syncwarp();
-        for (int r = 0; r < rows; ++r) {
-            const float *ar = as + r * K;
-            float *crow = a.C + (m0 + r) * ldc;
-            float *c2row = a.C2 ? a.C2 + (m0 + r) * ldc : nullptr;
 #pragma unroll
-            for (int j = 0; j < SK_MAXN / 32; ++j) {
+        for (int u = 0; u < KK; ++u) as[lane + 32 * u] = __bfloat162float(to_bf16<BF>(araw[u]));
+        __syncwarp();
+        if (t + tstep < tiles) load_tile(t + tstep);
+        for (int r = 0; r < rows; ++r) {
+            float ar[KK];
+#pragma unroll
+            for (int k = 0; k < KK; ++k) ar[k] = as[r * KK + k];
+            float *crow = a.C + (m0 + r) * ldc;
+#pragma unroll
+            for (int j = 0; j < SK_NJ; ++j) {
                 const int n = lane + 32 * j;
-                if (n >= N) break;
-                float acc = 0.f;
-                for (int k = 0; k < K; ++k) acc = fmaf(ar[k], Bs[k * N + n], acc);
-                float v = a.alpha * acc;
-                if (a.beta != 0.f) v += a.beta * crow[n];
-                if (a.bias) v += __ldg(a.bias + n);
-                crow[n] = v;
-                if (c2row) c2row[n] = gelu(v);
+                if (n < N) {
+                    float acc = 0.f;
+#pragma unroll
+                    for (int k = 0; k < KK; ++k) acc = fmaf(ar[k], bv[k][j], acc);
+                    float v = a.alpha * acc;
+                    if (a.beta != 0.f) v += a.beta * crow[n];
+                    if (a.bias) v += __ldg(a.bias + n);
+                    crow[n] = v;
+                    if (a.C2) a.C2[(m0 + r) * ldc + n] = gelu(v);
+                }
             }
         }
     }
@@ -1026,6 +1044,18 @@ bool try_leftmul(const GemmArgs &a, cudaStream_t s, cudaError_t *err) {
     return true;
 }
 
+using SmallKern = void (*)(const GemmArgs);
+template <int BF, int... KS>
+std::array<SmallKern, sizeof...(KS)> smallk_row(std::integer_sequence<int, KS...>) {
+    return {smallk_kernel<BF, KS + 1>...};
+}
+const std::array<std::array<SmallKern, SK_MAXK>, 2> &smallk_table() {
+    static const std::array<std::array<SmallKern, SK_MAXK>, 2> t = {
+        smallk_row<0>(std::make_integer_sequence<int, SK_MAXK>{}),
+        smallk_row<1>(std::make_integer_sequence<int, SK_MAXK>{})};
+    return t;
+}
+
 // The small-K kernel when the product has its shape: K <= 16, N <= 128, one
 // product (no batch, no split K), A with unit stride along k and C along n.
 bool try_smallk(const GemmArgs &a, cudaStream_t s, cudaError_t *err) {
@@ -1033,17 +1063,19 @@ bool try_smallk(const GemmArgs &a, cudaStream_t s, cudaError_t *err) {
     if (!one_level(a.ak) || a.ak.s0 != 1 || !one_level(a.am) || !one_level(a.cn) ||
         a.cn.s0 != 1 || !one_level(a.cm))
         return false;
-    int dev = 0, nsm = 0;
+    SmallKern k = smallk_table()[a.a_bf16 ? 1 : 0][a.K - 1];
+    int dev = 0, nsm = 0, occ = 0;
     cudaError_t e;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
-        (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) {
+        (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 256, 0)) != cudaSuccess) {
         *err = e;
         return true;
     }
+    // one wave of resident blocks, each warp walking its tiles
     const long long tiles = ((long long)a.M + 31) / 32;
-    const long long blocks = std::min((tiles + 7) / 8, (long long)nsm * 4);
-    if (a.a_bf16) smallk_kernel<1><<<(unsigned)blocks, 256, 0, s>>>(a);
-    else smallk_kernel<0><<<(unsigned)blocks, 256, 0, s>>>(a);
+    const long long blocks = std::min((tiles + 7) / 8, (long long)nsm * std::max(occ, 1));
+    k<<<(unsigned)blocks, 256, 0, s>>>(a);
     *err = cudaGetLastError();
     return true;
 }

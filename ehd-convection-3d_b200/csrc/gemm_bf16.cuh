@@ -19,6 +19,17 @@
 namespace ehd {
 namespace fno {
 
+// GELU (erf form) and its derivative, shared by the products' epilogues and
+// the FNO's elementwise kernels
+__device__ __forceinline__ float gelu(float v) {
+    return 0.5f * v * (1.f + erff(v * 0.70710678118654752f));
+}
+__device__ __forceinline__ float gelu_grad(float z) {
+    const float phi = 0.3989422804014327f * expf(-0.5f * z * z);
+    const float cdf = 0.5f * (1.f + erff(z * 0.70710678118654752f));
+    return cdf + z * phi;
+}
+
 struct Map {
     long long s0 = 1, s1 = 0;
     int g = 1 << 30;
