@@ -1330,6 +1330,195 @@ poisson_slab(typename Cplx<R>::T *__restrict__ spl, const typename Cplx<R>::T *_
     }
 }
 
+// ---- the y transform and z solve of NY x NZ columns in one kernel ----------
+//
+// The five-kernel path's middle three (forward y FFT of the columns, the
+// sine-transform z solve, inverse y FFT) in one launch where NY and
+// L = 2 (NZ - 1) are compile-time sizes and NY is not 64 S (the split-y path's
+// grids): one block per TB consecutive kx columns holds them for every
+// interior plane in shared memory ([c][z - 1][y], rows padded), loaded and
+// stored with the TB columns running fastest (TB consecutive 8-byte values of
+// the spectrum per (z, y)).  Every transform is warp-synchronous
+// (fft::WPlan): the y rows in place, the z columns through the odd extension
+// as poisson_slab.  The block of kx = 0 also forms the FP64 plane sums of the
+// source and solves the (0,0) mode in closed form, as poisson_zdst.
+template <typename R, int NY, int L>
+constexpr int yz_cols() {
+    constexpr size_t col = sizeof(typename Cplx<R>::T) * (size_t)(L / 2 - 1) * tstride<NY>();
+    constexpr int tb = (int)((80 * 1024) / col);
+    return tb < 1 ? 1 : (tb > 4 ? 4 : tb);
+}
+template <typename R, int NY, int L>
+constexpr int yz_rows() {  // slab rows TB n, rounded up to whole rounds of the row warps
+    constexpr int per = 8 * (32 / fft::WPlan<NY>::G);
+    return (yz_cols<R, NY, L>() * (L / 2 - 1) + per - 1) / per * per;
+}
+template <typename R, int NY, int L>
+constexpr size_t yz_smem() {
+    return sizeof(typename Cplx<R>::T) *
+           ((size_t)NY + L + (size_t)yz_rows<R, NY, L>() * tstride<NY>() +
+            (size_t)8 * (32 / fft::WPlan<L>::G) * tstride<L>());
+}
+
+template <typename R, int NY, int L>
+__global__ void __launch_bounds__(256)
+poisson_yz(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::T *__restrict__ twy,
+           const typename Cplx<R>::T *__restrict__ twz, const R *__restrict__ lamz,
+           const double *__restrict__ rowsum, double *__restrict__ planesum,
+           const double *__restrict__ qmean, double *__restrict__ phi00,
+           double *__restrict__ ez00, int nx, int nxh, int pitch, double dz, double eps,
+           double voltage, double kx0, double ky0, const PoissonPtrs *__restrict__ grp) {
+    if (grp) {  // one instance of a group launch per blockIdx.z
+        const PoissonPtrs &gp = grp[blockIdx.z];
+        spec = (typename Cplx<R>::T *)gp.spec;
+        rowsum = (const double *)gp.rowsum;
+        planesum = (double *)gp.planesum;
+        qmean = (const double *)gp.qmean;
+        phi00 = (double *)gp.phi00;
+        ez00 = (double *)gp.ez00;
+    }
+    using R2 = typename Cplx<R>::T;
+    constexpr int n = L / 2 - 1, nz = n + 2;
+    constexpr int TB = yz_cols<R, NY, L>(), NRY = yz_rows<R, NY, L>();
+    constexpr int PY = tstride<NY>(), PL = tstride<L>();
+    constexpr int GY = fft::WPlan<NY>::G, TPWY = 32 / GY;
+    constexpr int GZ = fft::WPlan<L>::G, TPWZ = 32 / GZ;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *tyy = reinterpret_cast<R2 *>(smem_raw);
+    R2 *twl = tyy + NY;
+    R2 *slab = twl + L;  // [c][zi][y]
+    R2 *zb = slab + NRY * PY;
+    __shared__ double mrhs[n], mphi[nz];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int kxb = blockIdx.x * TB;
+    const bool mean_block = blockIdx.x == 0;
+    const double dz2 = dz * dz;
+    const size_t plane = (size_t)NY * pitch;
+    for (int i = tid; i < NY; i += 256) tyy[i] = twy[i];
+    for (int i = tid; i < L; i += 256) twl[i] = twz[i];
+    if (mean_block) {
+        // FP64 plane sums of the source (fixed order, as plane_sum_warp), then
+        // the right-hand side of the mean mode (poisson.cu:97)
+        const double nxy = (double)nx * (double)NY;
+        for (int zi = warp; zi < n; zi += 8) {
+            double sum = 0.0;
+            for (int y = lane; y < NY; y += 32) sum += rowsum[(size_t)zi * NY + y];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            if (lane == 0) {
+                planesum[zi + 1] = sum;
+                double d = sum + nxy * (-(double)(R)qmean[2 * (zi + 1) + 1] / eps);
+                if (zi == 0) d += -voltage / dz2 * nxy;
+                mrhs[zi] = d * dz2;
+            }
+        }
+    }
+    for (int i = tid; i < TB * n * NY; i += 256) {
+        const int c = i % TB, rest = i / TB, y = rest % NY, zi = rest / NY;
+        const int kx = kxb + c;
+        slab[(c * n + zi) * PY + fft::pad(y)] =
+            kx < nxh ? spec[(size_t)zi * plane + (size_t)y * pitch + kx] : R2{(R)0, (R)0};
+    }
+    __syncthreads();
+    // forward y FFT of every (c, z) row, TPWY rows a warp
+    {
+        const int g = lane / GY, t0 = lane - g * GY;
+#pragma unroll 1
+        for (int r = warp * TPWY + g; r < NRY; r += 8 * TPWY) {
+            R2 *row = slab + r * PY;
+            const bool act = r < TB * n;
+            fft::WPlan<NY>::template run<-1>(
+                row, tyy, opaque(t0),
+                [&](int m) { return act ? row[fft::pad(m)] : R2{(R)0, (R)0}; },
+                [&](int m, R2 v) { row[fft::pad(m)] = v; });
+        }
+    }
+    __syncthreads();
+    // z solve of every (c, ky) column, TPWZ a warp
+    {
+        const R sc = (R)(dz2 / (double)L);
+        const int g = lane / GZ, t0 = lane - g * GZ;
+        R2 *zw = zb + (warp * TPWZ + g) * PL;
+        constexpr int NCOL = TB * NY, NCR = (NCOL + 8 * TPWZ - 1) / (8 * TPWZ) * (8 * TPWZ);
+#pragma unroll 1
+        for (int cc = warp * TPWZ + g; cc < NCR; cc += 8 * TPWZ) {
+            const int t = opaque(t0);
+            const bool act = cc < NCOL;
+            const int c = act ? cc / NY : 0, ky = act ? cc - (cc / NY) * NY : 0;
+            const int kx = kxb + c;
+            const double wx = kx * kx0, wy = (ky <= NY / 2 ? ky : ky - NY) * ky0;
+            const R h = (!act || kx >= nxh || (kx == 0 && ky == 0)) ? (R)-1
+                                                                      : (R)((wx * wx + wy * wy) * dz2);
+            R2 *col = slab + c * n * PY + fft::pad(ky);
+            auto ld = [&](int m) {
+                const bool up = m < L / 2;
+                // (rows 0..n-1 of the column; m = 0 and L/2 read row 0, unused)
+                const R2 v = col[(up ? (m > 0 ? m - 1 : 0) : (m == L / 2 ? 0 : L - 1 - m)) * PY];
+                return (!act || m == 0 || m == L / 2) ? R2{(R)0, (R)0}
+                                                      : (up ? v : R2{-v.x, -v.y});
+            };
+            auto div = [&](int k, R2 v) {
+                if (k == 0 || k == L / 2 || h < (R)0) return R2{(R)0, (R)0};
+                const R f = rcp(lamz[k < L / 2 ? k : L - k] + h);
+                return R2{v.x * f, v.y * f};
+            };
+            auto st = [&](int m, R2 v) {
+                if (act && m >= 1 && m <= n) col[(m - 1) * PY] = R2{v.x * sc, v.y * sc};
+            };
+            if constexpr (L == 64 || L == 256) {
+                fft::wfilter_sq<L, GZ, -1, -1>(zw, twl, t, ld, div, st);
+            } else {
+                fft::WPlan<L>::template run<-1>(zw, twl, t, ld,
+                                                [&](int k, R2 v) { zw[fft::pad(k)] = div(k, v); });
+                __syncwarp();
+                fft::WPlan<L>::template run<-1>(zw, twl, opaque(t0),
+                                                [&](int m) { return zw[fft::pad(m)]; }, st);
+                __syncwarp();
+            }
+        }
+    }
+    __syncthreads();
+    // inverse y FFT of every row
+    {
+        const int g = lane / GY, t0 = lane - g * GY;
+#pragma unroll 1
+        for (int r = warp * TPWY + g; r < NRY; r += 8 * TPWY) {
+            R2 *row = slab + r * PY;
+            fft::WPlan<NY>::template run<1>(
+                row, tyy, opaque(t0), [&](int m) { return row[fft::pad(m)]; },
+                [&](int m, R2 v) { row[fft::pad(m)] = v; });
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < TB * n * NY; i += 256) {
+        const int c = i % TB, rest = i / TB, y = rest % NY, zi = rest / NY;
+        const int kx = kxb + c;
+        if (kx < nxh) spec[(size_t)zi * plane + (size_t)y * pitch + kx] = slab[(c * n + zi) * PY + fft::pad(y)];
+    }
+    if (mean_block) {
+        const double nxy = (double)nx * (double)NY;
+        for (int i = tid; i < nz; i += 256) {
+            double x = 0.0;
+            if (i == 0) {
+                x = voltage;
+            } else if (i < nz - 1) {
+                for (int jz = 1; jz <= n; ++jz) {
+                    const int lo = i < jz ? i : jz, hi = i < jz ? jz : i;
+                    x -= (double)(lo * (n + 1 - hi)) * mrhs[jz - 1];
+                }
+                x = x / (double)(n + 1) / nxy;
+            }
+            mphi[i] = x;
+            phi00[i] = x;
+        }
+        __syncthreads();
+        for (int z = tid; z < nz; z += 256) {
+            const int zc = z < 1 ? 1 : (z > nz - 2 ? nz - 2 : z);
+            ez00[z] = 0.5 * (mphi[zc - 1] - mphi[zc + 1]) / dz;
+        }
+    }
+}
+
 // K3 of the split path: x[n + 64 m] = sum_j W_S^(-j m) b_j[n] from
 // spl[j][kx][z - 1][n], Hermitian completion of two rows per transform,
 // inverse x-FFT, phi' = Re / (NX NY) (odd_extract, poisson.cu:154-167).
@@ -1561,6 +1750,60 @@ static cudaError_t zdst(const PoissonArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// ---- the fused y transform and z solve (poisson_yz) ----
+
+template <typename R, int NY, int L>
+static cudaError_t yz_nl(const PoissonArgs &a, cudaStream_t s) {
+    using R2 = typename Cplx<R>::T;
+    constexpr size_t sm = yz_smem<R, NY, L>();
+    cudaError_t e = set_smem(poisson_yz<R, NY, L>, sm, s);
+    if (e != cudaSuccess) return e;
+    constexpr int TB = yz_cols<R, NY, L>();
+    const R2 *tw = (const R2 *)a.twz;
+    poisson_yz<R, NY, L><<<dim3((a.nxh + TB - 1) / TB, 1, a.ngrp), 256, sm, s>>>(
+        (R2 *)a.spec, (const R2 *)a.twy, tw, (const R *)(tw + L), a.rowsum, a.planesum, a.qmean,
+        a.phi00, a.ez00, a.nx, a.nxh, a.pitch, a.dz, a.eps, a.voltage, 2.0 * M_PI / a.lx,
+        2.0 * M_PI / a.ly, a.grp);
+    return cudaGetLastError();
+}
+template <typename R, int NY>
+static cudaError_t yz_n(const PoissonArgs &a, cudaStream_t s) {
+    switch (2 * (a.nz - 1)) {
+        case 48: return yz_nl<R, NY, 48>(a, s);
+        case 64: return yz_nl<R, NY, 64>(a, s);
+        case 80: return yz_nl<R, NY, 80>(a, s);
+        case 96: return yz_nl<R, NY, 96>(a, s);
+        default: return yz_nl<R, NY, 128>(a, s);
+    }
+}
+template <typename R>
+static cudaError_t yz_all(const PoissonArgs &a, cudaStream_t s) {
+    switch (a.ny) {
+        case 48: return yz_n<R, 48>(a, s);
+        case 80: return yz_n<R, 80>(a, s);
+        default: return yz_n<R, 96>(a, s);
+    }
+}
+// whether poisson_yz serves a grid: NY = 48, 80 or 96 (the widths the split-y
+// path does not take), L = 2 (NZ - 1) = 48, 64, 80, 96 or 128, the sine
+// transform z solve, and the split-y choice (ehd_tuning.poisson_path = 0)
+template <typename R>
+static bool yz_usable(const PoissonArgs &a) {
+    const int L = 2 * (a.nz - 1);
+    return a.split && a.twz && (a.ny == 48 || a.ny == 80 || a.ny == 96) &&
+           (L == 48 || L == 64 || L == 80 || L == 96 || L == 128);
+}
+template <typename R, int NY>
+static cudaError_t prepare_yz_n(int L) {
+    switch (L) {
+        case 48: return allow_max_dynamic_smem(poisson_yz<R, NY, 48>);
+        case 64: return allow_max_dynamic_smem(poisson_yz<R, NY, 64>);
+        case 80: return allow_max_dynamic_smem(poisson_yz<R, NY, 80>);
+        case 96: return allow_max_dynamic_smem(poisson_yz<R, NY, 96>);
+        default: return allow_max_dynamic_smem(poisson_yz<R, NY, 128>);
+    }
+}
+
 // ---- split-y path ----
 
 template <typename R, int N, int S>
@@ -1720,6 +1963,12 @@ cudaError_t prepare_poisson(const PoissonArgs &a) {
     if (e == cudaSuccess) e = prepare_fast<R>(a.nx);
     if (e == cudaSuccess) e = prepare_fast<R>(a.ny);
     if (e == cudaSuccess) e = prepare_fast<R>(2 * (a.nz - 1));
+    if (e == cudaSuccess && a.twz && (a.ny == 48 || a.ny == 80 || a.ny == 96)) {
+        const int L = 2 * (a.nz - 1);
+        if (L == 48 || L == 64 || L == 80 || L == 96 || L == 128)
+            e = a.ny == 48 ? prepare_yz_n<R, 48>(L)
+                           : (a.ny == 80 ? prepare_yz_n<R, 80>(L) : prepare_yz_n<R, 96>(L));
+    }
     if (e != cudaSuccess || !poisson_split_usable<R>(a)) return e;
     const int L = 2 * (a.nz - 1);
     switch (a.ny / 64) {
@@ -1745,6 +1994,10 @@ cudaError_t launch_poisson(const PoissonArgs &a, cudaStream_t s) {
         }
     }
     if ((e = rows_fwd<R>(a, s)) != cudaSuccess) return e;
+    if (yz_usable<R>(a)) {
+        if ((e = yz_all<R>(a, s)) != cudaSuccess) return e;
+        return rows_inv<R>(a, s);
+    }
     if ((e = cols<R, -1>(a, s)) != cudaSuccess) return e;
     if (a.twz && poisson_fast_size(2 * (a.nz - 1))) {
         switch (2 * (a.nz - 1)) {

@@ -222,6 +222,39 @@ def test_poisson_split_path_matches_oracle_and_five_kernel_path(shape, prec, tol
         assert relerr(out[0][k], out[1][k]) < tol, (k, "five-kernel", relerr(out[0][k], out[1][k]))
 
 
+@pytest.mark.parametrize("shape", [(96, 96, 49), (80, 80, 41), (48, 48, 25), (64, 96, 65),
+                                   (122, 80, 33)])
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("fp32", 2e-6)])
+def test_fused_yz_path_matches_oracle_and_five_kernel_path(shape, prec, tol):
+    """For NY = 48, 80 or 96 (the T-sweep grids, which the split-y path does
+    not take) and L = 2 (NZ - 1) a compile-time size, one kernel does the y
+    transform, the sine-transform z solve and the inverse y transform of
+    every kx column block (poisson_yz); against the oracle's odd-extension DFT
+    solve (poisson.cu:78-167) and the five-kernel path (ehd_tuning.poisson_path
+    = 1) on random charge, with a run-time-radix x transform in the last case
+    (122 = 2 x 61)."""
+    nx, ny, nz = shape
+    dz = 1.0 / (nz - 1)
+    p = O.params_from_groups(nx, ny, nz, nx * dz, ny * dz, T=200, M=10, C=10, Fe=4000)
+    f = random_fields(p, 6)
+    o = O.Oracle(p)
+    o.set_fields(f)
+    o.poisson()
+    o.efield()
+    b = o.get_fields()
+    o.close()
+    out = {}
+    for path in (0, 1):
+        with ehd.Simulation(to_ehd(p), prec) as sim:
+            sim.set_tuning(poisson_path=path)
+            sim.set_fields(f)
+            sim.poisson()
+            out[path] = sim.get_fields()
+    for k in ("phi", "ex", "ey", "ez"):
+        assert relerr(out[0][k], b[k]) < tol, (k, "oracle", relerr(out[0][k], b[k]))
+        assert relerr(out[0][k], out[1][k]) < tol, (k, "five-kernel", relerr(out[0][k], out[1][k]))
+
+
 @pytest.mark.parametrize("shape", [(48, 40, 27), (122, 122, 101), (30, 25, 7)])
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("fp32", 2e-6)])
 def test_z_solve_choices_match_oracle(shape, prec, tol):
