@@ -467,23 +467,30 @@ namespace {
 
 // average time of one batch step over `steps` steps of every instance (after
 // one untimed step, which also captures a new graph if the shapes changed)
+// The time of one batch step: the best of three runs of `steps` steps after a
+// warm-up step (the shortest run is the one least disturbed).
 int time_batch(ehd_batch *b, const std::vector<char> &act, int steps, float *ms) {
     int r = batch_step(b, act, 1);
     if (r != EHD_OK) return r;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    cudaEventRecord(e0, b->stream);
-    r = batch_step(b, act, steps);
-    cudaEventRecord(e1, b->stream);
-    cudaError_t e = cudaEventSynchronize(e1);
-    float t = 0.f;
-    if (r == EHD_OK && e == cudaSuccess) cudaEventElapsedTime(&t, e0, e1);
+    float best = 0.f;
+    cudaError_t e = cudaSuccess;
+    for (int rep = 0; rep < 3 && r == EHD_OK && e == cudaSuccess; ++rep) {
+        cudaEventRecord(e0, b->stream);
+        r = batch_step(b, act, steps);
+        cudaEventRecord(e1, b->stream);
+        e = cudaEventSynchronize(e1);
+        float t = 0.f;
+        if (r == EHD_OK && e == cudaSuccess) cudaEventElapsedTime(&t, e0, e1);
+        if (rep == 0 || t < best) best = t;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (r != EHD_OK) return r;
     if (e != cudaSuccess) return cuda_fail("autotune timing", e);
-    *ms = t / (float)steps;
+    *ms = best / (float)steps;
     return EHD_OK;
 }
 
@@ -517,7 +524,12 @@ int ehd_batch_autotune(ehd_batch *b, int trial_steps) {
     if (r == EHD_OK) r = batch_step(s, all, 1);
     float best_ms = 0.f;
     if (r == EHD_OK) r = time_batch(s, all, trial_steps, &best_ms);
-    std::vector<ehd_tuning> choice;
+    std::vector<ehd_tuning> choice, start;
+    for (auto &g : groups) {
+        ehd_tuning t{};
+        ehd_get_tuning(s->inst[g.second.front()], &t);
+        start.push_back(t);
+    }
     for (auto &g : groups) {
         if (r != EHD_OK) break;
         ehd_tuning best{};
@@ -574,6 +586,24 @@ int ehd_batch_autotune(ehd_batch *b, int trial_steps) {
                 if (cols != best.fft_cols) r = trial(t);
             }
         choice.push_back(best);
+    }
+    // coordinate descent over the grids can end worse than where it began
+    // (the grids' best shapes depend on one another): keep the starting
+    // shapes unless the final choice beats them
+    if (r == EHD_OK) {
+        auto apply_all = [&](const std::vector<ehd_tuning> &ts) {
+            size_t k = 0;
+            for (auto &g : groups) {
+                for (int i : g.second)
+                    if (ehd_set_tuning(s->inst[i], &ts[k]) != EHD_OK) return false;
+                ++k;
+            }
+            return true;
+        };
+        float chosen_ms = 0.f, start_ms = 0.f;
+        if (apply_all(choice)) r = time_batch(s, all, trial_steps, &chosen_ms);
+        if (r == EHD_OK && apply_all(start)) r = time_batch(s, all, trial_steps, &start_ms);
+        if (r == EHD_OK && start_ms > 0.f && start_ms <= chosen_ms) choice = start;
     }
     ehd_batch_destroy(s);
     if (r != EHD_OK) return r;

@@ -1049,15 +1049,24 @@ static StepArgs<T, R> make_step_args(const LbmArgs &la, const StepConst &c) {
 // constants (about 1.3 KB) into shared memory and runs the same node_block as
 // lbm_step_kernel, so an instance's result is bitwise that of a lone context
 // on the per-node kernel with the default block shape.
+// planes per block of the per-node group kernel
+constexpr int kGroupPlanes = 4;
+
 template <typename T, typename R, bool MACROS>
 __global__ void __launch_bounds__(128, sizeof(R) == 8 ? 2 : 4)
-lbm_group_kernel(const LbmGroupDesc<T, R> *__restrict__ desc, int nz) {
+lbm_group_kernel(const LbmGroupDesc<T, R> *__restrict__ desc, int nz, int zpb) {
+    // blockIdx.z: instance and a run of zpb consecutive planes, so that a
+    // block's copy of the instance's arguments serves several planes
     __shared__ LbmGroupDesc<T, R> sd;
-    const int inst = blockIdx.z / nz, z = blockIdx.z - inst * nz;
+    const int runs = (nz + zpb - 1) / zpb;
+    const int inst = blockIdx.z / runs, z0 = (blockIdx.z - inst * runs) * zpb;
     load_group_desc(sd, desc, inst);
     __syncthreads();
-    node_block<T, R, false, MACROS>(sd.a, sd.k, blockIdx.x, blockIdx.y, z, gridDim.x, gridDim.y,
-                                    0, 0);
+    const int z1 = z0 + zpb < nz ? z0 + zpb : nz;
+#pragma unroll 1
+    for (int z = z0; z < z1; ++z)
+        node_block<T, R, false, MACROS>(sd.a, sd.k, blockIdx.x, blockIdx.y, z, gridDim.x,
+                                        gridDim.y, 0, 0);
 }
 
 template <typename T, typename R>
@@ -1076,10 +1085,11 @@ template <typename T, typename R>
 cudaError_t launch_lbm_group(const void *desc_dev, int n, int nx, int ny, int nz, int bx,
                              bool macros, cudaStream_t s) {
     const dim3 block(bx, 128 / bx, 1);
-    const dim3 grid((nx + bx - 1) / bx, (ny + block.y - 1) / block.y, nz * n);
+    const dim3 grid((nx + bx - 1) / bx, (ny + block.y - 1) / block.y,
+                    (nz + kGroupPlanes - 1) / kGroupPlanes * n);
     const auto *d = reinterpret_cast<const LbmGroupDesc<T, R> *>(desc_dev);
-    if (macros) lbm_group_kernel<T, R, true><<<grid, block, 0, s>>>(d, nz);
-    else lbm_group_kernel<T, R, false><<<grid, block, 0, s>>>(d, nz);
+    if (macros) lbm_group_kernel<T, R, true><<<grid, block, 0, s>>>(d, nz, kGroupPlanes);
+    else lbm_group_kernel<T, R, false><<<grid, block, 0, s>>>(d, nz, kGroupPlanes);
     return cudaGetLastError();
 }
 
@@ -1092,8 +1102,8 @@ cudaError_t launch_lbm_rows_group(const void *desc_dev, int n, int nx, int ny, i
     const auto *d = reinterpret_cast<const LbmGroupDesc<T, R> *>(desc_dev);
     const int bx = z0_block_x(nx);
     const dim3 g0((nx + bx - 1) / bx, ny, n);
-    if (macros) lbm_group_kernel<T, R, true><<<g0, bx, 0, s>>>(d, 1);
-    else lbm_group_kernel<T, R, false><<<g0, bx, 0, s>>>(d, 1);
+    if (macros) lbm_group_kernel<T, R, true><<<g0, bx, 0, s>>>(d, 1, 1);
+    else lbm_group_kernel<T, R, false><<<g0, bx, 0, s>>>(d, 1, 1);
     const size_t sm = lbm_rows_smem(nx, sizeof(typename PopT<T>::F), sizeof(typename PopT<T>::G));
     const dim3 g1(per_inst, n, 1);
     rows_group_kernel<T, R>(macros, nx % 32 != 0)<<<g1, rows_block_x(nx), sm, s>>>(d);

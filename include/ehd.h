@@ -295,12 +295,14 @@ int ehd_batch_step(ehd_batch *batch, int nsteps);
 int ehd_batch_run_to_saturation(ehd_batch *batch, int sample_every, double tol, int hold,
                                 int64_t max_steps, int32_t *saturated, int64_t *steps,
                                 double *nu_e);
-/* Autotuner: times batch steps (trial_steps each) of a scratch batch with
- * the same parameters while it varies, one distinct grid at a time, the
- * launch shapes of that grid's instances (row or per-node kernel, per-node
- * block, run-time-radix FFT batches), keeps what is faster, and applies the
- * result to every instance of that grid (ehd_get_tuning reads the choice).
- * The instances' states are not touched. */
+/* Autotuner: times batch steps (the best of three runs of trial_steps each)
+ * of a scratch batch with the same parameters and mode while it varies, one
+ * distinct grid at a time, the launch shapes of that grid's instances (row or
+ * per-node kernel, per-node block, Poisson path, z solve, run-time-radix FFT
+ * batches), keeps a change that saves more than 1 %, keeps the starting
+ * shapes if the final choice is not faster than them, and applies the result
+ * to every instance of that grid (ehd_get_tuning reads the choice).  The
+ * instances' states are not touched. */
 int ehd_batch_autotune(ehd_batch *batch, int trial_steps);
 
 /* The context's launch shapes (defaults chosen at ehd_create) and a change
