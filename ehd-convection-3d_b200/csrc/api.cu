@@ -602,7 +602,11 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
     // available beside the run-time sine transform (ehd_tuning.z_solve)
     const bool thomas = !poisson_fast_size(lz2);
     double *cpt = nullptr;
-    void *twz = nullptr;
+    void *twz = nullptr, *cps = nullptr;
+    const bool split = poisson_split_grid(nx, ny, nz, c->rsize);
+    if (split) {
+        if ((r = dalloc(c, &cps, c->rsize * nmodes * (size_t)((nz - 1) / 2)))) return bail(r);
+    }
     if (zdst) {
         if ((r = dalloc(c, &twz, c->rsize * (size_t)(2 * lz2 + lz2 / 2 + 1)))) return bail(r);
     }
@@ -616,6 +620,7 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
     pa.lx = params->lx;
     pa.ly = params->ly;
     pa.cpt = cpt;
+    pa.cps = cps;
     pa.phi00 = c->phi00;
     pa.ez00 = c->ez00;
     pa.q = c->q;
@@ -662,21 +667,52 @@ int ehd_create(const ehd_params *params, const ehd_config *config, ehd_ctx **out
                 EHD_CK(cudaMemcpy(twz, tf.data(), sizeof(float) * tf.size(), cudaMemcpyHostToDevice));
             }
         }
+        // Thomas pivots per mode (kx, ky): beta = 2 + (kx^2 + ky^2) dz^2 with
+        // the wavenumbers of main.cu:110-129, cp_0 = -1/beta,
+        // cp_i = 1/(-beta - cp_{i-1})
+        std::vector<double> hx(pa.nxh), hy(ny);
+        for (int i = 0; i < pa.nxh; ++i) {
+            const double k = (double)i * 2.0 * M_PI / params->lx;
+            hx[i] = k * k;
+        }
+        for (int j = 0; j < ny; ++j) {
+            const double k = (j <= ny / 2 ? (double)j : (double)j - ny) * 2.0 * M_PI / params->ly;
+            hy[j] = k * k;
+        }
+        const int n = nz - 2;
+        const double dz2 = params->dz * params->dz;
+        if (split) {
+            // the split-y slab kernel's two-sided table, layout [kx][j][r][k']
+            // with ky = S k' + j, in the compute type: for n = NZ - 2 (odd)
+            // interior planes, c_0..c_{m-1} (m = (n - 1)/2, the pivots of
+            // either half) and mu = 1/(-beta - 2 c_{m-1}) (the middle plane)
+            const int S = ny / 64, m = (n - 1) / 2;
+            std::vector<double> cp(nmodes * (size_t)(m + 1));
+            size_t o = 0;
+            for (int i = 0; i < pa.nxh; ++i)
+                for (int j = 0; j < S; ++j) {
+                    double prev[64];
+                    for (int kp = 0; kp < 64; ++kp) prev[kp] = 0.0;
+                    for (int z = 0; z <= m; ++z)
+                        for (int kp = 0; kp < 64; ++kp) {
+                            const double beta = 2.0 + (hx[i] + hy[S * kp + j]) * dz2;
+                            if (z < m) {
+                                prev[kp] = 1.0 / (-beta - prev[kp]);
+                                cp[o++] = prev[kp];
+                            } else {
+                                cp[o++] = 1.0 / (-beta - 2.0 * prev[kp]);
+                            }
+                        }
+                }
+            if (c->rsize == 8) {
+                EHD_CK(cudaMemcpy(cps, cp.data(), sizeof(double) * cp.size(), cudaMemcpyHostToDevice));
+            } else {
+                std::vector<float> cf(cp.begin(), cp.end());
+                EHD_CK(cudaMemcpy(cps, cf.data(), sizeof(float) * cf.size(), cudaMemcpyHostToDevice));
+            }
+        }
         if (thomas) {
-            // Thomas pivots per mode (kx, ky): beta = 2 + (kx^2 + ky^2) dz^2 with
-            // the wavenumbers of main.cu:110-129, cp_0 = -1/beta,
-            // cp_i = 1/(-beta - cp_{i-1}); layout [i][ky*nxh + kx].
-            std::vector<double> hx(pa.nxh), hy(ny);
-            for (int i = 0; i < pa.nxh; ++i) {
-                const double k = (double)i * 2.0 * M_PI / params->lx;
-                hx[i] = k * k;
-            }
-            for (int j = 0; j < ny; ++j) {
-                const double k = (j <= ny / 2 ? (double)j : (double)j - ny) * 2.0 * M_PI / params->ly;
-                hy[j] = k * k;
-            }
-            const int n = nz - 2;
-            const double dz2 = params->dz * params->dz;
+            // layout [i][ky*nxh + kx]
             std::vector<double> cp(nmodes * (size_t)n);
             for (int j = 0; j < ny; ++j)
                 for (int i = 0; i < pa.nxh; ++i) {

@@ -137,15 +137,18 @@ int build_group(ehd_batch *b, const std::vector<size_t> &members, bool macros,
 template <typename T, typename R>
 int capture_groups(ehd_batch *b, const std::vector<char> &act, bool macros,
                    std::vector<void *> &bufs, cudaGraph_t *graph) {
-    // instances with the same grid and launch shapes form one group
-    std::map<std::vector<int>, std::vector<size_t>> groups;
+    // instances with the same grid, domain, spacing, permittivity, voltage
+    // and launch shapes form one group (the group's Poisson launches take
+    // their tables and those constants from its first member)
+    std::map<std::vector<double>, std::vector<size_t>> groups;
     for (size_t i = 0; i < b->inst.size(); ++i) {
         if (!act[i]) continue;
         const ehd_params *p = ctx_params(b->inst[i]);
         ehd_tuning t{};
         ctx_tuning(b->inst[i], &t);
-        groups[{p->nx, p->ny, p->nz, t.lbm_kernel, t.node_block_x, t.fft_rows, t.fft_cols,
-                t.poisson_path, t.z_solve}]
+        groups[{(double)p->nx, (double)p->ny, (double)p->nz, p->lx, p->ly, p->dz, p->eps,
+                p->voltage, (double)t.lbm_kernel, (double)t.node_block_x, (double)t.fft_rows,
+                (double)t.fft_cols, (double)t.poisson_path, (double)t.z_solve}]
             .push_back(i);
     }
     std::vector<Group> gl;

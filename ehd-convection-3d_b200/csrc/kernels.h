@@ -158,6 +158,9 @@ struct PoissonArgs {
                              // (L/2 + 1 real); nullptr: Thomas solve
     double lx, ly;           // domain lengths (wavenumbers 2 pi k / l)
     const double *cpt;       // Thomas pivots [z-1][ky*nxh + kx], FP64
+    const void *cps;         // split-y path: two-sided Thomas pivots [kx][j][r][k'] (ky = S k' + j,
+                             // NY = 64 S; r < (NZ - 1)/2: c_r, then the middle plane's mu)
+                             // in the compute type; nullptr: no split path
     double2 *dpw;            // FP64 scratch of the forward sweep, same layout
     void *spec;              // complex compute type
     double *rowsum;          // [z-1][y] FP64 sums of the source
@@ -179,6 +182,9 @@ template <typename R>
 cudaError_t prepare_poisson(const PoissonArgs &a);
 
 bool poisson_fast_size(int n);
+// whether the split-y path serves a grid in the compute type of rsize bytes
+// (the context then builds its pivot table, PoissonArgs::cps)
+bool poisson_split_grid(int nx, int ny, int nz, size_t rsize);
 // shared memory of the run-time-radix sine-transform z solve with tb modes
 // per block (compute type of rsize bytes)
 size_t zdst_rt_smem(int L, int tb, size_t rsize);

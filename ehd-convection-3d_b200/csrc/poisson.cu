@@ -983,8 +983,9 @@ poisson_zdst_rt(typename Cplx<R>::T *__restrict__ spec, const typename Cplx<R>::
 // (W_N = exp(-2 pi i / N)).  The x-row kernels form a_j (after the forward x
 // transform) and consume b_j (before the inverse one); in between one slab
 // kernel per (kx, j) holds a_j for every plane z on chip and runs the forward
-// FFT64 along n, the sine-transform z solve of each of its 64 modes, and the
-// inverse FFT64, so the spectrum goes through L2 twice instead of four times.
+// FFT64 along n, the tridiagonal (Thomas) z solve of each of its 64 modes, and
+// the inverse FFT64, so the spectrum goes through L2 twice instead of four
+// times.
 // The split spectrum is laid out [j][kx][z - 1][n], so that a slab is one
 // contiguous block.
 namespace {
@@ -1137,43 +1138,61 @@ poisson_rows_fwd_split(const R *__restrict__ q, typename Cplx<R>::T *__restrict_
     }
 }
 
-// dynamic shared memory of the slab kernel: the FFT64 and z twiddles, the
-// output twiddles, the slab and the z-transform buffers of the 8 warps
+// pivot rows of a mode in the split path's table: the two-sided Thomas
+// solve of n = L/2 - 1 (odd) planes eliminates (n - 1)/2 planes from each
+// electrode with the same pivots c_0..c_{m-1}, then the middle plane with
+// mu = 1/(-beta - 2 c_{m-1})
+template <int L> constexpr int slab_piv_rows() { return (L / 2 - 1 + 1) / 2; }
+// dynamic shared memory of the slab kernel: the FFT64 twiddles, the output
+// twiddles, the block's pivot rows [r][k'] and the slab
 template <typename R, int L>
 constexpr size_t slab_smem() {
-    constexpr int TPW = 32 / fft::WPlan<L>::G;
-    return sizeof(typename Cplx<R>::T) * ((size_t)128 + L + (size_t)slab_rows<L>() * tstride<64>() +
-                                          (size_t)8 * TPW * tstride<L>());
+    return sizeof(typename Cplx<R>::T) * ((size_t)128 + (size_t)slab_rows<L>() * tstride<64>()) +
+           sizeof(R) * (size_t)slab_piv_rows<L>() * 64;
 }
-// two resident blocks per SM where their shared memory allows, which caps
-// the registers at 128 a thread; one block (and up to 255 registers) otherwise
-// and for the FP64 transforms longer than 64, which spill under that cap
+// resident blocks per SM that their shared memory allows (two at most)
 template <typename R, int L>
 constexpr int slab_min_blocks() {
-    return 2 * slab_smem<R, L>() + 4096 <= 227 * 1024 && (sizeof(R) == 4 || L == 64) ? 2 : 1;
+    return 2 * slab_smem<R, L>() + 4096 <= 227 * 1024 ? 2 : 1;
+}
+
+// 16-byte asynchronous copy global -> shared (cp.async), and the wait for all
+// of a thread's copies
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
 }
 
 // K2 of the split path, one block per (kx, j): the slab a_j[z - 1][n] of all
 // interior planes in shared memory; FFT64 along n (ky = S k' + j), the
-// sine-transform z solve of each of the 64 modes (as poisson_zdst: odd
-// extension of length L = 2 (NZ - 1), forward FFT, division by
-// lambda_k + h dz^2, forward FFT), inverse FFT64, the twiddle W_NY^(-j n),
-// written back in place as b_j.  Every transform is warp-synchronous (fft::WPlan): the rows n of a plane are
-// transformed on their way in from global memory and on their way out, the
-// odd extension is gathered from the slab's column by the first pass and the
-// division applied by the last, so the block synchronises only between the
-// three phases.  The block (kx, j) = (0, 0) also forms the FP64 plane sums of
-// the source and solves the (0,0) mode in closed form (as poisson_zdst),
-// writing phi00 and its Ez.
+// tridiagonal z solve of each of the 64 modes, inverse FFT64, the twiddle
+// W_NY^(-j n), written back in place as b_j.  The z solve is the system of
+// poisson_zsolve, phi(z-1) - beta phi(z) + phi(z+1) = dz^2 s(z),
+// beta = 2 + (kx^2 + ky^2) dz^2, phi = 0 on the electrodes, solved from both
+// ends at once in FP64 arithmetic: one thread eliminates the upper half of the
+// planes downwards and one the lower half upwards with the same pivots (the
+// matrix is symmetric Toeplitz), they meet at the middle plane, and each
+// substitutes back over its half.  The pivots come from the table built once
+// per context, in the compute type.  The 64-point
+// transforms are warp-synchronous (fft::WPlan): the rows n of a plane are
+// transformed on their way in from global memory and on their way out, so the
+// block synchronises only between the three phases; the block's pivots
+// arrive by cp.async during the first.  Block x = 0 of y = 0 (one more block
+// than kx columns) forms the FP64 plane sums of the source and solves the
+// (0,0) mode in closed form (as poisson_zdst), writing phi00 and its Ez, on
+// its own beside the slabs; the (0,0) mode of the fluctuation is 0.
 template <typename R, int L, int S>
 __global__ void __launch_bounds__(256, slab_min_blocks<R, L>())
 poisson_slab(typename Cplx<R>::T *__restrict__ spl, const typename Cplx<R>::T *__restrict__ twy,
-             const typename Cplx<R>::T *__restrict__ twz, const R *__restrict__ lamz,
-             const double *__restrict__ rowsum, double *__restrict__ planesum,
-             const double *__restrict__ qmean, double *__restrict__ phi00,
-             double *__restrict__ ez00, int nx, int nxh, double dz, double eps,
-             double voltage, double kx0, double ky0,
-    const PoissonPtrs *__restrict__ grp) {
+             const R *__restrict__ cps, const double *__restrict__ rowsum,
+             double *__restrict__ planesum, const double *__restrict__ qmean,
+             double *__restrict__ phi00, double *__restrict__ ez00, int nx, int nxh, double dz,
+             double eps, double voltage, const PoissonPtrs *__restrict__ grp) {
     if (grp) {  // one instance of a group launch per blockIdx.z
         const PoissonPtrs &gp = grp[blockIdx.z];
         spl = (typename Cplx<R>::T *)gp.spec;
@@ -1186,49 +1205,41 @@ poisson_slab(typename Cplx<R>::T *__restrict__ spl, const typename Cplx<R>::T *_
     using R2 = typename Cplx<R>::T;
     constexpr int NY = 64 * S;
     constexpr int n = L / 2 - 1, nz = n + 2;
-    constexpr int P64 = tstride<64>(), PL = tstride<L>();
-    constexpr int NR = slab_rows<L>();     // slab rows, whole rounds of 32
-    constexpr int GZ = fft::WPlan<L>::G;   // threads per z transform
-    constexpr int TPW = 32 / GZ;           // z transforms per warp
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    R2 *tw64 = reinterpret_cast<R2 *>(smem_raw);
-    R2 *twj = tw64 + 64;  // conj W_NY^(j n), n < 64
-    R2 *twl = twj + 64;
-    R2 *slab = twl + L;
-    R2 *zb = slab + NR * P64;
-    __shared__ double mrhs[n], mphi[nz];
+    constexpr int P64 = tstride<64>();
+    constexpr int NR = slab_rows<L>();  // slab rows, whole rounds of 32
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int kx = blockIdx.x, j = blockIdx.y;
-    const bool mean_block = kx == 0 && j == 0;
     const double dz2 = dz * dz;
-    R2 *base = spl + ((size_t)j * nxh + kx) * n * 64;
-    for (int i = tid; i < 64; i += 256) {
-        tw64[i] = twy[S * i];
-        R2 w = twy[(j * i) % NY];
-        w.y = -w.y;
-        twj[i] = w;
-    }
-    for (int i = tid; i < L; i += 256) twl[i] = twz[i];
-    if (mean_block) {
+    if (blockIdx.x == 0) {
+        if (blockIdx.y != 0) return;
+        __shared__ double mrhs[n], mphi[nz];
         // FP64 plane sums of the source (fixed order), then the right-hand
         // side of the mean mode (poisson.cu:97 for the voltage on z = 1); the
-        // row sums of four planes in flight at a time (this block is the
-        // longest of the launch otherwise)
+        // row sums of four planes in flight at a time, in chunks of up to
+        // four rows a lane
         const double nxy = (double)nx * (double)NY;
-        constexpr int PW = 4, YL = NY / 32;
+        constexpr int PW = 4, YL = NY / 32, YC = YL < 4 ? YL : 4;
         for (int z0 = warp * PW; z0 < n; z0 += 8 * PW) {
-            double v[PW][YL];
+            double acc[PW];
 #pragma unroll
-            for (int u = 0; u < PW; ++u)
+            for (int u = 0; u < PW; ++u) acc[u] = 0.0;
+#pragma unroll 1
+            for (int t0 = 0; t0 < YL; t0 += YC) {
+                double v[PW][YC];
 #pragma unroll
-                for (int t = 0; t < YL; ++t)
-                    v[u][t] = z0 + u < n ? rowsum[(size_t)(z0 + u) * NY + lane + 32 * t] : 0.0;
+                for (int u = 0; u < PW; ++u)
+#pragma unroll
+                    for (int t = 0; t < YC; ++t)
+                        v[u][t] = z0 + u < n ? rowsum[(size_t)(z0 + u) * NY + lane + 32 * (t0 + t)]
+                                             : 0.0;
+#pragma unroll
+                for (int u = 0; u < PW; ++u)
+#pragma unroll
+                    for (int t = 0; t < YC; ++t) acc[u] += v[u][t];
+            }
 #pragma unroll
             for (int u = 0; u < PW; ++u) {
                 const int zi = z0 + u;
-                double sum = 0.0;
-#pragma unroll
-                for (int t = 0; t < YL; ++t) sum += v[u][t];
+                double sum = acc[u];
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
                 if (lane == 0 && zi < n) {
@@ -1239,75 +1250,7 @@ poisson_slab(typename Cplx<R>::T *__restrict__ spl, const typename Cplx<R>::T *_
                 }
             }
         }
-    }
-    __syncthreads();
-    // phase 1: forward FFT64 of each plane's row on its way in, 4 rows a warp
-    const int g8 = lane >> 3, t8 = lane & 7;
-#pragma unroll 1
-    for (int zi = warp * 4 + g8; zi < NR; zi += 32) {
-        const bool act = zi < n;
-        const R2 *src = base + (size_t)zi * 64;
-        R2 *row = slab + zi * P64;
-        fft::WPlan<64>::template run<-1>(
-            row, tw64, opaque(t8), [&](int m) { return act ? src[m] : R2{(R)0, (R)0}; },
-            [&](int m, R2 v) { row[fft::pad(m)] = v; });
-    }
-    __syncthreads();
-    // phase 2: z solve of the modes k', TPW per warp
-    {
-        const R sc = (R)(dz2 / (double)L);
-        const int g = lane / GZ, t0 = lane - g * GZ;
-        R2 *zw = zb + (warp * TPW + g) * PL;
-#pragma unroll 1
-        for (int kp = warp * TPW + g; kp < 64; kp += 8 * TPW) {
-            const int t = opaque(t0);
-            const int ky = S * kp + j;
-            const double wx = kx * kx0, wy = (ky <= NY / 2 ? ky : ky - NY) * ky0;
-            const R h = (kx == 0 && ky == 0) ? (R)-1 : (R)((wx * wx + wy * wy) * dz2);
-            R2 *col = slab + fft::pad(kp);
-            // odd extension x[m] = s[m], x[L - m] = -s[m] (m = 1..n), x[0] = x[L/2] = 0
-            auto ld = [&](int m) {
-                const bool up = m < L / 2;
-                const R2 v = col[(up ? (m > 0 ? m - 1 : 0) : L - 1 - m) * P64];
-                return (m == 0 || m == L / 2) ? R2{(R)0, (R)0} : (up ? v : R2{-v.x, -v.y});
-            };
-            auto div = [&](int k, R2 v) {
-                if (k == 0 || k == L / 2 || h < (R)0) return R2{(R)0, (R)0};
-                const R f = rcp(lamz[k < L / 2 ? k : L - k] + h);
-                return R2{v.x * f, v.y * f};
-            };
-            auto st = [&](int m, R2 v) {
-                if (m >= 1 && m <= n) col[(m - 1) * P64] = R2{v.x * sc, v.y * sc};
-            };
-            // both transforms forward, as poisson_zdst: the sign of the
-            // solution follows from the two factors -2i of the odd extension
-            if constexpr (L == 64 || L == 256) {
-                fft::wfilter_sq<L, GZ, -1, -1>(zw, twl, t, ld, div, st);
-            } else {
-                fft::WPlan<L>::template run<-1>(zw, twl, t, ld,
-                                                [&](int k, R2 v) { zw[fft::pad(k)] = div(k, v); });
-                __syncwarp();
-                fft::WPlan<L>::template run<-1>(zw, twl, opaque(t0),
-                                                [&](int m) { return zw[fft::pad(m)]; }, st);
-                __syncwarp();
-            }
-        }
-    }
-    __syncthreads();
-    // phase 3: inverse FFT64 of each row and the twiddle on the way out
-#pragma unroll 1
-    for (int zi = warp * 4 + g8; zi < NR; zi += 32) {
-        const bool act = zi < n;
-        R2 *dst = base + (size_t)zi * 64;
-        R2 *row = slab + zi * P64;
-        fft::WPlan<64>::template run<1>(
-            row, tw64, opaque(t8), [&](int m) { return row[fft::pad(m)]; },
-            [&](int m, R2 v) {
-                if (act) dst[m] = j * m != 0 ? cmul(v, twj[m]) : v;
-            });
-    }
-    if (mean_block) {
-        const double nxy = (double)nx * (double)NY;
+        __syncthreads();
         for (int i = tid; i < nz; i += 256) {
             double x = 0.0;
             if (i == 0) {
@@ -1327,6 +1270,134 @@ poisson_slab(typename Cplx<R>::T *__restrict__ spl, const typename Cplx<R>::T *_
             const int zc = z < 1 ? 1 : (z > nz - 2 ? nz - 2 : z);
             ez00[z] = 0.5 * (mphi[zc - 1] - mphi[zc + 1]) / dz;
         }
+        return;
+    }
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *tw64 = reinterpret_cast<R2 *>(smem_raw);
+    R2 *twj = tw64 + 64;  // conj W_NY^(j n), n < 64
+    R *piv = reinterpret_cast<R *>(twj + 64);
+    R2 *slab = reinterpret_cast<R2 *>(piv + slab_piv_rows<L>() * 64);
+    const int kx = blockIdx.x - 1, j = blockIdx.y;
+    R2 *base = spl + ((size_t)j * nxh + kx) * n * 64;
+    {
+        // the block's pivot rows [r][k'], contiguous in the table
+        constexpr int PR = slab_piv_rows<L>(), V = 16 / sizeof(R), NV = PR * 64 / V;
+        const R *src = cps + ((size_t)kx * S + j) * PR * 64;
+        for (int i = tid; i < NV; i += 256) cp_async16(piv + V * i, src + V * i);
+    }
+    for (int i = tid; i < 64; i += 256) {
+        tw64[i] = twy[S * i];
+        R2 w = twy[(j * i) % NY];
+        w.y = -w.y;
+        twj[i] = w;
+    }
+    __syncthreads();
+    // phase 1: forward FFT64 of each plane's row on its way in, 4 rows a
+    // warp; each thread's inputs t8 + 8 r of the next round's row are loaded
+    // while this round's row is transformed (the first pass takes its inputs
+    // in that order)
+    const int g8 = lane >> 3, t8 = lane & 7;
+    R2 cur[8];
+    {
+        const int zi = warp * 4 + g8;
+        const R2 *src = base + (size_t)zi * 64;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) cur[r] = zi < n ? src[t8 + 8 * r] : R2{(R)0, (R)0};
+    }
+#pragma unroll 1
+    for (int zi = warp * 4 + g8; zi < NR; zi += 32) {
+        const int zn = zi + 32;
+        const R2 *srcn = base + (size_t)zn * 64;
+        R2 nxt[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) nxt[r] = zn < n ? srcn[t8 + 8 * r] : R2{(R)0, (R)0};
+        R2 *row = slab + zi * P64;
+        int c = 0;
+        fft::WPlan<64>::template run<-1>(
+            row, tw64, opaque(t8), [&](int) { return cur[c++]; },
+            [&](int m, R2 v) { row[fft::pad(m)] = v; });
+#pragma unroll
+        for (int r = 0; r < 8; ++r) cur[r] = nxt[r];
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // phase 2: the two-sided Thomas solve of the 64 modes k', 16 modes a warp:
+    // lanes 0-15 take the planes 0..m-1 from the top, lanes 16-31 the planes
+    // n-1..n-m from the bottom; loads issued kB planes ahead of the chain
+    static_assert(n % 2 == 1, "odd number of interior planes");
+    if (tid < 128) {
+        constexpr int m = (n - 1) / 2, kB = 8;
+        const int kp = (warp << 4) | (lane & 15), side = lane >> 4;
+        R2 *col = slab + fft::pad(kp);
+        const R *pc = piv + kp;
+        // plane of elimination step k on this side
+        auto plane = [&](int k) { return side ? n - 1 - k : k; };
+        // the (0,0) mode is solved like the others (every lane takes part in
+        // the exchange) and stored as 0
+        const R keep = (kx == 0 && S * kp + j == 0) ? (R)0 : (R)1;
+        {
+            double dr = 0.0, di = 0.0;
+#pragma unroll 1
+            for (int k0 = 0; k0 < m; k0 += kB) {
+                R2 sv[kB];
+                R cv[kB];
+#pragma unroll
+                for (int u = 0; u < kB; ++u) {
+                    const int k = k0 + u < m ? k0 + u : m - 1;
+                    sv[u] = col[plane(k) * P64];
+                    cv[u] = pc[k * 64];
+                }
+#pragma unroll
+                for (int u = 0; u < kB; ++u) {
+                    if (k0 + u < m) {
+                        dr = ((double)sv[u].x * dz2 - dr) * (double)cv[u];
+                        di = ((double)sv[u].y * dz2 - di) * (double)cv[u];
+                        col[plane(k0 + u) * P64] = R2{(R)dr, (R)di};
+                    }
+                }
+            }
+            // the middle plane from both sides' last eliminated rows
+            const double or_ = __shfl_xor_sync(0xffffffffu, dr, 16);
+            const double oi = __shfl_xor_sync(0xffffffffu, di, 16);
+            const R2 sm = col[m * P64];
+            const double mu = (double)pc[m * 64];
+            double xr = ((double)sm.x * dz2 - dr - or_) * mu;
+            double xi = ((double)sm.y * dz2 - di - oi) * mu;
+            __syncwarp();
+            if (side == 0) col[m * P64] = R2{(R)xr * keep, (R)xi * keep};
+#pragma unroll 1
+            for (int k1 = m - 1; k1 >= 0; k1 -= kB) {
+                R2 dv[kB];
+                R cv[kB];
+#pragma unroll
+                for (int u = 0; u < kB; ++u) {
+                    const int k = k1 - u >= 0 ? k1 - u : 0;
+                    dv[u] = col[plane(k) * P64];
+                    cv[u] = pc[k * 64];
+                }
+#pragma unroll
+                for (int u = 0; u < kB; ++u) {
+                    if (k1 - u >= 0) {
+                        xr = (double)dv[u].x - (double)cv[u] * xr;
+                        xi = (double)dv[u].y - (double)cv[u] * xi;
+                        col[plane(k1 - u) * P64] = R2{(R)xr * keep, (R)xi * keep};
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // phase 3: inverse FFT64 of each row and the twiddle on the way out
+#pragma unroll 1
+    for (int zi = warp * 4 + g8; zi < NR; zi += 32) {
+        const bool act = zi < n;
+        R2 *dst = base + (size_t)zi * 64;
+        R2 *row = slab + zi * P64;
+        fft::WPlan<64>::template run<1>(
+            row, tw64, opaque(t8), [&](int m) { return row[fft::pad(m)]; },
+            [&](int m, R2 v) {
+                if (act) dst[m] = j * m != 0 ? cmul(v, twj[m]) : v;
+            });
     }
 }
 
@@ -1841,11 +1912,10 @@ static cudaError_t split_slab(const PoissonArgs &a, cudaStream_t s) {
     constexpr size_t sm = slab_smem<R, L>();
     cudaError_t e = set_smem(poisson_slab<R, L, S>, sm, s);
     if (e != cudaSuccess) return e;
-    const R2 *tw = (const R2 *)a.twz;
-    poisson_slab<R, L, S><<<dim3(a.nxh, S, a.ngrp), 256, sm, s>>>(
-        (R2 *)a.spec, (const R2 *)a.twy, tw, (const R *)(tw + L), a.rowsum, a.planesum, a.qmean,
-        a.phi00, a.ez00, a.nx, a.nxh, a.dz, a.eps, a.voltage, 2.0 * M_PI / a.lx,
-        2.0 * M_PI / a.ly, a.grp);
+    // one block more than kx columns: block x = 0 solves the mean mode
+    poisson_slab<R, L, S><<<dim3(a.nxh + 1, S, a.ngrp), 256, sm, s>>>(
+        (R2 *)a.spec, (const R2 *)a.twy, (const R *)a.cps, a.rowsum, a.planesum, a.qmean,
+        a.phi00, a.ez00, a.nx, a.nxh, a.dz, a.eps, a.voltage, a.grp);
     return cudaGetLastError();
 }
 
@@ -1883,14 +1953,14 @@ static size_t split_slab_smem(int L) {
 }
 
 // whether the split-y path serves a grid: NX a compile-time FFT size,
-// NY = 64 S (S = 1, 2, 4, 8), the sine-transform z solve, and the slab in
-// shared memory
+// NY = 64 S (S = 1, 2, 4, 8), 2 (NZ - 1) one of the slab kernel's sizes, and
+// the slab with its pivots in shared memory
 template <typename R>
-bool poisson_split_usable(const PoissonArgs &a) {
-    if (!split_size(a.nx) || !a.twz || !split_size(2 * (a.nz - 1))) return false;
-    const int S = a.ny / 64;
-    if (a.ny % 64 != 0 || (S != 1 && S != 2 && S != 4 && S != 8)) return false;
-    const int L = 2 * (a.nz - 1);
+static bool split_grid(int nx, int ny, int nz) {
+    if (!split_size(nx) || !split_size(2 * (nz - 1))) return false;
+    const int S = ny / 64;
+    if (ny % 64 != 0 || (S != 1 && S != 2 && S != 4 && S != 8)) return false;
+    const int L = 2 * (nz - 1);
     size_t sm = 0;
     switch (S) {
         case 1: sm = split_slab_smem<R, 1>(L); break;
@@ -1899,6 +1969,13 @@ bool poisson_split_usable(const PoissonArgs &a) {
         default: sm = split_slab_smem<R, 8>(L); break;
     }
     return sm + 4 * 1024 <= 227 * 1024;  // with the static shared arrays
+}
+bool poisson_split_grid(int nx, int ny, int nz, size_t rsize) {
+    return rsize == 8 ? split_grid<double>(nx, ny, nz) : split_grid<float>(nx, ny, nz);
+}
+template <typename R>
+bool poisson_split_usable(const PoissonArgs &a) {
+    return a.cps && split_grid<R>(a.nx, a.ny, a.nz);
 }
 
 // The split path's shared-memory attributes, set before any stream capture

@@ -196,8 +196,8 @@ def test_poisson_fft_sizes_match_oracle(shape, prec, tol):
 def test_poisson_split_path_matches_oracle_and_five_kernel_path(shape, prec, tol):
     """The three-kernel split-y Poisson solve (the x-row kernels fold in the
     radix-S first and last stages of the y transform, NY = 64 S; one slab
-    kernel per (kx, j) runs the 64-point y transforms and the sine-transform z
-    solve on chip) against the oracle's odd-extension DFT solve
+    kernel per (kx, j) runs the 64-point y transforms and the Thomas z solve
+    in FP64 arithmetic on chip) against the oracle's odd-extension DFT solve
     (poisson.cu:78-167) and against the five-kernel path of the same context
     type (ehd_tuning.poisson_path = 1), on random charge."""
     nx, ny, nz = shape
