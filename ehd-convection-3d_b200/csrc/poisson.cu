@@ -1073,12 +1073,20 @@ poisson_rows_fwd_split(const R *__restrict__ q, typename Cplx<R>::T *__restrict_
     const R qm = (R)qmean[2 * (zi + 1) + 1];
     const R ieps = (R)(1.0 / eps);
     load_twiddles<R, N>(tws, tw);
+    // each warp loads a contiguous run of the block's (transform, x) items,
+    // 32 consecutive x at a time, and sums its rows from the registers
+    constexpr int IT = TB * N / 256;            // items per thread
+    constexpr int WI = 32 * IT;                 // items per warp
+    constexpr int SEG = WI >= N ? 1 : N / WI;   // warps per transform
+    constexpr int TPW = WI >= N ? WI / N : 1;   // transforms per warp
+    constexpr int RPT = IT / TPW;               // items per thread and transform
+    __shared__ double part[2 * TB * SEG];
     {
-        constexpr int IT = TB * N / 256;
+        const int warp = tid >> 5, lane = tid & 31;
         R va[IT], vb[IT];
 #pragma unroll
         for (int r = 0; r < IT; ++r) {
-            const int i = tid + 256 * r;
+            const int i = warp * WI + 32 * r + lane;
             const int tr = i / N, x = i - tr * N;
             int ya, yb, g, a;
             split_rows<S, TB>(tr, ya, yb, g, a);
@@ -1087,25 +1095,41 @@ poisson_rows_fwd_split(const R *__restrict__ q, typename Cplx<R>::T *__restrict_
         }
 #pragma unroll
         for (int r = 0; r < IT; ++r) {
-            const int i = tid + 256 * r;
+            const int i = warp * WI + 32 * r + lane;
             const int tr = i / N, x = i - tr * N;
             buf[tr * P + fft::pad(x)] = R2{-(va[r] - qm) * ieps, -(vb[r] - qm) * ieps};
         }
-    }
-    {  // FP64 row sums, one warp per row, fixed order
-        const int warp = tid >> 5, lane = tid & 31;
-        for (int r = warp; r < 2 * TB; r += 8) {
-            int ya, yb, g, a;
-            split_rows<S, TB>(r >> 1, ya, yb, g, a);
-            const int y = (r & 1) ? yb : ya;
-            double sum = 0.0;
-            for (int x = lane; x < N; x += 32) sum += (double)qp[(size_t)N * y + x] - (double)qm;
+        // FP64 sums of q - q_m of both rows of each transform, fixed order
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-            if (lane == 0) rowsum[(size_t)zi * NY + y] = -sum / eps;
+        for (int c = 0; c < TPW; ++c) {
+            double sa = 0.0, sb = 0.0;
+#pragma unroll
+            for (int u = 0; u < RPT; ++u) {
+                sa += (double)va[c * RPT + u] - (double)qm;
+                sb += (double)vb[c * RPT + u] - (double)qm;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                sa += __shfl_xor_sync(0xffffffffu, sa, o);
+                sb += __shfl_xor_sync(0xffffffffu, sb, o);
+            }
+            if (lane == 0) {
+                const int i0 = warp * WI + 32 * RPT * c;
+                const int tr = i0 / N, seg = SEG > 1 ? (i0 - tr * N) / WI : 0;
+                part[(2 * tr) * SEG + seg] = sa;
+                part[(2 * tr + 1) * SEG + seg] = sb;
+            }
         }
     }
     __syncthreads();
+    if (tid < 2 * TB) {
+        double sum = 0.0;
+#pragma unroll
+        for (int k = 0; k < SEG; ++k) sum += part[tid * SEG + k];
+        int ya, yb, g, a;
+        split_rows<S, TB>(tid >> 1, ya, yb, g, a);
+        rowsum[(size_t)zi * NY + ((tid & 1) ? yb : ya)] = -sum / eps;
+    }
     {
         const int tr = tid / G, jj = tid - tr * G;
         fft::run_tile<N, -1>(buf + tr * P, tws, jj);
