@@ -1139,6 +1139,12 @@ poisson_rows_fwd_split(const R *__restrict__ q, typename Cplx<R>::T *__restrict_
     // n per (j, kx)
     const int nblk = S == 1 ? 2 * TB : GB;
     const int n0 = blockIdx.x * nblk;
+    // the twiddles W_NY^(j n) of the block's n, from shared memory
+    __shared__ R2 twn[S == 1 ? 1 : S * GB];
+    if constexpr (S > 1) {
+        for (int i = tid; i < S * GB; i += 256) twn[i] = twy[(i / GB) * (n0 + i % GB)];
+        __syncthreads();
+    }
     for (int i = tid; i < nxh * nblk; i += 256) {
         const int g = i % nblk, kx = i / nblk;
         const int n = n0 + g;
@@ -1155,7 +1161,7 @@ poisson_rows_fwd_split(const R *__restrict__ q, typename Cplx<R>::T *__restrict_
                 R2 acc = x[0];
 #pragma unroll
                 for (int m = 1; m < S; ++m) acc = cadd(acc, mul_ws<S>(x[m], j * m));
-                if (j != 0 && n != 0) acc = cmul(acc, __ldg(twy + j * n));
+                if (j != 0 && n != 0) acc = cmul(acc, twn[j * GB + g]);
                 spl[(((size_t)j * nxh + kx) * nzi + zi) * 64 + n] = acc;
             }
         }
@@ -1643,22 +1649,37 @@ poisson_rows_inv_split(const typename Cplx<R>::T *__restrict__ spl, R *__restric
     // b_j of the group's n at bin kx, the inverse radix-S DFT over j, and the
     // packed inputs Z = A + i B of its transforms at k = kx and k = N - kx
     // (Hermitian completion; the imaginary parts of the bins 0 and N/2 dropped)
+    // every item's loads are issued before the first item is combined
     constexpr int NI = S == 1 ? TB : GB;
-    for (int i = tid; i < nxh * NI; i += 256) {
-        const int g = i % NI, kx = i / NI;
-        R2 xm[S == 1 ? 2 : S];
-        if constexpr (S == 1) {
-            xm[0] = spl[((size_t)kx * nzi + zi) * 64 + n0 + 2 * g];
-            xm[1] = spl[((size_t)kx * nzi + zi) * 64 + n0 + 2 * g + 1];
-        } else {
-            R2 b[S];
+    constexpr int NIT = ((N / 2 + 1) * NI + 255) / 256;  // items per thread (nxh = N/2 + 1)
+    constexpr int NL = S == 1 ? 2 : S;                   // loads per item
+    R2 bv[NIT][NL];
 #pragma unroll
-            for (int j = 0; j < S; ++j) b[j] = spl[(((size_t)j * nxh + kx) * nzi + zi) * 64 + n0 + g];
+    for (int t = 0; t < NIT; ++t) {
+        const int i = tid + 256 * t;
+        if (i < nxh * NI) {
+            const int g = i % NI, kx = i / NI;
+#pragma unroll
+            for (int j = 0; j < NL; ++j)
+                bv[t][j] = S == 1 ? spl[((size_t)kx * nzi + zi) * 64 + n0 + 2 * g + j]
+                                  : spl[(((size_t)j * nxh + kx) * nzi + zi) * 64 + n0 + g];
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < NIT; ++t) {
+        const int i = tid + 256 * t;
+        if (i >= nxh * NI) break;
+        const int g = i % NI, kx = i / NI;
+        R2 xm[NL];
+        if constexpr (S == 1) {
+            xm[0] = bv[t][0];
+            xm[1] = bv[t][1];
+        } else {
 #pragma unroll
             for (int m = 0; m < S; ++m) {
-                R2 acc = b[0];
+                R2 acc = bv[t][0];
 #pragma unroll
-                for (int j = 1; j < S; ++j) acc = cadd(acc, mul_ws<S>(b[j], S - (j * m) % S));
+                for (int j = 1; j < S; ++j) acc = cadd(acc, mul_ws<S>(bv[t][j], S - (j * m) % S));
                 xm[m] = acc;
             }
         }
