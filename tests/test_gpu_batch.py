@@ -66,6 +66,32 @@ def test_batch_steps_match_lone_contexts(mode):
                 assert d == lone[i][1]
 
 
+def test_grouped_launches_keep_each_instances_voltage_and_permittivity():
+    """Mode 0 groups instances only where a grouped Poisson launch may take
+    its constants from the group's first member: three instances on one grid
+    that differ in electrode voltage or permittivity (both enter the Poisson
+    right-hand side, poisson.cu:87-117) each match a lone context."""
+    base = params(SHAPES[0], 200.0).as_dict()
+    ds = [base, dict(base, voltage=1.5 * base["voltage"]), dict(base, eps=2.0 * base["eps"])]
+    p0 = params(SHAPES[0], 200.0)
+    fs = [fields(p0, 50 + i) for i in range(len(ds))]
+    lone = []
+    for d, f in zip(ds, fs):
+        with ehd.Simulation(ehd.Params.from_dict(d), "fp32", row_kernel=False) as sim:
+            sim.set_fields(f)
+            sim.step(5)
+            lone.append(sim.get_fields())
+    with ehd.Batch([ehd.Params.from_dict(d) for d in ds], "fp32") as b:
+        b.set_mode(0)
+        for sim, f in zip(b, fs):
+            sim.set_fields(f)
+        b.step(5)
+        for i, sim in enumerate(b):
+            out = sim.get_fields()
+            for k in O.FIELDS:
+                assert relerr(out[k], lone[i][k]) < 1e-5, (i, k, relerr(out[k], lone[i][k]))
+
+
 def test_batch_inactive_instances_do_not_advance():
     ps = [params(s) for s in SHAPES[:2]]
     with ehd.Batch([to_ehd(p) for p in ps], "fp32") as b:
