@@ -265,10 +265,28 @@ __global__ void gelu_back_kernel(float *__restrict__ d, const float *__restrict_
          i += (size_t)gridDim.x * blockDim.x)
         d[i] *= gelu_grad(z[i]);
 }
+__device__ __forceinline__ float4 gelu_back4(float4 a, float4 b) {
+    return make_float4(a.x * gelu_grad(b.x), a.y * gelu_grad(b.y), a.z * gelu_grad(b.z),
+                       a.w * gelu_grad(b.w));
+}
+// the same on 16-byte vectors (both arrays 16-byte aligned, n4 = n / 4), two
+// vectors a thread in flight per iteration; elementwise the same arithmetic
+__global__ void gelu_back4_kernel(float4 *__restrict__ d, const float4 *__restrict__ z, size_t n4) {
+    const size_t st = (size_t)gridDim.x * blockDim.x;
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    for (; i + st < n4; i += 2 * st) {
+        const float4 a = d[i], b = d[i + st], za = z[i], zb = z[i + st];
+        d[i] = gelu_back4(a, za);
+        d[i + st] = gelu_back4(b, zb);
+    }
+    if (i < n4) d[i] = gelu_back4(d[i], z[i]);
+}
 
-// du = 2 (u - t) / n and the sum of squares (FP64)
+// du = 2 (u - t) / n and the sum of squares (FP64), reduced over the block
+// before one atomic addition per block (256 threads)
 __global__ void mse_kernel(const float *__restrict__ u, const float *__restrict__ t,
                            float *__restrict__ du, size_t n, double *sum) {
+    __shared__ double ws[8];
     double s = 0.0;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x) {
@@ -278,24 +296,76 @@ __global__ void mse_kernel(const float *__restrict__ u, const float *__restrict_
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(sum, s);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = 0.0;
+        for (int w = 0; w < 8; ++w) b += ws[w];
+        atomicAdd(sum, b);
+    }
 }
 
+__device__ __forceinline__ void adam_one(float &p, float g, float &m, float &v, float lr, float b1,
+                                         float b2, float eps, float c1, float c2) {
+    m = b1 * m + (1.f - b1) * g;
+    v = b2 * v + (1.f - b2) * g * g;
+    p -= lr * (m / c1) / (sqrtf(v / c2) + eps);
+}
 __global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g,
                             float *__restrict__ m, float *__restrict__ v, size_t n, float lr,
                             float b1, float b2, float eps, float c1, float c2) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x) {
-        const float gi = g[i];
-        const float mi = b1 * m[i] + (1.f - b1) * gi;
-        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        float pi = p[i], mi = m[i], vi = v[i];
+        adam_one(pi, g[i], mi, vi, lr, b1, b2, eps, c1, c2);
         m[i] = mi;
         v[i] = vi;
-        p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        p[i] = pi;
     }
+}
+// the same on 16-byte vectors (all four arrays 16-byte aligned): the first
+// 4 (n / 4) parameters as vectors, the last n % 4 by the first thread
+__global__ void adam4_kernel(float *__restrict__ p, const float *__restrict__ g,
+                             float *__restrict__ m, float *__restrict__ v, size_t n, float lr,
+                             float b1, float b2, float eps, float c1, float c2) {
+    const size_t n4 = n / 4;
+    float4 *p4 = reinterpret_cast<float4 *>(p), *m4 = reinterpret_cast<float4 *>(m),
+           *v4 = reinterpret_cast<float4 *>(v);
+    const float4 *g4 = reinterpret_cast<const float4 *>(g);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4;
+         i += (size_t)gridDim.x * blockDim.x) {
+        float4 pi = p4[i], mi = m4[i], vi = v4[i];
+        const float4 gi = g4[i];
+        adam_one(pi.x, gi.x, mi.x, vi.x, lr, b1, b2, eps, c1, c2);
+        adam_one(pi.y, gi.y, mi.y, vi.y, lr, b1, b2, eps, c1, c2);
+        adam_one(pi.z, gi.z, mi.z, vi.z, lr, b1, b2, eps, c1, c2);
+        adam_one(pi.w, gi.w, mi.w, vi.w, lr, b1, b2, eps, c1, c2);
+        m4[i] = mi;
+        v4[i] = vi;
+        p4[i] = pi;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        for (size_t i = 4 * n4; i < n; ++i) {
+            float pi = p[i], mi = m[i], vi = v[i];
+            adam_one(pi, g[i], mi, vi, lr, b1, b2, eps, c1, c2);
+            m[i] = mi;
+            v[i] = vi;
+            p[i] = pi;
+        }
 }
 
 unsigned grid_for(size_t n) { return (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16); }
+
+bool aligned16(const void *a) { return ((uintptr_t)a & 15) == 0; }
+
+// d *= gelu'(z) over n elements, on vectors where the layout allows
+void gelu_back(float *d, const float *z, size_t n, cudaStream_t s) {
+    if (n % 4 == 0 && aligned16(d) && aligned16(z))
+        gelu_back4_kernel<<<grid_for(n / 8), 256, 0, s>>>(reinterpret_cast<float4 *>(d),
+                                                         reinterpret_cast<const float4 *>(z), n / 4);
+    else
+        gelu_back_kernel<<<grid_for(n), 256, 0, s>>>(d, z, n);
+}
 
 }  // namespace
 
@@ -957,7 +1027,7 @@ int ehd_fno_backward(ehd_fno *f, int B, const float *a, const float *target, dou
     FNO_CK(weight_bias_grad((long long)rows, f->H, f->cout, f->h, f->H, f->du, f->cout,
                             g + f->oQ2, f->cout, g + f->oq2, s));
     FNO_CK(gemm(input_grad(rows, f->H, f->cout, f->du, pb + f->oQ2, f->dh, 0.f), s));
-    gelu_back_kernel<<<grid_for(rows * f->H), 256, 0, s>>>(f->dh, f->hpre, rows * f->H);
+    gelu_back(f->dh, f->hpre, rows * f->H, s);
     FNO_CK(cudaGetLastError());
     const float *vL = f->z[f->L - 1];
     FNO_CK(weight_bias_grad((long long)rows, f->W, f->H, vL, f->W, f->dh, f->H, g + f->oQ1, f->H,
@@ -967,7 +1037,7 @@ int ehd_fno_backward(ehd_fno *f, int B, const float *a, const float *target, dou
     for (int l = f->L - 1; l >= 0; --l) {
         float *dz = f->dv;  // gradient of the pre-activation, in place
         if (l != f->L - 1) {
-            gelu_back_kernel<<<grid_for(rows * f->W), 256, 0, s>>>(dz, f->z[l], rows * f->W);
+            gelu_back(dz, f->z[l], rows * f->W, s);
             FNO_CK(cudaGetLastError());
         }
         const Off &o = f->lo[l];
@@ -1003,8 +1073,12 @@ int ehd_fno_adam_step(ehd_fno *f, float lr, float b1, float b2, float eps) {
     Dev dg(f->c.device);
     f->adam_t += 1;
     const float c1 = 1.f - std::pow(b1, (float)f->adam_t), c2 = 1.f - std::pow(b2, (float)f->adam_t);
-    adam_kernel<<<grid_for(f->nparam), 256, 0, f->stream>>>(f->param, f->grad, f->adam_m, f->adam_v,
-                                                            f->nparam, lr, b1, b2, eps, c1, c2);
+    if (aligned16(f->param) && aligned16(f->grad) && aligned16(f->adam_m) && aligned16(f->adam_v))
+        adam4_kernel<<<grid_for(f->nparam / 4 + 1), 256, 0, f->stream>>>(
+            f->param, f->grad, f->adam_m, f->adam_v, f->nparam, lr, b1, b2, eps, c1, c2);
+    else
+        adam_kernel<<<grid_for(f->nparam), 256, 0, f->stream>>>(
+            f->param, f->grad, f->adam_m, f->adam_v, f->nparam, lr, b1, b2, eps, c1, c2);
     FNO_CK(cudaGetLastError());
     FNO_CK(refresh(f));
     return EHD_OK;
