@@ -747,9 +747,11 @@ __global__ void __launch_bounds__(256) smallk_kernel(const GemmArgs a) {
 // memory (lanes along the channel: every load reads four fully used 32-byte
 // sectors), the bias sums are taken in FP32 from the same D values before
 // they are rounded to BF16; the block reduces its warps' partial sums in
-// shared memory and adds them to G and gb atomically.
+// shared memory and adds them to G and gb atomically.  Two blocks per SM: at
+// 64 accumulators a thread (MT NT = 16) that spills a few registers and is
+// faster than one block.
 template <int MT, int NT>
-__global__ void __launch_bounds__(256) wgrad_kernel(const float *__restrict__ X, int ldx, int M,
+__global__ void __launch_bounds__(256, 2) wgrad_kernel(const float *__restrict__ X, int ldx, int M,
                                                     const float *__restrict__ D, int ldd, int N,
                                                     long long rows, float *__restrict__ G,
                                                     int ldg, float *__restrict__ gb) {
