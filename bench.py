@@ -148,6 +148,67 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+class NvmlSampler:
+    """SM clock and clock-event reasons read through NVML about every
+    millisecond in a background thread, so that a timed region of a few
+    milliseconds still holds samples (nvidia-smi takes longer than that to
+    start).  The device is found by the PCI bus id of the CUDA device; the
+    nvidia-smi sampler stands in where NVML cannot be loaded."""
+
+    REASONS = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+               "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+               "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+               "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
+
+    def __init__(self, cuda_device: int):
+        import threading
+
+        import pynvml
+        import torch
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(cuda_device)
+        bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+        self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        self.bits = {k: getattr(pynvml, v) for k, v in self.REASONS.items()}
+        self.samples, self.reasons = [], set()
+        self.stop = threading.Event()
+        self.thread = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        nv = self.nv
+        try:
+            while not self.stop.is_set():
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.reasons.update(k for k, b in self.bits.items() if r & b)
+                time.sleep(0.001)
+        except Exception:
+            pass  # the samples so far stand
+
+    def __enter__(self):
+        self.thread.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.thread.join(timeout=5)
+
+    def summary(self):
+        if not self.samples:
+            return None
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": float(self.max_mhz),
+                "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "nvml"}
+
+
+def clock_sampler(cuda_device: int):
+    try:
+        return NvmlSampler(cuda_device)
+    except Exception:
+        return ClockSampler(cuda_device)
+
+
 def workload_params(ehd):
     return ehd.params_from_groups(NX, NY, NZ, 2.0, 2.0, T=200, M=10, C=10, Fe=4000,
                                   lambda_f=0.25, lambda_g=0.25)
@@ -194,17 +255,22 @@ def run_ours(args, rank, world, local_rank):
                              row_kernel=not args.node_kernel)
         if args.poisson_path is not None:
             sim.set_tuning(poisson_path=args.poisson_path)
-        cs = ClockSampler(sampler_gpu) if sampler_gpu is not None else None
+        cs = clock_sampler(sampler_gpu) if sampler_gpu is not None else None
+        # NVML samples the timed region alone; nvidia-smi, slow to start,
+        # samples the warm-up too
+        early = cs is not None and not isinstance(cs, NvmlSampler)
         try:
             sim.set_fields(fields)
-            if cs:
-                cs.__enter__()  # samples through the warm-up and the timed region
+            if early:
+                cs.__enter__()
             sim.step(W)
             sim.synchronize()
             torch.cuda.synchronize()
             barrier()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             clocks = None
+            if cs and not early:
+                cs.__enter__()
             e0.record(stream)
             sim.step(K)
             e1.record(stream)
