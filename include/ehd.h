@@ -276,10 +276,11 @@ int ehd_batch_set_active(ehd_batch *batch, int i, int active);
  * mode 1 (the default): one CUDA graph per step with a branch per instance
  * holding that instance's own launches (the row kernel where it applies);
  * each instance's result is bitwise that of a lone context.  mode 0: instances
- * with the same grid and launch shapes form a group, and each kernel of the
- * step is one launch over every instance of a group (the LBM half on the
- * persistent row kernel or the per-node kernel, as the instances' tuning
- * says), one graph per step holding the groups' launches; an instance's
+ * with the same grid, domain, spacing, permittivity, voltage and launch shapes
+ * form a group, and each kernel of the step is one launch over every instance
+ * of a group (the LBM half on the persistent row kernel or the per-node
+ * kernel, as the instances' tuning says), one graph per step holding the
+ * groups' launches; an instance's
  * result agrees with a lone context to FP32 round-off (the grouped kernels
  * are separate compilations, whose multiply-add contractions may differ). */
 int ehd_batch_set_mode(ehd_batch *batch, int mode);
